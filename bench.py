@@ -1,0 +1,303 @@
+"""Benchmark: viscous (3+1)D hydro step, cell-updates per second.
+
+Workload (the large single event): 385 x 385 x 115 cells, dx = dy = 0.08 fm,
+deta = 0.15, dtau = 0.01 fm, tau0 = 0.6 fm, eta/s = 0.08, s95p-PCE165 EOS,
+FP32, seeded Pb+Pb initial condition (seed 5, b = 8 fm, peak 50 GeV/fm^3).
+One step = one full Runge-Kutta time step (both stages, Israel-Stewart and
+Kurganov-Tadmor parts), i.e. one cell-update per cell.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+value: cell-updates/s over the K timed steps with the state resident in HBM
+(CUDA events on the launch stream, max over ranks). e2e: the same metric
+through the public API with host buffers: load_ini from pinned host memory,
+CLVisc.evolve for K steps, ev_to_host. With N > 1 every rank advances its own
+replica of the event (weak scaling; the path has no exchange step).
+--impl reference times the oracle (the C++/OpenMP restatement of the
+reference kernels, all host threads) on a bounded slab of the same workload.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+NX, NY, NZ = 385, 385, 115
+DX, DZ, DT = 0.08, 0.15, 0.01
+METRIC = 'viscous cell-updates/s (385x385x115)'
+UNIT = 'cell-updates/s'
+# bytes per cell-update the step must move, FP32: 78 reals (5S + 2U with
+# S = 14 state reals, U = 4 udiff reals; the stencil halo and EOS table
+# counted as cache hits)
+ALG_BYTES_PER_CELL_UPDATE = 312
+SLAB_NZ = 16  # CPU-baseline sample: a 385 x 385 x 16 eta slab of the event
+
+
+def make_cfg(nz=NZ, out='/tmp/clv_bench'):
+    from clvisc_b200.config import read_config, set_real
+    cfg = read_config([])
+    cfg.NX, cfg.NY, cfg.NZ = NX, NY, nz
+    cfg.DX = cfg.DY = DX
+    cfg.DZ = DZ
+    cfg.DT = DT
+    cfg.TAU0 = 0.6
+    cfg.eos_type = 'lattice_pce165'
+    cfg.use_float32 = True
+    cfg.ETAOS_XMIN, cfg.ETAOS_YMIN, cfg.ETAOS_LEFT_SLOP, cfg.ETAOS_RIGHT_SLOP = 0.18, 0.08, 0.0, 0.0
+    cfg.TFRZ = 0.137
+    cfg.ntskip = 20
+    cfg.nxskip = cfg.nyskip = 2
+    cfg.nzskip = 1
+    cfg.fPathOut = out
+    return set_real(cfg)
+
+
+def initial_condition(seed=5):
+    from clvisc_b200.initial import glauber_event
+    return glauber_event(NX, NY, NZ, DX, DX, DZ, b=8.0, seed=seed, edmax=50.0)
+
+
+class ClockSampler(object):
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
+         'clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,'
+         'clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap')
+
+    def __init__(self, gpu_index):
+        self.gpu = str(gpu_index)
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(['nvidia-smi', '-i', self.gpu, '--query-gpu=' + self.Q,
+                                          '--format=csv,noheader,nounits', '-lms', '200'],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.t.join(timeout=2)
+
+    def summary(self):
+        sm, smax, reasons = [], [], set()
+        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(',')]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == 'active':
+                    reasons.add(n)
+        if not sm:
+            return {'sm_mhz': None, 'sm_max_mhz': None, 'reasons': [], 'samples': 0}
+        return {'sm_mhz': statistics.median(sm), 'sm_max_mhz': max(smax), 'reasons': sorted(reasons),
+                'samples': len(sm)}
+
+
+def read_peaks():
+    try:
+        with open(os.path.join(ROOT, 'MEASURED_PEAKS.json')) as f:
+            p = json.load(f)
+        return float(p['hbm_gbs']), 'measured'
+    except (OSError, KeyError, ValueError):
+        return 6650.0, 'fallback'
+
+
+def read_traffic():
+    """DRAM bytes per cell-update of the stage kernel from the committed ncu
+    summary (profiles/visc_stage_*.txt, line 'dram_bytes_per_cell_update: X')."""
+    d = os.path.join(ROOT, 'profiles')
+    try:
+        for fn in sorted(os.listdir(d)):
+            if fn.startswith('visc_stage') and fn.endswith('.txt'):
+                for ln in open(os.path.join(d, fn)):
+                    if ln.startswith('dram_bytes_per_cell_update:'):
+                        return float(ln.split(':')[1])
+    except OSError:
+        pass
+    return None
+
+
+def cpu_baseline(steps=2, warmup=0):
+    """The oracle on a 385 x 385 x SLAB_NZ slab, all host threads."""
+    sys.path.insert(0, os.path.join(ROOT, 'oracle'))
+    import numpy as np
+    import oracle as O
+    cfg = make_cfg(nz=SLAB_NZ)
+    ic = initial_condition().reshape(NX, NY, NZ, 4)
+    k0 = NZ // 2 - SLAB_NZ // 2
+    sub = np.ascontiguousarray(ic[:, :, k0:k0 + SLAB_NZ]).reshape(-1, 4)
+    o = O.OracleVisc(cfg)
+    o.load_ini(sub)
+    for n in range(warmup):
+        o.step(n)
+    t = time.perf_counter()
+    for n in range(warmup, warmup + steps):
+        o.step(n)
+    dt = time.perf_counter() - t
+    cores = int(os.environ.get('OMP_NUM_THREADS', os.cpu_count() or 1))
+    cells = NX * NY * SLAB_NZ
+    return {'value': cells * steps / dt, 'unit': UNIT, 'cores': cores, 'kind': 'port',
+            'sample': '%d steps of a %dx%dx%d eta slab of the same event (oracle, OpenMP)' % (steps, NX, NY, SLAB_NZ),
+            'seconds': dt}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    cb = cpu_baseline(steps=max(1, args.steps), warmup=min(args.warmup, 1))
+    line = {'impl': 'reference', 'metric': METRIC, 'value': cb['value'], 'unit': UNIT, 'n_gpus': world,
+            'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': 1e3 * cb['seconds'] / max(1, args.steps),
+            'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic',
+            'config': {'workload': 'viscous 385x385x115 Pb+Pb b=8 fm, FP32, lattice EOS (slab sample)'},
+            'cpu_baseline': {k: cb[k] for k in ('value', 'unit', 'cores', 'kind', 'sample')},
+            'e2e': {'value': cb['value'], 'unit': UNIT, 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_gpu(args, rank, world, dist):
+    import numpy as np
+    import torch
+    from clvisc_b200.visc import CLVisc
+    dev = int(os.environ.get('LOCAL_RANK', 0))
+    torch.cuda.set_device(dev)
+    cfg = make_cfg(out='/tmp/clv_bench_r%d' % rank)
+    ic = initial_condition(seed=5)
+    v = CLVisc(cfg, gpu_id=dev)
+    v.load_ini(ic)
+    stream = torch.cuda.current_stream()
+    cells = NX * NY * NZ
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    # device-resident timing: K fused steps
+    for n in range(args.warmup):
+        v.step(n)
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(dev) as clocks:
+        e0.record(stream)
+        for n in range(args.warmup, args.warmup + args.steps):
+            v.step(n)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    barrier()
+    if dist is not None:
+        t = torch.tensor([ms], device='cuda')
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * cells * args.steps / (ms * 1e-3)
+
+    # end to end through the public API with host buffers
+    host_ic = torch.from_numpy(np.ascontiguousarray(ic)).pin_memory()
+    v2 = CLVisc(cfg, gpu_id=dev)
+    torch.cuda.synchronize()
+    barrier()
+    t0 = time.perf_counter()
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    v2.load_ini(host_ic)
+    v2.evolve(max_loops=args.steps, force_run_to_maxloop=True, save_hypersf=False, save_pi=False)
+    out = v2.ideal.ev_to_host()
+    f1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = f0.elapsed_time(f1)
+    e2e_wall = time.perf_counter() - t0
+    if dist is not None:
+        t = torch.tensor([e2e_ms], device='cuda')
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e = world * cells * args.steps / (e2e_ms * 1e-3)
+    h2d = ic.nbytes / args.steps
+    d2h = out.nbytes / args.steps
+
+    peak, peak_kind = read_peaks()
+    achieved = value / world * ALG_BYTES_PER_CELL_UPDATE / 1e9
+    traffic = read_traffic()
+    if rank == 0:
+        line = {
+            'metric': METRIC, 'value': value, 'unit': UNIT, 'n_gpus': world, 'steps': args.steps,
+            'warmup': args.warmup, 'ms_per_step': ms / args.steps, 'higher_is_better': True, 'scaling': 'weak',
+            'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic',
+            'config': {'workload': 'viscous 385x385x115 Pb+Pb b=8 fm seed 5, FP32, lattice EOS, dtau=0.01',
+                       'cells': cells, 'l2': 'inputs larger than L2 (state 0.95 GB per stage)',
+                       'parallelism': 'replicas x%d' % world},
+            'e2e': {'value': e2e, 'unit': UNIT, 'h2d_bytes_per_step': h2d, 'd2h_bytes_per_step': d2h,
+                    'wall_s': e2e_wall},
+            'gpu_launches': 2 * args.steps,
+            'roofline': {'bound': 'hbm', 'achieved': achieved, 'peak': peak, 'unit': 'GB/s',
+                         'frac': achieved / peak, 'peak_kind': peak_kind,
+                         'traffic': None if traffic is None else traffic * cells / 2,
+                         'alg_bytes_per_launch': ALG_BYTES_PER_CELL_UPDATE * cells / 2,
+                         'kernel': 'visc_stage_kernel<float,IS+KT> (2 launches per step)'},
+            'clocks': clocks.summary(),
+        }
+        if not args.no_cpu_baseline:
+            cb = cpu_baseline(steps=2)
+            line['cpu_baseline'] = {k: cb[k] for k in ('value', 'unit', 'cores', 'kind', 'sample')}
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--gpus', type=int, default=1)
+    ap.add_argument('--steps', type=int, default=20)
+    ap.add_argument('--warmup', type=int, default=3)
+    ap.add_argument('--impl', default='b200', choices=['b200', 'reference'])
+    ap.add_argument('--no-cpu-baseline', action='store_true')
+    args = ap.parse_args()
+    world = int(os.environ.get('WORLD_SIZE', '1'))
+    rank = int(os.environ.get('RANK', '0'))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as tdist
+        backend = 'gloo' if args.impl == 'reference' else 'nccl'
+        if backend == 'nccl':
+            import torch
+            torch.cuda.set_device(int(os.environ.get('LOCAL_RANK', 0)))
+        tdist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+        dist = tdist
+    try:
+        if args.impl == 'reference':
+            run_reference(args, rank, world)
+        else:
+            run_gpu(args, rank, world, dist)
+    finally:
+        if dist is not None:
+            dist.destroy_process_group()
+
+
+if __name__ == '__main__':
+    main()

@@ -1,0 +1,106 @@
+"""ctypes binding of libclvisc_b200.so (include/clvisc_b200.h).
+
+The library is the only compute path: if it cannot be loaded, every entry
+point raises, there is no CPU fallback.
+"""
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, 'libclvisc_b200.so')
+
+CLV_PART_IS = 1
+CLV_PART_KT = 2
+CLV_FLAG_RIEMANN_TEST = 1
+CLV_FLAG_GUBSER_VISC_TEST = 2
+CLV_FLAG_PIMN_OMEGA_COUPLING = 4
+CLV_FLAG_OMEGA_OMEGA_COUPLING = 8
+
+CLV_ERR = {-1: 'invalid argument', -2: 'CUDA error', -3: 'capacity exceeded'}
+
+
+class ClvParams(ctypes.Structure):
+    _fields_ = [
+        ('nx', ctypes.c_int), ('ny', ctypes.c_int), ('nz', ctypes.c_int),
+        ('ld', ctypes.c_longlong),
+        ('precision', ctypes.c_int),
+        ('dt', ctypes.c_float), ('dx', ctypes.c_float), ('dy', ctypes.c_float), ('dz', ctypes.c_float),
+        ('tau0', ctypes.c_float),
+        ('etaos_xmin', ctypes.c_float), ('etaos_ymin', ctypes.c_float),
+        ('etaos_left_slop', ctypes.c_float), ('etaos_right_slop', ctypes.c_float), ('lam1', ctypes.c_float),
+        ('efrz', ctypes.c_float),
+        ('nxskip', ctypes.c_int), ('nyskip', ctypes.c_int), ('nzskip', ctypes.c_int),
+        ('eos_ed_start', ctypes.c_float), ('eos_ed_step', ctypes.c_float),
+        ('eos_num_ed', ctypes.c_int), ('eos_nrow', ctypes.c_int), ('eos_ncol', ctypes.c_int),
+        ('eos_table', ctypes.c_void_p),
+        ('flags', ctypes.c_int),
+    ]
+
+
+class ClvViscBuffers(ctypes.Structure):
+    _fields_ = [
+        ('ev_st', ctypes.c_void_p), ('pi_st', ctypes.c_void_p),
+        ('ev1', ctypes.c_void_p), ('ev2_ed', ctypes.c_void_p),
+        ('pi1', ctypes.c_void_p), ('pi_n', ctypes.c_void_p), ('pi_new_in', ctypes.c_void_p),
+        ('ev_new', ctypes.c_void_p), ('pi_new', ctypes.c_void_p),
+        ('src', ctypes.c_void_p), ('udiff', ctypes.c_void_p), ('goodcell', ctypes.c_void_p),
+        ('edmax_key', ctypes.c_void_p),
+        ('write_src', ctypes.c_int), ('write_udiff', ctypes.c_int),
+    ]
+
+
+_lib = None
+_load_error = None
+
+_P = ctypes.POINTER(ClvParams)
+_VP = ctypes.c_void_p
+_SIGS = {
+    'clv_version': ([], ctypes.c_int),
+    'clv_last_error': ([], ctypes.c_char_p),
+    'clv_alignment': ([], ctypes.c_int),
+    'clv_ideal_stage': ([_P, ctypes.c_int, ctypes.c_double, _VP, _VP, _VP, _VP, ctypes.c_int, _VP, _VP], ctypes.c_int),
+    'clv_visc_stage': ([_P, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.POINTER(ClvViscBuffers), _VP],
+                       ctypes.c_int),
+    'clv_visc_initialize': ([_P, _VP, _VP, _VP, _VP, ctypes.c_double, _VP], ctypes.c_int),
+    'clv_get_udiff': ([_P, _VP, _VP, _VP, _VP], ctypes.c_int),
+    'clv_max_ed_reset': ([_P, _VP, _VP], ctypes.c_int),
+    'clv_max_ed': ([_P, _VP, _VP, _VP], ctypes.c_int),
+    'clv_max_ed_read': ([_P, _VP, ctypes.POINTER(ctypes.c_double), _VP], ctypes.c_int),
+    'clv_hypersf_scratch_bytes': ([_P], ctypes.c_size_t),
+    'clv_hypersf_append': ([_P, ctypes.c_int, ctypes.c_double, ctypes.c_double, _VP, _VP, _VP, _VP, _VP, _VP, _VP,
+                            ctypes.c_longlong, _VP, _VP, ctypes.c_size_t, _VP], ctypes.c_int),
+    'clv_aos_to_soa': ([_P, _VP, _VP, ctypes.c_longlong, ctypes.c_int, _VP], ctypes.c_int),
+    'clv_soa_to_aos': ([_P, _VP, _VP, ctypes.c_longlong, ctypes.c_int, _VP], ctypes.c_int),
+}
+
+
+def exported_symbols():
+    """Names of the entry points this binding expects the library to export."""
+    return sorted(_SIGS)
+
+
+def load(path=LIB_PATH):
+    """Load the CUDA library (raises if it is missing or incomplete)."""
+    global _lib, _load_error
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError('libclvisc_b200.so not built (%s); run python -m clvisc_b200.build' % path)
+    lib = ctypes.CDLL(path)
+    for name, (args, res) in _SIGS.items():
+        f = getattr(lib, name)
+        f.argtypes = args
+        f.restype = res
+    _lib = lib
+    return lib
+
+
+def check(rc, what):
+    if rc != 0:
+        msg = _lib.clv_last_error().decode() if _lib is not None else ''
+        raise RuntimeError('%s failed: %s (%d) %s' % (what, CLV_ERR.get(rc, 'error'), rc, msg))
+
+
+def ptr(t):
+    """Device pointer of a torch tensor (or None)."""
+    return None if t is None else ctypes.c_void_p(t.data_ptr())

@@ -1,0 +1,55 @@
+"""Build libclvisc_b200.so in-tree with nvcc for sm_100a.
+
+The library is compiled without fused multiply-add contraction and with IEEE
+division and square root, so each kernel's arithmetic matches a plain
+evaluation of the reference OpenCL source in the same precision.
+
+    python -m clvisc_b200.build          # build if sources changed
+    python -m clvisc_b200.build --force  # rebuild
+"""
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+LIB = os.path.join(HERE, 'libclvisc_b200.so')
+SOURCES = ['csrc/clv_capi.cu']
+DEPS = ['csrc/clv_device.cuh', 'csrc/clv_stage.cuh', 'csrc/clv_misc.cuh', 'csrc/clv_hypersf.cuh',
+        '../include/clvisc_b200.h']
+
+NVCC_FLAGS = [
+    '-gencode', 'arch=compute_100a,code=sm_100a',
+    '-O3', '-lineinfo', '-std=c++17',
+    '--fmad=false', '-prec-div=true', '-prec-sqrt=true', '-ftz=false',
+    '-Xcompiler', '-fPIC', '-shared',
+]
+
+
+def nvcc():
+    for cand in (os.environ.get('NVCC'), '/usr/local/cuda/bin/nvcc', 'nvcc'):
+        if cand and (os.path.isabs(cand) and os.path.exists(cand) or not os.path.isabs(cand)):
+            return cand
+    return 'nvcc'
+
+
+def stale():
+    if not os.path.exists(LIB):
+        return True
+    t = os.path.getmtime(LIB)
+    return any(os.path.getmtime(os.path.join(HERE, s)) > t for s in SOURCES + DEPS)
+
+
+def build(force=False, verbose=False, extra=()):
+    if not force and not stale():
+        return LIB
+    cmd = [nvcc()] + NVCC_FLAGS + list(extra) + ['-o', LIB] + [os.path.join(HERE, s) for s in SOURCES]
+    if verbose:
+        print(' '.join(cmd))
+    subprocess.check_call(cmd, cwd=HERE)
+    return LIB
+
+
+if __name__ == '__main__':
+    extra = ['-Xptxas', '-v'] if '-v' in sys.argv else []
+    print(build(force='--force' in sys.argv, verbose=True, extra=extra))

@@ -1,0 +1,289 @@
+// extern "C" entry points of libclvisc_b200.so (declared in include/clvisc_b200.h).
+#include <cfloat>
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "../../include/clvisc_b200.h"
+#include "clv_device.cuh"
+#include "clv_hypersf.cuh"
+#include "clv_misc.cuh"
+#include "clv_stage.cuh"
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const char* fmt, const char* what = "") {
+  char buf[256];
+  snprintf(buf, sizeof(buf), fmt, what);
+  g_err = buf;
+  return code;
+}
+int cuda_check(const char* where) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    g_err = std::string(where) + ": " + cudaGetErrorString(e);
+    return CLV_ERR_CUDA;
+  }
+  return CLV_OK;
+}
+inline cudaStream_t S(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+constexpr int kAlign = 16;
+inline bool aligned(const void* q) { return (reinterpret_cast<uintptr_t>(q) % kAlign) == 0; }
+
+int to_params(const clv_params* in, clv::Params* out) {
+  if (!in) return fail(CLV_ERR_INVALID, "null clv_params%s");
+  if (in->precision != 4 && in->precision != 8) return fail(CLV_ERR_INVALID, "precision must be 4 or 8%s");
+  if (in->nx < 1 || in->ny < 1 || in->nz < 1) return fail(CLV_ERR_INVALID, "grid sizes must be >= 1%s");
+  long long n = (long long)in->nx * in->ny * in->nz;
+  if (in->ld < n) return fail(CLV_ERR_INVALID, "ld must be >= nx*ny*nz%s");
+  if ((in->ld * in->precision) % kAlign) return fail(CLV_ERR_INVALID, "ld*precision must be a multiple of 16%s");
+  if (10 * in->ld >= (1ll << 40)) return fail(CLV_ERR_INVALID, "grid too large%s");
+  if (!in->eos_table || in->eos_nrow < 1 || in->eos_ncol < 1) return fail(CLV_ERR_INVALID, "EOS table missing%s");
+  if (!(in->eos_ed_step > 0.0f)) return fail(CLV_ERR_INVALID, "eos_ed_step must be > 0%s");
+  if (in->nxskip < 1 || in->nyskip < 1 || in->nzskip < 1) return fail(CLV_ERR_INVALID, "skips must be >= 1%s");
+  clv::Params& p = *out;
+  p.nx = in->nx; p.ny = in->ny; p.nz = in->nz; p.ld = in->ld;
+  p.DT = in->dt; p.DX = in->dx; p.DY = in->dy; p.DZ = in->dz; p.TAU0 = in->tau0;
+  p.ETAOS_XMIN = in->etaos_xmin; p.ETAOS_YMIN = in->etaos_ymin;
+  p.ETAOS_LEFT_SLOP = in->etaos_left_slop; p.ETAOS_RIGHT_SLOP = in->etaos_right_slop; p.LAM1 = in->lam1;
+  p.EFRZ = in->efrz;
+  p.nxskip = in->nxskip; p.nyskip = in->nyskip; p.nzskip = in->nzskip;
+  p.eos_start = in->eos_ed_start; p.eos_step = in->eos_ed_step;
+  p.eos_num = in->eos_num_ed; p.eos_nrow = in->eos_nrow; p.eos_ncol = in->eos_ncol;
+  p.eos = in->eos_table;
+  p.flags = in->flags;
+  return CLV_OK;
+}
+inline long long ncell(const clv::Params& p) { return (long long)p.nx * p.ny * p.nz; }
+inline unsigned int nblk(long long n, int bs) { return (unsigned int)((n + bs - 1) / bs); }
+
+template <class real>
+int visc_stage_t(const clv::Params& p, int step, double tau, int parts, const clv_visc_buffers* b, cudaStream_t s) {
+  clv::ViscBuffers<real> v;
+  v.ev_st = (const real*)b->ev_st; v.pi_st = (const real*)b->pi_st;
+  v.ev1 = (const real*)b->ev1; v.ev2e = (const real*)b->ev2_ed;
+  v.pi1 = (const real*)b->pi1; v.pin = (const real*)b->pi_n; v.pi2in = (const real*)b->pi_new_in;
+  v.evnew = (real*)b->ev_new; v.pinew = (real*)b->pi_new;
+  v.src = (real*)b->src; v.udiff = (real*)b->udiff; v.goodcell = b->goodcell;
+  v.edmax_key = (typename clv::KeyT<real>::type*)b->edmax_key;
+  v.write_src = b->write_src; v.write_udiff = b->write_udiff;
+  const bool is = parts & CLV_PART_IS, kt = parts & CLV_PART_KT;
+  if (!v.ev_st || !v.pi_st || !v.ev1 || !v.src) return fail(CLV_ERR_INVALID, "visc stage: null stencil/src buffer%s");
+  if (is && (!v.pi1 || !v.pinew || !v.udiff || !v.goodcell || (step == 1 && !v.ev2e)))
+    return fail(CLV_ERR_INVALID, "visc stage: null buffer for the pi update%s");
+  if (kt && (!v.evnew || !v.pin || (!is && !v.pi2in))) return fail(CLV_ERR_INVALID, "visc stage: null buffer for update_ev%s");
+  if (v.write_udiff && (!kt || !v.udiff)) return fail(CLV_ERR_INVALID, "visc stage: write_udiff needs CLV_PART_KT%s");
+  const int bs = 128;
+  dim3 grid(nblk(ncell(p), bs));
+  real t = (real)tau;
+  if (is && kt) clv::visc_stage_kernel<real, true, true><<<grid, bs, 0, s>>>(p, v, step, t);
+  else if (is) clv::visc_stage_kernel<real, true, false><<<grid, bs, 0, s>>>(p, v, step, t);
+  else clv::visc_stage_kernel<real, false, true><<<grid, bs, 0, s>>>(p, v, step, t);
+  return cuda_check("visc_stage_kernel");
+}
+
+template <class real>
+int ideal_stage_t(const clv::Params& p, int step, double tau, const void* ev_st, const void* ev1, void* ev_new,
+                  void* src, int write_src, void* key, cudaStream_t s) {
+  clv::IdealBuffers<real> b;
+  b.ev_st = (const real*)ev_st; b.ev1 = (const real*)ev1; b.evnew = (real*)ev_new; b.src = (real*)src;
+  b.edmax_key = (typename clv::KeyT<real>::type*)key; b.write_src = write_src;
+  const int bs = 128;
+  clv::ideal_stage_kernel<real><<<nblk(ncell(p), bs), bs, 0, s>>>(p, b, step, (real)tau);
+  return cuda_check("ideal_stage_kernel");
+}
+
+template <class real>
+size_t hsf_scratch(const clv::Params& p) {
+  clv::CubeGrid g = clv::cube_grid(p);
+  long long nc = (long long)g.nx * g.ny * g.nz;
+  long long nb = (nc + 255) / 256;
+  size_t bytes = 0;
+  bytes += ((nc + 255) / 256) * 256;          // marks
+  bytes += (size_t)nb * sizeof(int) + 256;    // block counts / offsets
+  bytes += (size_t)nc * sizeof(int) + 256;    // cube list
+  bytes += 2 * sizeof(long long) + 256;       // count
+  return bytes;
+}
+
+template <class real>
+int hypersf_t(const clv::Params& p, int visc, double tau_old, double tau_new, const void* ev_old,
+              const void* ev_new, const void* pi_old, const void* pi_new, void* sf, void* txyz, void* pisf,
+              long long capacity, long long* total, void* scratch, size_t scratch_bytes, cudaStream_t s) {
+  if (!ev_old || !ev_new || !sf || !txyz || !total || !scratch) return fail(CLV_ERR_INVALID, "hypersf: null pointer%s");
+  if (visc && (!pi_old || !pi_new)) return fail(CLV_ERR_INVALID, "hypersf: visc needs pi_old and pi_new%s");
+  if (scratch_bytes < hsf_scratch<real>(p)) return fail(CLV_ERR_INVALID, "hypersf: scratch too small%s");
+  clv::CubeGrid g = clv::cube_grid(p);
+  long long nc = (long long)g.nx * g.ny * g.nz;
+  unsigned int nb = nblk(nc, 256);
+  char* sp = (char*)scratch;
+  uint8_t* mark = (uint8_t*)sp; sp += ((nc + 255) / 256) * 256;
+  int* bcount = (int*)sp; sp += (((size_t)nb * sizeof(int) + 255) / 256) * 256;
+  int* list = (int*)sp; sp += (((size_t)nc * sizeof(int) + 255) / 256) * 256;
+  long long* count = (long long*)sp;
+  clv::hsf_mark_kernel<real><<<nb, 256, 0, s>>>(p, (const real*)ev_old, (const real*)ev_new, visc, mark, bcount);
+  clv::hsf_scan_kernel<<<1, 1024, 0, s>>>(bcount, (int)nb, count);
+  clv::hsf_compact_kernel<<<nb, 256, 0, s>>>(nc, mark, bcount, list);
+  clv::hsf_element_kernel<real><<<148 * 4, 128, 0, s>>>(
+      p, (const real*)ev_old, (const real*)ev_new, (const real*)pi_old, (const real*)pi_new, (real)tau_old,
+      (real)tau_new, visc, list, count, total, (real*)sf, (real*)txyz, (real*)pisf, capacity);
+  clv::hsf_advance_kernel<<<1, 1, 0, s>>>(count, total);
+  return cuda_check("hypersf kernels");
+}
+
+}  // namespace
+
+extern "C" {
+
+int clv_version(void) { return 0x000101; }
+const char* clv_last_error(void) { return g_err.c_str(); }
+int clv_alignment(void) { return kAlign; }
+
+int clv_ideal_stage(const clv_params* pp, int step, double tau, const void* ev_st, const void* ev1, void* ev_new,
+                    void* src, int write_src, void* edmax_key, void* stream) {
+  clv::Params p;
+  int rc = to_params(pp, &p);
+  if (rc) return rc;
+  if (step != 1 && step != 2) return fail(CLV_ERR_INVALID, "step must be 1 or 2%s");
+  if (!ev_st || !ev1 || !ev_new || !src) return fail(CLV_ERR_INVALID, "ideal stage: null buffer%s");
+  if (!aligned(ev_st) || !aligned(ev1) || !aligned(ev_new) || !aligned(src)) return fail(CLV_ERR_INVALID, "ideal stage: misaligned buffer%s");
+  if (pp->precision == 4) return ideal_stage_t<float>(p, step, tau, ev_st, ev1, ev_new, src, write_src, edmax_key, S(stream));
+  return ideal_stage_t<double>(p, step, tau, ev_st, ev1, ev_new, src, write_src, edmax_key, S(stream));
+}
+
+int clv_visc_stage(const clv_params* pp, int step, double tau, int parts, const clv_visc_buffers* b, void* stream) {
+  clv::Params p;
+  int rc = to_params(pp, &p);
+  if (rc) return rc;
+  if (step != 1 && step != 2) return fail(CLV_ERR_INVALID, "step must be 1 or 2%s");
+  if (!b || !(parts & (CLV_PART_IS | CLV_PART_KT)) || (parts & ~3)) return fail(CLV_ERR_INVALID, "bad parts or buffers%s");
+  if (pp->precision == 4) return visc_stage_t<float>(p, step, tau, parts, b, S(stream));
+  return visc_stage_t<double>(p, step, tau, parts, b, S(stream));
+}
+
+int clv_visc_initialize(const clv_params* pp, void* pi1, unsigned char* goodcell, void* udiff, const void* ev,
+                        double tau, void* stream) {
+  clv::Params p;
+  int rc = to_params(pp, &p);
+  if (rc) return rc;
+  if (!pi1 || !goodcell || !udiff || !ev) return fail(CLV_ERR_INVALID, "visc_initialize: null buffer%s");
+  const int bs = 256;
+  if (pp->precision == 4)
+    clv::visc_initialize_kernel<float><<<nblk(ncell(p), bs), bs, 0, S(stream)>>>(p, (float*)pi1, goodcell, (float*)udiff, (const float*)ev, (float)tau);
+  else
+    clv::visc_initialize_kernel<double><<<nblk(ncell(p), bs), bs, 0, S(stream)>>>(p, (double*)pi1, goodcell, (double*)udiff, (const double*)ev, tau);
+  return cuda_check("visc_initialize_kernel");
+}
+
+int clv_get_udiff(const clv_params* pp, void* udiff, const void* ev0, const void* ev1, void* stream) {
+  clv::Params p;
+  int rc = to_params(pp, &p);
+  if (rc) return rc;
+  if (!udiff || !ev0 || !ev1) return fail(CLV_ERR_INVALID, "get_udiff: null buffer%s");
+  const int bs = 256;
+  if (pp->precision == 4)
+    clv::get_udiff_kernel<float><<<nblk(ncell(p), bs), bs, 0, S(stream)>>>(p, (float*)udiff, (const float*)ev0, (const float*)ev1);
+  else
+    clv::get_udiff_kernel<double><<<nblk(ncell(p), bs), bs, 0, S(stream)>>>(p, (double*)udiff, (const double*)ev0, (const double*)ev1);
+  return cuda_check("get_udiff_kernel");
+}
+
+int clv_max_ed_reset(const clv_params* pp, void* key, void* stream) {
+  if (!pp || !key || (pp->precision != 4 && pp->precision != 8)) return fail(CLV_ERR_INVALID, "max_ed_reset: bad argument%s");
+  cudaMemsetAsync(key, 0, pp->precision, S(stream));
+  return cuda_check("cudaMemsetAsync");
+}
+
+int clv_max_ed(const clv_params* pp, const void* ev, void* key, void* stream) {
+  clv::Params p;
+  int rc = to_params(pp, &p);
+  if (rc) return rc;
+  if (!ev || !key) return fail(CLV_ERR_INVALID, "max_ed: null buffer%s");
+  const long long n = ncell(p);
+  unsigned int g = (unsigned int)((n + 255) / 256);
+  if (g > 148u * 16u) g = 148u * 16u;
+  if (pp->precision == 4)
+    clv::max_key_kernel<float><<<g, 256, 0, S(stream)>>>((const float*)ev, n, (unsigned int*)key);
+  else
+    clv::max_key_kernel<double><<<g, 256, 0, S(stream)>>>((const double*)ev, n, (unsigned long long*)key);
+  return cuda_check("max_key_kernel");
+}
+
+int clv_max_ed_read(const clv_params* pp, const void* key, double* out, void* stream) {
+  if (!pp || !key || !out) return fail(CLV_ERR_INVALID, "max_ed_read: null argument%s");
+  if (pp->precision == 4) {
+    unsigned int k = 0;
+    cudaMemcpyAsync(&k, key, sizeof(k), cudaMemcpyDeviceToHost, S(stream));
+    cudaStreamSynchronize(S(stream));
+    int rc = cuda_check("max_ed_read");
+    if (rc) return rc;
+    if (k == 0) { *out = -FLT_MAX; return CLV_OK; }
+    unsigned int b = (k & 0x80000000u) ? (k & 0x7fffffffu) : ~k;
+    float f;
+    memcpy(&f, &b, 4);
+    *out = f;
+  } else {
+    unsigned long long k = 0;
+    cudaMemcpyAsync(&k, key, sizeof(k), cudaMemcpyDeviceToHost, S(stream));
+    cudaStreamSynchronize(S(stream));
+    int rc = cuda_check("max_ed_read");
+    if (rc) return rc;
+    if (k == 0) { *out = -FLT_MAX; return CLV_OK; }
+    unsigned long long b = (k & 0x8000000000000000ull) ? (k & 0x7fffffffffffffffull) : ~k;
+    double f;
+    memcpy(&f, &b, 8);
+    *out = f;
+  }
+  return CLV_OK;
+}
+
+size_t clv_hypersf_scratch_bytes(const clv_params* pp) {
+  clv::Params p;
+  if (to_params(pp, &p)) return 0;
+  return pp->precision == 4 ? hsf_scratch<float>(p) : hsf_scratch<double>(p);
+}
+
+int clv_hypersf_append(const clv_params* pp, int visc, double tau_old, double tau_new, const void* ev_old,
+                       const void* ev_new, const void* pi_old, const void* pi_new, void* sf, void* txyz, void* pisf,
+                       long long capacity, long long* total, void* scratch, size_t scratch_bytes, void* stream) {
+  clv::Params p;
+  int rc = to_params(pp, &p);
+  if (rc) return rc;
+  if (capacity < 0) return fail(CLV_ERR_INVALID, "hypersf: negative capacity%s");
+  if (pp->precision == 4)
+    return hypersf_t<float>(p, visc, tau_old, tau_new, ev_old, ev_new, pi_old, pi_new, sf, txyz, pisf, capacity,
+                            total, scratch, scratch_bytes, S(stream));
+  return hypersf_t<double>(p, visc, tau_old, tau_new, ev_old, ev_new, pi_old, pi_new, sf, txyz, pisf, capacity,
+                           total, scratch, scratch_bytes, S(stream));
+}
+
+int clv_aos_to_soa(const clv_params* pp, const void* aos, void* soa, long long n, int w, void* stream) {
+  clv::Params p;
+  int rc = to_params(pp, &p);
+  if (rc) return rc;
+  if (!aos || !soa || n < 0 || n > p.ld || w < 1 || w > 16) return fail(CLV_ERR_INVALID, "aos_to_soa: bad argument%s");
+  if (n == 0) return CLV_OK;
+  if (pp->precision == 4)
+    clv::aos_to_soa_kernel<float><<<nblk(n * w, 256), 256, 0, S(stream)>>>((const float*)aos, (float*)soa, n, w, p.ld);
+  else
+    clv::aos_to_soa_kernel<double><<<nblk(n * w, 256), 256, 0, S(stream)>>>((const double*)aos, (double*)soa, n, w, p.ld);
+  return cuda_check("aos_to_soa_kernel");
+}
+
+int clv_soa_to_aos(const clv_params* pp, const void* soa, void* aos, long long n, int w, void* stream) {
+  clv::Params p;
+  int rc = to_params(pp, &p);
+  if (rc) return rc;
+  if (!aos || !soa || n < 0 || n > p.ld || w < 1 || w > 16) return fail(CLV_ERR_INVALID, "soa_to_aos: bad argument%s");
+  if (n == 0) return CLV_OK;
+  if (pp->precision == 4)
+    clv::soa_to_aos_kernel<float><<<nblk(n * w, 256), 256, 0, S(stream)>>>((const float*)soa, (float*)aos, n, w, p.ld);
+  else
+    clv::soa_to_aos_kernel<double><<<nblk(n * w, 256), 256, 0, S(stream)>>>((const double*)soa, (double*)aos, n, w, p.ld);
+  return cuda_check("soa_to_aos_kernel");
+}
+
+}  // extern "C"

@@ -1,0 +1,281 @@
+// Device-side building blocks of the CLVisc hydro step for sm_100a.
+//
+// Every floating-point expression keeps the operand order and the
+// float-literal constants of the reference OpenCL kernels
+// (pyvisc/kernel/helper.h, eos_table.h, kernel_*.cl), and the library is
+// compiled with --fmad=false and IEEE division/square root, so each cell's
+// result is bit-identical to a straightforward evaluation of the reference
+// source in the same precision.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace clv {
+
+// run constants, passed by value to every kernel
+struct Params {
+  int nx, ny, nz;
+  long long ld;  // plane stride of every SoA field, in elements
+  float DT, DX, DY, DZ, TAU0;
+  float ETAOS_XMIN, ETAOS_YMIN, ETAOS_LEFT_SLOP, ETAOS_RIGHT_SLOP, LAM1;
+  float EFRZ;
+  int nxskip, nyskip, nzskip;
+  float eos_start, eos_step;
+  int eos_num, eos_nrow, eos_ncol;
+  const float* eos;  // nrow*ncol texels of (cs2, p, T, s)
+  int flags;
+};
+
+enum : int {
+  FLAG_RIEMANN = 1,
+  FLAG_GUBSER_VISC = 2,
+  FLAG_PIMN_OMEGA = 4,
+  FLAG_OMEGA_OMEGA = 8,
+};
+
+template <class real> struct Acu;
+template <> struct Acu<float> { static constexpr float v = 1.0E-7f; };
+template <> struct Acu<double> { static constexpr double v = 1.0E-14; };
+
+#define CLV_THETA 1.1f
+#define CLV_HBARC 0.19733f
+
+// OpenCL min/max/sign semantics (helper.h uses the builtins)
+template <class real> __device__ __forceinline__ real cmin(real x, real y) { return (y < x) ? y : x; }
+template <class real> __device__ __forceinline__ real cmax(real x, real y) { return (x < y) ? y : x; }
+template <class real> __device__ __forceinline__ real csign(real x) {
+  return x > (real)0 ? (real)1 : (x < (real)0 ? (real)-1 : (x != x ? (real)0 : x));
+}
+
+// ------------------------------------------------------------------ EOS
+// Table lookup of eos_table.h:39-62: row/col from the energy density, two
+// nearest texels (the second wraps to the next row), clamp-to-edge, lerp.
+template <class real>
+__device__ __forceinline__ real eos_comp(const Params& p, real eps, int c) {
+  real ed_per_row = p.eos_step * p.eos_ncol;
+  int row = (int)(eps / ed_per_row);
+  int col = (int)((eps - p.eos_start - row * ed_per_row) / p.eos_step);
+  real eps_low = p.eos_start + row * ed_per_row + col * p.eos_step;
+  int col2 = col + 1, row2 = row;
+  if (col2 == p.eos_ncol) {
+    row2 += 1;
+    col2 = 0;
+  }
+  int c0 = min(max(col, 0), p.eos_ncol - 1), r0 = min(max(row, 0), p.eos_nrow - 1);
+  int c1 = min(max(col2, 0), p.eos_ncol - 1), r1 = min(max(row2, 0), p.eos_nrow - 1);
+  float lo = __ldg(p.eos + 4 * ((long long)r0 * p.eos_ncol + c0) + c);
+  float hi = __ldg(p.eos + 4 * ((long long)r1 * p.eos_ncol + c1) + c);
+  real r = (eps - eps_low) / p.eos_step;
+  return (real)(1.0f - r) * (real)lo + r * (real)hi;
+}
+template <class real> __device__ __forceinline__ bool eos_in_table(const Params& p, real eps) {
+  return eps < p.eos_start + p.eos_num * p.eos_step;
+}
+// P(e): eos_table.h:65-71
+template <class real> __device__ __forceinline__ real eosP(const Params& p, real eps) {
+  if (eos_in_table(p, eps)) return eos_comp(p, eps, 1);
+  return 0.3327f * eps - 0.3223f * pow(eps, (real)0.4585f) - 0.003906f * eps * exp(-0.05697f * eps);
+}
+// CS2(e): eos_table.h:94-100
+template <class real> __device__ __forceinline__ real eosCS2(const Params& p, real eps) {
+  if (eos_in_table(p, eps)) return eos_comp(p, eps, 0);
+  return 0.333333333f;
+}
+
+// ---------------------------------------------------------------- helper.h
+template <class real> __device__ __forceinline__ real gamma3(real vx, real vy, real vz) {  // helper.h:46-48
+  return 1.0f / sqrt(cmax<real>(1.0f - vx * vx - vy * vy - vz * vz, Acu<real>::v));
+}
+template <class real> __device__ __forceinline__ real minmod(real x, real y) {  // helper.h:74-77
+  real res = cmin<real>(fabs(x), fabs(y));
+  return res * (csign(x) + csign(y)) * 0.5f;
+}
+// slope limiter of kt1d (helper.h:213-217): minmod(0.5(R-L), minmod(TH(R-C), TH(C-L)))
+template <class real> __device__ __forceinline__ real slope(real L, real C, real R) {
+  const real TH = CLV_THETA;
+  return minmod<real>(0.5f * (R - L), minmod<real>(TH * (R - C), TH * (C - L)));
+}
+// velocity-gradient limiter of kernel_IS.cl:134-137 (argument order differs)
+template <class real> __device__ __forceinline__ real grad_limit(real L, real C, real R) {
+  const real TH = CLV_THETA;
+  return minmod<real>(0.5f * (R - L), minmod<real>(TH * (C - L), TH * (R - C)));
+}
+
+// helper.h:94-105, with edv = 0.5*(ev_L + ev_R)
+template <class real>
+__device__ __forceinline__ real max_speed(const Params& p, real e, real vx, real vy, real vz, real vk) {
+  real ut = gamma3<real>(vx, vy, vz);
+  real uk = ut * vk;
+  real ut2 = ut * ut;
+  real uk2 = uk * uk;
+  real cs2 = eosCS2<real>(p, e);
+  real lam = (fabs(ut * uk * (1.0f - cs2)) + sqrt((ut2 - uk2 - (ut2 - uk2 - 1.0f) * cs2) * cs2)) /
+             (ut2 - (ut2 - 1.0f) * cs2);
+  return cmax<real>(lam, 1.0f);
+}
+
+// helper.h:128-167; returns the energy density
+template <class real> __device__ __forceinline__ real root_newton(const Params& p, real T00, real M) {
+  real vl = 0.0f;
+  real vh = 1.0f;
+  real dpe = 1.0f / 3.0f;
+  real v = 0.5f * (vl + vh);
+  real ed = T00 - M * v;
+  real pr = eosP<real>(p, ed);
+  real f = (T00 + pr) * v - M;
+  real df = (T00 + pr) - M * v * dpe;
+  real dvold = vh - vl;
+  real dv = dvold;
+  int i = 0;
+  while (true) {
+    if ((f + df * (vh - v)) * (f + df * (vl - v)) > 0.0f || fabs(2.f * f) > fabs(dvold * df)) {
+      dvold = dv;
+      dv = 0.5f * (vh - vl);
+      v = vl + dv;
+    } else {
+      dvold = dv;
+      dv = f / df;
+      v -= dv;
+    }
+    i++;
+    if (fabs(dv) < 0.00001f || i > 100) break;
+    ed = T00 - M * v;
+    pr = eosP<real>(p, ed);
+    f = (T00 + pr) * v - M;
+    df = (T00 + pr) - M * v * dpe;
+    if (f > 0.0f) {
+      vh = v;
+    } else {
+      vl = v;
+    }
+  }
+  return T00 - M * v;
+}
+
+// helper.h:23-26
+template <class real> __device__ __forceinline__ real etaos(const Params& p, real T) {
+  return (T < p.ETAOS_XMIN) ? (p.ETAOS_LEFT_SLOP * (T - p.ETAOS_XMIN) + p.ETAOS_YMIN)
+                            : (p.ETAOS_RIGHT_SLOP * (T - p.ETAOS_XMIN) + p.ETAOS_YMIN);
+}
+
+// kernel_IS.cl:3-6 and helper.h:59-63 as scalar lookups
+template <class real> __device__ __forceinline__ real gmn(int a, int b) {
+  return a != b ? (real)0.0f : (a == 0 ? (real)1.0f : (real)-1.0f);
+}
+__host__ __device__ constexpr int pidx(int i, int j) {  // helper.h:31
+  return (i < j) ? ((7 * i + 2 * j - i * i) / 2) : ((7 * j + 2 * i - j * j) / 2);
+}
+
+// OpenCL dot(): left to right, separate multiply and add
+template <class real> __device__ __forceinline__ real dot4(const real a[4], const real b[4]) {
+  real r = a[0] * b[0];
+  r = r + a[1] * b[1];
+  r = r + a[2] * b[2];
+  r = r + a[3] * b[3];
+  return r;
+}
+
+// Delta^{k c} = g^{k c} - u^k u^c (kernel_IS.cl:333-334)
+template <class real> __device__ __forceinline__ void delta4(const real u[4], real D[4][4]) {
+#pragma unroll
+  for (int k = 0; k < 4; k++)
+#pragma unroll
+    for (int c = 0; c < 4; c++) D[k][c] = gmn<real>(k, c) - u[k] * u[c];
+}
+// pi_{mu}^{lam} as a lowered 4-vector (kernel_IS.cl:328-329)
+template <class real> __device__ __forceinline__ void pi_low(int lam, const real pimn[10], real A[4]) {
+  A[0] = pimn[pidx(0, lam)];
+  A[1] = -pimn[pidx(1, lam)];
+  A[2] = -pimn[pidx(2, lam)];
+  A[3] = -pimn[pidx(3, lam)];
+}
+// omega_{a}^{lam} (kernel_IS.cl:406-417)
+template <class real> __device__ __forceinline__ void omega_col(int lam, const real om[6], real B[4]) {
+  if (lam == 0) { B[0] = 0.0f; B[1] = om[0]; B[2] = om[1]; B[3] = om[2]; }
+  else if (lam == 1) { B[0] = om[0]; B[1] = 0.0f; B[2] = om[3]; B[3] = om[4]; }
+  else if (lam == 2) { B[0] = om[1]; B[1] = -om[3]; B[2] = 0.0f; B[3] = om[5]; }
+  else { B[0] = om[2]; B[1] = -om[4]; B[2] = -om[5]; B[3] = 0.0f; }
+}
+// pi^{<mu}_{lam} pi^{nu>lam} (kernel_IS.cl:324-346), GUBSER_VISC_TEST only
+template <class real> __device__ real pipi(int lam, int mu, int nu, const real pimn[10], const real u[4]) {
+  real A[4], D[4][4], temp[4];
+  pi_low<real>(lam, pimn, A);
+  delta4<real>(u, D);
+  real firstTerm = dot4<real>(D[mu], A) * dot4<real>(D[nu], A);
+#pragma unroll
+  for (int q = 0; q < 4; q++) temp[q] = dot4<real>(D[q], A);
+  real secondTerm = -1.0f / 3.0f * (gmn<real>(mu, nu) - u[mu] * u[nu]) * dot4<real>(temp, A);
+  return firstTerm + secondTerm;
+}
+// Omega^{mu nu} (kernel_IS.cl:355-377)
+template <class real> __device__ real omega_munu(int mu, int nu, const real om[6], const real u[4]) {
+  real ua[4] = {u[0], -u[1], -u[2], -u[3]};
+  real D[4][4], A[4][4], temp[4];
+#pragma unroll
+  for (int k = 0; k < 4; k++)
+#pragma unroll
+    for (int c = 0; c < 4; c++) D[k][c] = (k == c ? (real)1.0f : (real)0.0f) - u[k] * ua[c];
+  A[0][0] = 0.0f;   A[0][1] = om[0];  A[0][2] = om[1];  A[0][3] = om[2];
+  A[1][0] = -om[0]; A[1][1] = 0.0f;   A[1][2] = om[3];  A[1][3] = om[4];
+  A[2][0] = -om[1]; A[2][1] = -om[3]; A[2][2] = 0.0f;   A[2][3] = om[5];
+  A[3][0] = -om[2]; A[3][1] = -om[4]; A[3][2] = -om[5]; A[3][3] = 0.0f;
+#pragma unroll
+  for (int q = 0; q < 4; q++) temp[q] = dot4<real>(D[nu], A[q]);
+  return 0.5f * dot4<real>(D[mu], temp);
+}
+// the six Omega components from the velocity gradients (kernel_IS.cl:637-651)
+template <class real>
+__device__ void omega_tensor(const real udt[4], const real g[3][4], const real u[4], real Om[6]) {
+  real om[6];
+  om[0] = udt[1] - g[0][0];
+  om[1] = udt[2] - g[1][0];
+  om[2] = udt[3] - g[2][0];
+  om[3] = g[0][2] - g[1][1];
+  om[4] = g[0][3] - g[2][1];
+  om[5] = g[1][3] - g[2][2];
+  Om[0] = omega_munu<real>(0, 1, om, u);
+  Om[1] = omega_munu<real>(0, 2, om, u);
+  Om[2] = omega_munu<real>(0, 3, om, u);
+  Om[3] = omega_munu<real>(1, 2, om, u);
+  Om[4] = omega_munu<real>(1, 3, om, u);
+  Om[5] = omega_munu<real>(2, 3, om, u);
+}
+// pi^{<mu}_{lam} omega^{nu>lam} (kernel_IS.cl:390-437)
+template <class real>
+__device__ real pi_omega(int lam, int mu, int nu, const real pimn[10], const real Om[6], const real u[4]) {
+  real A[4], B[4], D[4][4], temp[4];
+  pi_low<real>(lam, pimn, A);
+  omega_col<real>(lam, Om, B);
+  delta4<real>(u, D);
+  real firstTerm = 0.5f * (dot4<real>(D[mu], A) * dot4<real>(D[nu], B) + dot4<real>(D[mu], B) * dot4<real>(D[nu], A));
+#pragma unroll
+  for (int q = 0; q < 4; q++) temp[q] = dot4<real>(D[q], A);
+  real secondTerm = -1.0f / 3.0f * (gmn<real>(mu, nu) - u[mu] * u[nu]) * dot4<real>(temp, B);
+  return firstTerm + secondTerm;
+}
+// omega^{<mu}_{lam} omega^{nu>lam} (kernel_IS.cl:449-487)
+template <class real> __device__ real omega_omega(int lam, int mu, int nu, const real Om[6], const real u[4]) {
+  real B[4], D[4][4], temp[4];
+  omega_col<real>(lam, Om, B);
+  delta4<real>(u, D);
+  real firstTerm = dot4<real>(D[mu], B) * dot4<real>(D[nu], B);
+#pragma unroll
+  for (int q = 0; q < 4; q++) temp[q] = dot4<real>(D[q], B);
+  real secondTerm = -1.0f / 3.0f * (gmn<real>(mu, nu) - u[mu] * u[nu]) * dot4<real>(temp, B);
+  return firstTerm + secondTerm;
+}
+
+// ordered-integer keys for an atomic max over floating values
+__device__ __forceinline__ unsigned int fkey(float f) {
+  unsigned int b = __float_as_uint(f);
+  return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+__device__ __forceinline__ unsigned long long fkey(double f) {
+  unsigned long long b = (unsigned long long)__double_as_longlong(f);
+  return (b & 0x8000000000000000ull) ? ~b : (b | 0x8000000000000000ull);
+}
+template <class real> struct KeyT;
+template <> struct KeyT<float> { typedef unsigned int type; };
+template <> struct KeyT<double> { typedef unsigned long long type; };
+
+}  // namespace clv

@@ -1,0 +1,574 @@
+// Fused Runge-Kutta stage kernels of the CLVisc hydro step.
+//
+// One thread owns one cell and produces, in a single pass over HBM, what the
+// reference computes with ten separate launches per stage
+// (visc.py:232-314): the Christoffel sources, the three directional
+// Kurganov-Tadmor flux differences of T^{tau mu} (kernel_visc.cl:68-318) and
+// of u0*pi^{mu nu} (kernel_IS.cl:74-318) with the minmod-limited velocity
+// gradients, the implicit Israel-Stewart update (kernel_IS.cl:501-709) and
+// the T^{tau mu} -> (e, v) root find (kernel_visc.cl:322-393). The ideal
+// variant covers kernel_ideal.cl.
+//
+// Fields are structure-of-arrays planes of Params::ld elements in the
+// reference's cell order I = i*NY*NZ + j*NZ + k. A face flux is evaluated from
+// the two cells that share the face, so the value at face i+1/2 is the same
+// for cells i and i+1, as in the reference.
+#pragma once
+#include "clv_device.cuh"
+
+namespace clv {
+
+template <class real> struct ViscBuffers {
+  const real* ev_st;   // 4 planes: d_ev[step], stencil input
+  const real* pi_st;   // 10 planes: d_pi[step], stencil input
+  const real* ev1;     // 4 planes: d_ev[1]
+  const real* ev2e;    // plane 0 of d_ev[2] (read at stage 1)
+  const real* pi1;     // 10 planes: d_pi[1], start point of the pi update
+  const real* pin;     // 10 planes: pi at the start of the step (update_ev base)
+  const real* pi2in;   // 10 planes: new pi, read when the pi update is not fused
+  real* evnew;         // 4 planes
+  real* pinew;         // 10 planes
+  real* src;           // 14 planes: KT sources 0..3, IS sources 4..13
+  real* udiff;         // 4 planes
+  uint8_t* goodcell;   // 1 byte per cell
+  typename KeyT<real>::type* edmax_key;  // optional max of evnew energy density
+  int write_src;       // keep the accumulated sources for the next stage
+  int write_udiff;     // udiff = u(evnew) - u(ev1) (fused second stage)
+};
+
+template <class real> struct IdealBuffers {
+  const real* ev_st;  // d_ev[step]
+  const real* ev1;    // d_ev[1]
+  real* evnew;        // d_ev[3-step]
+  real* src;          // 4 planes
+  typename KeyT<real>::type* edmax_key;
+  int write_src;
+};
+
+// neighbour offsets along one axis, clamped at the edges: the reference's
+// two ghost cells repeat the edge cell (kernel_ideal.cl:166-172)
+struct Stencil {
+  long long off[5];
+};
+__device__ __forceinline__ Stencil make_stencil(int q, int L, long long stride) {
+  Stencil s;
+#pragma unroll
+  for (int d = -2; d <= 2; d++) {
+    int qq = min(max(q + d, 0), L - 1);
+    s.off[d + 2] = (long long)(qq - q) * stride;
+  }
+  return s;
+}
+
+// --------------------------------------------------------------- viscous
+template <class real, bool DO_IS, bool DO_KT>
+__global__ void __launch_bounds__(128) visc_stage_kernel(Params p, ViscBuffers<real> b, int step, real tau) {
+  const long long N = (long long)p.nx * p.ny * p.nz;
+  const long long I = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (I >= N) return;
+  const long long ld = p.ld;
+  const int k = (int)(I % p.nz);
+  const long long t = I / p.nz;
+  const int j = (int)(t % p.ny);
+  const int i = (int)(t / p.ny);
+  const real acu = Acu<real>::v;
+
+  // centre cell of the stage input
+  real e0[4];
+#pragma unroll
+  for (int c = 0; c < 4; c++) e0[c] = b.ev_st[c * ld + I];
+  real pc[10];
+#pragma unroll
+  for (int m = 0; m < 10; m++) pc[m] = b.pi_st[m * ld + I];
+  // pi at the start of the step: read before this thread's pi_new store,
+  // which may alias it (in-place second stage)
+  real pin[4];
+#pragma unroll
+  for (int c = 0; c < 4; c++) pin[c] = DO_KT ? b.pin[c * ld + I] : (real)0.0f;
+
+  real S4[4], S10[10];
+  if (step == 1) {
+#pragma unroll
+    for (int c = 0; c < 4; c++) S4[c] = 0.0f;
+#pragma unroll
+    for (int m = 0; m < 10; m++) S10[m] = 0.0f;
+  } else {
+#pragma unroll
+    for (int c = 0; c < 4; c++) S4[c] = DO_KT ? b.src[c * ld + I] : (real)0.0f;
+#pragma unroll
+    for (int m = 0; m < 10; m++) S10[m] = DO_IS ? b.src[(4 + m) * ld + I] : (real)0.0f;
+  }
+
+  // Christoffel terms
+  if (DO_IS) {  // kernel_IS.cl:56-65
+    real uz = e0[3] * gamma3<real>(e0[1], e0[2], e0[3]);
+    S10[0] -= 2.0f * uz * pc[pidx(0, 3)] / tau;
+    S10[1] -= uz * pc[pidx(1, 3)] / tau;
+    S10[2] -= uz * pc[pidx(2, 3)] / tau;
+    S10[3] -= uz * (pc[pidx(0, 0)] + pc[pidx(3, 3)]) / tau;
+    S10[6] -= uz * pc[pidx(0, 1)] / tau;
+    S10[8] -= uz * pc[pidx(0, 2)] / tau;
+    S10[9] -= 2.0f * uz * pc[pidx(0, 3)] / tau;
+  }
+  if (DO_KT) {  // kernel_visc.cl:24-50
+    real ed = e0[0], vx = e0[1], vy = e0[2], vz = e0[3];
+    real u0 = gamma3<real>(vx, vy, vz);
+    real bulkpi = 0.0f;
+    real pressure = eosP<real>(p, ed) + bulkpi;
+    real Tzz_tilde = (ed + pressure) * u0 * u0 * vz * vz + pressure + pc[pidx(3, 3)];
+    real Ttz_tilde = (ed + pressure) * u0 * u0 * vz + pc[pidx(0, 3)];
+    S4[0] = S4[0] - Tzz_tilde;
+    S4[1] = S4[1] - (real)0.0f;
+    S4[2] = S4[2] - (real)0.0f;
+    S4[3] = S4[3] - Ttz_tilde;
+    if (p.flags & FLAG_RIEMANN) {
+      real Ttt_tilde = (ed + pressure) * u0 * u0 - pressure;
+      real Ttx_tilde = (ed + pressure) * u0 * u0 * vx;
+      real Tty_tilde = (ed + pressure) * u0 * u0 * vy;
+      S4[0] = S4[0] + (Tzz_tilde + Ttt_tilde);
+      S4[1] = S4[1] + Ttx_tilde;
+      S4[2] = S4[2] + Tty_tilde;
+      S4[3] = S4[3] + 3.0f * Ttz_tilde;
+    }
+  }
+
+  real grad[3][4];  // d_udx, d_udy, d_udz of kernel_IS.cl
+
+#pragma unroll 1
+  for (int a = 0; a < 3; a++) {
+    const int q = a == 0 ? i : (a == 1 ? j : k);
+    const int L = a == 0 ? p.nx : (a == 1 ? p.ny : p.nz);
+    const long long stride = a == 0 ? (long long)p.ny * p.nz : (a == 1 ? (long long)p.nz : 1ll);
+    const Stencil st = make_stencil(q, L, stride);
+    const real D = a == 0 ? (real)p.DX : (a == 1 ? (real)p.DY : tau * p.DZ);
+
+    real E[5][4];
+#pragma unroll
+    for (int d = 0; d < 5; d++)
+#pragma unroll
+      for (int c = 0; c < 4; c++) E[d][c] = (d == 2) ? e0[c] : b.ev_st[c * ld + I + st.off[d]];
+    real u0[5];
+#pragma unroll
+    for (int d = 0; d < 5; d++) u0[d] = gamma3<real>(E[d][1], E[d][2], E[d][3]);
+
+    // face (i-1/2) uses cells 1,2 and face (i+1/2) cells 2,3 of the stencil
+    real vh[2], lam[2];
+#pragma unroll
+    for (int f = 0; f < 2; f++) {
+      const int l = 1 + f, r = 2 + f;
+      real h[4];
+#pragma unroll
+      for (int c = 0; c < 4; c++) h[c] = 0.5f * (E[l][c] + E[r][c]);
+      vh[f] = h[a + 1];
+      lam[f] = max_speed<real>(p, h[0], h[1], h[2], h[3], vh[f]);
+    }
+
+    if (DO_KT) {  // kt1d_visc, kernel_visc.cl:68-127
+      real pr[5], Q[5][4];
+#pragma unroll
+      for (int d = 0; d < 5; d++) {
+        const long long J = I + st.off[d];
+        pr[d] = eosP<real>(p, E[d][0]);
+        real A = (E[d][0] + pr[d]) * u0[d];
+        real u4[4] = {(real)1.0f * u0[d], E[d][1] * u0[d], E[d][2] * u0[d], E[d][3] * u0[d]};
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+          real g0 = c == 0 ? (real)1.0f : (real)0.0f;
+          real T0m = A * u4[c] - g0 * pr[d];
+          real pim0 = (d == 2) ? pc[c] : b.pi_st[c * ld + J];
+          Q[d][c] = tau * (T0m + pim0);
+        }
+      }
+      real F[2][4];
+#pragma unroll
+      for (int f = 0; f < 2; f++) {
+        const int l = 1 + f, r = 2 + f;
+        const long long Jl = I + st.off[l], Jr = I + st.off[r];
+        real pr_half = 0.5f * (pr[l] + pr[r]);
+        real pt = pr_half * tau;
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+          real DAl = slope<real>(Q[l - 1][c], Q[l][c], Q[l + 1][c]);
+          real DAr = slope<real>(Q[r - 1][c], Q[r][c], Q[r + 1][c]);
+          real AL = Q[l][c] + 0.5f * DAl;
+          real AR = Q[r][c] - 0.5f * DAr;
+          real p0l = (l == 2) ? pc[c] : b.pi_st[c * ld + Jl];
+          real p0r = (r == 2) ? pc[c] : b.pi_st[c * ld + Jr];
+          const int mi = pidx(a + 1, c);
+          real pil = (l == 2) ? pc[mi] : b.pi_st[mi * ld + Jl];
+          real pir = (r == 2) ? pc[mi] : b.pi_st[mi * ld + Jr];
+          real pim0_half = 0.5f * (p0l + p0r);
+          real pimi_half = 0.5f * (pil + pir);
+          real g0 = c == 0 ? (real)1.0f : (real)0.0f;
+          real ga = c == a + 1 ? (real)-1.0f : (real)0.0f;
+          real Jp = (AR + pt * g0 - tau * pim0_half) * vh[f] - pt * ga + tau * pimi_half;
+          real Jm = (AL + pt * g0 - tau * pim0_half) * vh[f] - pt * ga + tau * pimi_half;
+          F[f][c] = 0.5f * (Jp + Jm) - 0.5f * lam[f] * (AR - AL);
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < 4; c++) {
+        real src = F[1][c];
+        src -= F[0][c];
+        S4[c] = S4[c] - src / D;
+      }
+    }
+
+    if (DO_IS) {
+      // velocity gradient, kernel_IS.cl:134-137 / 217-220 / 299-304
+      real um[3][4];
+#pragma unroll
+      for (int d = 0; d < 3; d++) {
+        um[d][0] = u0[d + 1] * 1.0f;
+        um[d][1] = u0[d + 1] * E[d + 1][1];
+        um[d][2] = u0[d + 1] * E[d + 1][2];
+        um[d][3] = u0[d + 1] * E[d + 1][3];
+      }
+      const real Dg = a == 2 ? (real)(p.DZ * tau) : D;
+#pragma unroll
+      for (int c = 0; c < 4; c++) grad[a][c] = grad_limit<real>(um[0][c], um[1][c], um[2][c]) / Dg;
+      if (a == 2) {
+        grad[2][0] = grad[2][0] + E[2][3] * u0[2] / tau;
+        grad[2][1] = grad[2][1] + (real)0.0f * u0[2] / tau;
+        grad[2][2] = grad[2][2] + (real)0.0f * u0[2] / tau;
+        grad[2][3] = grad[2][3] + (real)1.0f * u0[2] / tau;
+      }
+      // KT flux of u0*pi^{mn}, kt1d_real (helper.h:249-285)
+#pragma unroll 2
+      for (int m = 0; m < 10; m++) {
+        real U[5];
+#pragma unroll
+        for (int d = 0; d < 5; d++) U[d] = u0[d] * ((d == 2) ? pc[m] : b.pi_st[m * ld + I + st.off[d]]);
+        real Fm[2];
+#pragma unroll
+        for (int f = 0; f < 2; f++) {
+          const int l = 1 + f, r = 2 + f;
+          real DAl = slope<real>(U[l - 1], U[l], U[l + 1]);
+          real DAr = slope<real>(U[r - 1], U[r], U[r + 1]);
+          real AL = U[l] + 0.5f * DAl;
+          real AR = U[r] - 0.5f * DAr;
+          real Jp = AR * vh[f];
+          real Jm = AL * vh[f];
+          Fm[f] = 0.5f * (Jp + Jm) - 0.5f * lam[f] * (AR - AL);
+        }
+        real src = Fm[1];
+        src -= Fm[0];
+        S10[m] = S10[m] - src / D;
+      }
+    }
+  }
+
+  // ------------------------------------------------ pi update (update_pimn)
+  real pinew[10];
+  if (DO_IS) {
+    real e1[4];
+#pragma unroll
+    for (int c = 0; c < 4; c++) e1[c] = b.ev1[c * ld + I];
+    real g1 = gamma3<real>(e1[1], e1[2], e1[3]);
+    real u_old[4] = {g1 * 1.0f, g1 * e1[1], g1 * e1[2], g1 * e1[3]};
+    real u_new[4], udt[4];
+    real e2s0;
+    if (step == 1) {
+#pragma unroll
+      for (int c = 0; c < 4; c++) {
+        real ud = b.udiff[c * ld + I];
+        udt[c] = ud / (real)p.DT;
+        u_new[c] = u_old[c] + ud;
+      }
+      e2s0 = b.ev2e[I];
+    } else {
+      real g2 = gamma3<real>(e0[1], e0[2], e0[3]);
+      u_new[0] = g2 * 1.0f;
+      u_new[1] = g2 * e0[1];
+      u_new[2] = g2 * e0[2];
+      u_new[3] = g2 * e0[3];
+#pragma unroll
+      for (int c = 0; c < 4; c++) udt[c] = (u_new[c] - u_old[c]) / (real)p.DT;
+      e2s0 = e0[0];
+    }
+    real da[4][4];
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+      da[c][0] = udt[c];
+      da[c][1] = grad[0][c];
+      da[c][2] = grad[1][c];
+      da[c][3] = grad[2][c];
+    }
+    real u[4], DU[4];
+#pragma unroll
+    for (int c = 0; c < 4; c++) u[c] = (step == 1) ? u_old[c] : u_new[c];
+#pragma unroll
+    for (int c = 0; c < 4; c++) DU[c] = dot4<real>(u, da[c]);
+    real ed_step = (step == 1) ? e1[0] : e2s0;
+    real theta = udt[0] + grad[0][1] + grad[1][2] + grad[2][3];
+    real temperature = eos_comp<real>(p, ed_step, 2);
+    real sdens = eos_comp<real>(p, ed_step, 3);
+    real local_etaos = etaos<real>(p, temperature);
+    real etav = local_etaos * sdens * CLV_HBARC;
+    real one_over_taupi = temperature / (3.0f * cmax<real>(acu, local_etaos) * CLV_HBARC);
+    real coef_pipi = 0.0f;
+    if (p.flags & FLAG_GUBSER_VISC) {  // kernel_IS.cl:581-590
+      real ETAOS = p.ETAOS_YMIN;
+      real etavH = ETAOS * 4.0f / 3.0f;
+      real taupiH = p.LAM1 * p.LAM1 * etavH / 3.0f;
+      one_over_taupi = 1.0f / (taupiH * pow(ed_step, (real)-0.25f));
+      coef_pipi = p.LAM1 / ed_step;
+      etav = ETAOS * 4.0f / 3.0f * pow(ed_step, (real)0.75f);
+    }
+    real Omega[6] = {0, 0, 0, 0, 0, 0};
+    if (p.flags & (FLAG_PIMN_OMEGA | FLAG_OMEGA_OMEGA)) omega_tensor<real>(udt, grad, u, Omega);
+
+    real max_pimn_abs = 0.0f;
+#pragma unroll
+    for (int mu = 0; mu < 4; mu++)
+#pragma unroll
+      for (int nu = mu; nu < 4; nu++) {
+        real gmu[4] = {gmn<real>(mu, 0), gmn<real>(mu, 1), gmn<real>(mu, 2), gmn<real>(mu, 3)};
+        real gnu[4] = {gmn<real>(nu, 0), gmn<real>(nu, 1), gmn<real>(nu, 2), gmn<real>(nu, 3)};
+        real sigma = dot4<real>(gmu, da[nu]) + dot4<real>(gnu, da[mu]) - (u[mu] * DU[nu] + u[nu] * DU[mu]) -
+                     2.0f / 3.0f * (gmn<real>(mu, nu) - u[mu] * u[nu]) * theta;
+        const int mn = pidx(mu, nu);
+        if (u[0] > 10000.0f) sigma = 0.0f;
+        real piNS = etav * sigma;
+        real pi_old = b.pi1[mn * ld + I] * u_old[0];
+        real src = -pc[mn] * theta / 3.0f - pc[mn] * u[0] / tau;
+        src -= (u[mu] * pc[pidx(nu, 0)] + u[nu] * pc[pidx(mu, 0)]) * DU[0] * gmn<real>(0, 0);
+        src -= (u[mu] * pc[pidx(nu, 1)] + u[nu] * pc[pidx(mu, 1)]) * DU[1] * gmn<real>(1, 1);
+        src -= (u[mu] * pc[pidx(nu, 2)] + u[nu] * pc[pidx(mu, 2)]) * DU[2] * gmn<real>(2, 2);
+        src -= (u[mu] * pc[pidx(nu, 3)] + u[nu] * pc[pidx(mu, 3)]) * DU[3] * gmn<real>(3, 3);
+        if (p.flags & FLAG_GUBSER_VISC)
+          src -= one_over_taupi * coef_pipi *
+                 (pipi<real>(0, mu, nu, pc, u) - pipi<real>(1, mu, nu, pc, u) - pipi<real>(2, mu, nu, pc, u) -
+                  pipi<real>(3, mu, nu, pc, u));
+        if (p.flags & FLAG_PIMN_OMEGA)
+          src += 2.0f * (pi_omega<real>(0, mu, nu, pc, Omega, u) - pi_omega<real>(1, mu, nu, pc, Omega, u) -
+                         pi_omega<real>(2, mu, nu, pc, Omega, u) - pi_omega<real>(3, mu, nu, pc, Omega, u));
+        if (p.flags & FLAG_OMEGA_OMEGA)
+          src -= 1.0f * one_over_taupi *
+                 (omega_omega<real>(0, mu, nu, Omega, u) - omega_omega<real>(1, mu, nu, Omega, u) -
+                  omega_omega<real>(2, mu, nu, Omega, u) - omega_omega<real>(3, mu, nu, Omega, u));
+        S10[mn] += src;
+        pi_old = (pi_old + S10[mn] * p.DT / step + p.DT * one_over_taupi * piNS) / (u_new[0] + p.DT * one_over_taupi);
+        if (fabs(pi_old) > max_pimn_abs) max_pimn_abs = fabs(pi_old);
+        pinew[mn] = pi_old;
+      }
+    real pre = eosP<real>(p, e2s0);
+    real T00 = (e2s0 + pre) * u_new[0] * u_new[0] - pre;
+    uint8_t good = 1;
+    if (max_pimn_abs > T00) {
+#pragma unroll
+      for (int m = 0; m < 10; m++) pinew[m] = 0.0f;
+      good = 0;
+    }
+#pragma unroll
+    for (int m = 0; m < 10; m++) b.pinew[m * ld + I] = pinew[m];
+    b.goodcell[I] = good;
+  }
+
+  // ------------------------------------------- T^{tau mu} update (update_ev)
+  if (DO_KT) {
+    real e1[4];
+#pragma unroll
+    for (int c = 0; c < 4; c++) e1[c] = b.ev1[c * ld + I];
+    real ed = e1[0], vx = e1[1], vy = e1[2], vz = e1[3];
+    real pressure = eosP<real>(p, ed);
+    real u0 = gamma3<real>(vx, vy, vz);
+    real umu[4] = {u0 * 1.0f, u0 * vx, u0 * vy, u0 * vz};
+    real old_time = tau - (step - 1) * p.DT;
+    real T0m[4];
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+      real g0 = c == 0 ? (real)1.0f : (real)0.0f;
+      T0m[c] = ((ed + pressure) * u0 * umu[c] - pressure * g0 + pin[c]) * old_time;
+    }
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+      real pim2 = DO_IS ? pinew[c] : b.pi2in[c * ld + I];
+      T0m[c] = T0m[c] + S4[c] * p.DT / step - pim2 * tau;
+    }
+    real T00 = cmax<real>(acu, T0m[0]) / tau;
+    real T01 = (fabs(T0m[1]) < acu) ? (real)0.0f : T0m[1] / tau;
+    real T02 = (fabs(T0m[2]) < acu) ? (real)0.0f : T0m[2] / tau;
+    real T03 = (fabs(T0m[3]) < acu) ? (real)0.0f : T0m[3] / tau;
+    real M = sqrt(T01 * T01 + T02 * T02 + T03 * T03);
+    real SCALE_COEF = 0.999f;
+    if (M > T00) {
+      T01 *= SCALE_COEF * T00 / M;
+      T02 *= SCALE_COEF * T00 / M;
+      T03 *= SCALE_COEF * T00 / M;
+      M = SCALE_COEF * T00;
+    }
+    real ed_find = root_newton<real>(p, T00, M);
+    if (ed_find < acu) {
+      T01 = 0.0f;
+      T02 = 0.0f;
+      T03 = 0.0f;
+    }
+    ed_find = cmax<real>(0.0f, ed_find);
+    real pr = eosP<real>(p, ed_find);
+    real epv = cmax<real>(acu, T00 + pr);
+    real en[4] = {ed_find, T01 / epv, T02 / epv, T03 / epv};
+#pragma unroll
+    for (int c = 0; c < 4; c++) b.evnew[c * ld + I] = en[c];
+    if (b.write_udiff) {  // get_udiff, kernel_IS.cl:714-724
+      real gn = gamma3<real>(en[1], en[2], en[3]);
+      real go = gamma3<real>(e1[1], e1[2], e1[3]);
+      b.udiff[0 * ld + I] = gn * 1.0f - go * 1.0f;
+      b.udiff[1 * ld + I] = gn * en[1] - go * e1[1];
+      b.udiff[2 * ld + I] = gn * en[2] - go * e1[2];
+      b.udiff[3 * ld + I] = gn * en[3] - go * e1[3];
+    }
+    if (b.edmax_key && en[0] == en[0]) atomicMax(b.edmax_key, fkey(en[0]));
+  }
+
+  if (b.write_src) {
+    if (DO_KT)
+#pragma unroll
+      for (int c = 0; c < 4; c++) b.src[c * ld + I] = S4[c];
+    if (DO_IS)
+#pragma unroll
+      for (int m = 0; m < 10; m++) b.src[(4 + m) * ld + I] = S10[m];
+  }
+}
+
+// ----------------------------------------------------------------- ideal
+template <class real>
+__global__ void __launch_bounds__(128) ideal_stage_kernel(Params p, IdealBuffers<real> b, int step, real tau) {
+  const long long N = (long long)p.nx * p.ny * p.nz;
+  const long long I = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (I >= N) return;
+  const long long ld = p.ld;
+  const int k = (int)(I % p.nz);
+  const long long t = I / p.nz;
+  const int j = (int)(t % p.ny);
+  const int i = (int)(t / p.ny);
+  const real acu = Acu<real>::v;
+  const bool riemann = (p.flags & FLAG_RIEMANN) != 0;
+
+  real e0[4];
+#pragma unroll
+  for (int c = 0; c < 4; c++) e0[c] = b.ev_st[c * ld + I];
+  real S[4];
+#pragma unroll
+  for (int c = 0; c < 4; c++) S[c] = (step == 1) ? (real)0.0f : b.src[c * ld + I];
+
+  {  // kernel_ideal.cl:125-143
+    real ed = e0[0], vz = e0[3];
+    real pressure = eosP<real>(p, ed);
+    real u0 = gamma3<real>(e0[1], e0[2], vz);
+    real Tzz_tilde = (ed + pressure) * u0 * u0 * vz * vz + pressure;
+    real Ttz_tilde = (ed + pressure) * u0 * u0 * vz;
+    if (!riemann) {
+      S[0] = S[0] - Tzz_tilde;
+      S[1] = S[1] - (real)0.0f;
+      S[2] = S[2] - (real)0.0f;
+      S[3] = S[3] - Ttz_tilde;
+    }
+  }
+
+#pragma unroll 1
+  for (int a = 0; a < 3; a++) {
+    const int q = a == 0 ? i : (a == 1 ? j : k);
+    const int L = a == 0 ? p.nx : (a == 1 ? p.ny : p.nz);
+    const long long stride = a == 0 ? (long long)p.ny * p.nz : (a == 1 ? (long long)p.nz : 1ll);
+    const Stencil st = make_stencil(q, L, stride);
+    real E[5][4], pr[5], T[5][4];
+#pragma unroll
+    for (int d = 0; d < 5; d++) {
+#pragma unroll
+      for (int c = 0; c < 4; c++) E[d][c] = (d == 2) ? e0[c] : b.ev_st[c * ld + I + st.off[d]];
+      pr[d] = eosP<real>(p, E[d][0]);
+      real u0 = gamma3<real>(E[d][1], E[d][2], E[d][3]);
+      real A = (E[d][0] + pr[d]) * u0;
+      real u4[4] = {(real)1.0f * u0, E[d][1] * u0, E[d][2] * u0, E[d][3] * u0};
+#pragma unroll
+      for (int c = 0; c < 4; c++) {
+        real g0 = c == 0 ? (real)1.0f : (real)0.0f;
+        T[d][c] = A * u4[c] - g0 * pr[d];
+      }
+    }
+    real F[2][4];
+#pragma unroll
+    for (int f = 0; f < 2; f++) {  // kt1d, helper.h:199-262
+      const int l = 1 + f, r = 2 + f;
+      real h[4];
+#pragma unroll
+      for (int c = 0; c < 4; c++) h[c] = 0.5f * (E[l][c] + E[r][c]);
+      real vh = h[a + 1];
+      real lam = max_speed<real>(p, h[0], h[1], h[2], h[3], vh);
+      real pr_half = 0.5f * (pr[l] + pr[r]);
+#pragma unroll
+      for (int c = 0; c < 4; c++) {
+        real DAl = slope<real>(T[l - 1][c], T[l][c], T[l + 1][c]);
+        real DAr = slope<real>(T[r - 1][c], T[r][c], T[r + 1][c]);
+        real AL = T[l][c] + 0.5f * DAl;
+        real AR = T[r][c] - 0.5f * DAr;
+        real g0 = c == 0 ? (real)1.0f : (real)0.0f;
+        real ga = c == a + 1 ? (real)-1.0f : (real)0.0f;
+        real Jp = (AR + pr_half * g0) * vh - pr_half * ga;
+        real Jm = (AL + pr_half * g0) * vh - pr_half * ga;
+        F[f][c] = 0.5f * (Jp + Jm) - 0.5f * lam * (AR - AL);
+      }
+    }
+    const real D = a == 0 ? (real)p.DX : (a == 1 ? (real)p.DY : (real)p.DZ);
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+      real src = F[1][c];
+      src -= F[0][c];
+      if (riemann) S[c] = S[c] - src / D;
+      else if (a < 2) S[c] = S[c] - tau * src / D;
+      else S[c] = S[c] - tau * src / (tau * p.DZ);
+    }
+  }
+
+  // update_ev, kernel_ideal.cl:283-339
+  real e1[4];
+#pragma unroll
+  for (int c = 0; c < 4; c++) e1[c] = b.ev1[c * ld + I];
+  real ed = e1[0], vx = e1[1], vy = e1[2], vz = e1[3];
+  real pressure = eosP<real>(p, ed);
+  real u0 = gamma3<real>(vx, vy, vz);
+  real umu[4] = {u0 * 1.0f, u0 * vx, u0 * vy, u0 * vz};
+  real old_time = tau - (step - 1) * p.DT;
+  real T0m[4];
+#pragma unroll
+  for (int c = 0; c < 4; c++) {
+    real g0 = c == 0 ? (real)1.0f : (real)0.0f;
+    T0m[c] = (ed + pressure) * u0 * umu[c] - pressure * g0;
+    if (!riemann) T0m[c] = T0m[c] * old_time;
+    T0m[c] = T0m[c] + S[c] * p.DT / step;
+  }
+  real T00, T01, T02, T03;
+  if (riemann) {
+    T00 = cmax<real>(acu, T0m[0]);
+    T01 = (fabs(T0m[1]) < acu) ? (real)0.0f : T0m[1];
+    T02 = (fabs(T0m[2]) < acu) ? (real)0.0f : T0m[2];
+    T03 = (fabs(T0m[3]) < acu) ? (real)0.0f : T0m[3];
+  } else {
+    T00 = cmax<real>(acu, T0m[0]) / tau;
+    T01 = (fabs(T0m[1]) < acu) ? (real)0.0f : T0m[1] / tau;
+    T02 = (fabs(T0m[2]) < acu) ? (real)0.0f : T0m[2] / tau;
+    T03 = (fabs(T0m[3]) < acu) ? (real)0.0f : T0m[3] / tau;
+  }
+  real M = sqrt(T01 * T01 + T02 * T02 + T03 * T03);
+  real SCALE_COEF = 0.999f;
+  if (M > T00) {
+    T01 *= SCALE_COEF * T00 / M;
+    T02 *= SCALE_COEF * T00 / M;
+    T03 *= SCALE_COEF * T00 / M;
+    M = SCALE_COEF * T00;
+  }
+  real ed_find = root_newton<real>(p, T00, M);
+  ed_find = cmax<real>(0.0f, ed_find);
+  real pr = eosP<real>(p, ed_find);
+  real epv = cmax<real>(acu, T00 + pr);
+  real en[4] = {ed_find, T01 / epv, T02 / epv, T03 / epv};
+#pragma unroll
+  for (int c = 0; c < 4; c++) b.evnew[c * ld + I] = en[c];
+  if (b.write_src)
+#pragma unroll
+    for (int c = 0; c < 4; c++) b.src[c * ld + I] = S[c];
+  if (b.edmax_key && en[0] == en[0]) atomicMax(b.edmax_key, fkey(en[0]));
+}
+
+}  // namespace clv

@@ -1,0 +1,108 @@
+"""Equation-of-state tables, mirroring pyvisc/eos/eos.py (class Eos).
+
+An Eos carries the tabulated (cs2, p, T, s) on a uniform energy-density grid
+(ed_start, ed_step, num_of_ed) plus the host-side functions f_P, f_T, f_S,
+f_ed, f_cs2 the reference exposes. create_table() returns the float32 image
+the kernels read (the reference's RGBA image2d, eos.py:184-203): nrow x ncol
+texels of (cs2, p, T, s), read with clamp-to-edge nearest sampling and a
+manual linear interpolation (eos_table.h:39-62).
+
+Supported eos_type values: 'ideal_gas' (eos.py:42-59, computed here) and
+'lattice_pce165' (eos.py:102-113; the table is regenerated from the s95p
+source grids by eos_tables/make_pce165.py because EOS_PST.dat is absent from
+the reference snapshot). A user-built table can be passed as a
+handcrafted_eos object with the same attributes (ideal.py:60-69).
+"""
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+
+# (nrow, ncol) that CLIdeal passes to create_table per eos_type (ideal.py:67-83)
+TABLE_SHAPE = {
+    'ideal_gas': (200, 1000),
+    'lattice_pce165': (100, 1555),
+}
+
+
+class Eos(object):
+    """EOS table and host-side thermodynamic functions (pyvisc/eos/eos.py:20)."""
+
+    def __init__(self, eos_type='ideal_gas'):
+        self.eos_type = eos_type
+        if eos_type == 'ideal_gas':
+            self.ideal_gas()
+        elif eos_type == 'lattice_pce165':
+            self.lattice_pce165()
+        else:
+            raise ValueError('unsupported eos_type %r (supported: %s)'
+                             % (eos_type, ', '.join(sorted(TABLE_SHAPE))))
+
+    def ideal_gas(self):
+        """Conformal gas p = e/3 with 169/4 degrees of freedom (eos.py:42-59)."""
+        hbarc = 0.1973269
+        dof = 169.0 / 4.0
+        coef = np.pi * np.pi / 30.0
+        self.f_P = lambda ed: np.array(ed) / 3.0
+        self.f_T = lambda ed: hbarc * (1.0 / (dof * coef) * np.array(ed) / hbarc) ** 0.25 + 1.0E-10
+        self.f_S = lambda ed: (np.array(ed) + self.f_P(ed)) / self.f_T(ed)
+        self.f_ed = lambda T: dof * coef * hbarc * (np.array(T) / hbarc) ** 4.0
+        self.f_cs2 = lambda ed: 1.0 / 3.0 * np.ones_like(ed)
+        self.ed = np.linspace(0, 1999.99, 200000)
+        self.pr = self.f_P(self.ed)
+        self.T = self.f_T(self.ed)
+        self.s = self.f_S(self.ed)
+        self.cs2 = self.f_cs2(self.ed)
+        self.ed_start = 0.0
+        self.ed_step = 0.01
+        self.num_of_ed = 200000
+
+    def lattice_pce165(self):
+        """s95p-PCE165-v0 lattice + partial-chemical-equilibrium HRG EOS."""
+        d = np.load(os.path.join(_HERE, 'eos_tables', 'lattice_pce165.npz'))
+        self.ed_start = float(d['ed_start'])
+        self.ed_step = float(d['ed_step'])
+        self.num_of_ed = int(d['num_of_ed'])
+        self.ed = np.arange(self.num_of_ed) * self.ed_step
+        e = d['src_e']
+        self.pr = np.interp(self.ed, e, d['src_p'])
+        self.s = np.interp(self.ed, e, d['src_s'])
+        self.T = np.interp(self.ed, e, d['src_T'])
+        self.cs2 = d['cs2'].astype(np.float64)
+        self._from_arrays()
+
+    def _from_arrays(self):
+        """Linear (k=1) interpolants as eos.py:78-83 builds them."""
+        ed, pr, T, s = self.ed, self.pr, self.T, self.s
+
+        def lin(x, xp, fp):
+            x = np.asarray(x, dtype=np.float64)
+            y = np.interp(x, xp, fp)
+            # InterpolatedUnivariateSpline(k=1, ext=0) extrapolates linearly
+            lo = x < xp[0]
+            hi = x > xp[-1]
+            if np.any(lo):
+                y = np.where(lo, fp[0] + (x - xp[0]) * (fp[1] - fp[0]) / (xp[1] - xp[0]), y)
+            if np.any(hi):
+                y = np.where(hi, fp[-1] + (x - xp[-1]) * (fp[-1] - fp[-2]) / (xp[-1] - xp[-2]), y)
+            return y[()] if y.ndim == 0 else y
+
+        self.f_ed = lambda t: lin(t, T, ed)
+        self.f_T = lambda e: lin(e, ed, T)
+        self.f_P = lambda e: lin(e, ed, pr)
+        self.f_S = lambda e: lin(e, ed, s)
+        self.f_cs2 = lambda e: lin(e, ed, self.cs2)
+
+    def create_table(self, nrow=None, ncol=None):
+        """Return (table, meta): the float32 (nrow, ncol, 4) image of
+        (cs2, p, T, s) and the constants the kernels use (eos.py:184-203)."""
+        if nrow is None or ncol is None:
+            nrow, ncol = TABLE_SHAPE.get(self.eos_type, (200, 1000))
+        src = np.stack([np.asarray(self.cs2, np.float64), self.pr, self.T, self.s], axis=1).astype(np.float32)
+        if src.shape[0] != nrow * ncol:
+            raise ValueError('EOS table has %d rows, image is %dx%d' % (src.shape[0], nrow, ncol))
+        src = np.ascontiguousarray(src.reshape(nrow, ncol, 4))
+        meta = dict(ed_start=self.ed_start, ed_step=self.ed_step, num_of_ed=self.num_of_ed,
+                    nrow=nrow, ncol=ncol)
+        return src, meta

@@ -1,0 +1,144 @@
+/* clvisc_b200 -- C ABI of the B200 (sm_100a) backend for the CLVisc hydro step.
+ *
+ * This ABI replaces the OpenCL programs that CLVisc builds and launches from
+ * Python (pyvisc/backend_opencl.py and pyvisc/kernel/*.cl, driven by
+ * pyvisc/ideal.py and pyvisc/visc.py). Every entry point below names the
+ * reference kernel(s) it stands in for.
+ *
+ * Conventions
+ *   - Plain pointers and sizes only. Field pointers are DEVICE pointers to
+ *     structure-of-arrays planes: a field with w components occupies w planes
+ *     of `ld` elements each (plane c starts at ptr + c*ld), and cell
+ *     I = i*NY*NZ + j*NZ + k, the reference's order (kernel_visc.cl:145).
+ *     ev has 4 planes (ed, vx, vy, veta); pi has 10 planes in the reference's
+ *     packed order 00 01 02 03 11 12 13 22 23 33 (helper.h:31).
+ *   - The element type is float when clv_params.precision == 4 and double
+ *     when it is 8 (the reference's use_float32 flag, config.py:200).
+ *   - `stream` is a cudaStream_t passed as void* (NULL = legacy stream).
+ *   - Every function returns 0 (CLV_OK) or a negative CLV_ERR_* code; no
+ *     exception crosses the ABI and nothing is printed. clv_last_error()
+ *     gives a one-line message for the last failure of the calling thread.
+ *   - Launches are asynchronous on `stream` unless stated otherwise.
+ */
+#ifndef CLVISC_B200_H
+#define CLVISC_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CLV_OK 0
+#define CLV_ERR_INVALID (-1)  /* bad argument (null pointer, size, precision) */
+#define CLV_ERR_CUDA (-2)     /* CUDA runtime error (launch, copy)            */
+#define CLV_ERR_CAPACITY (-3) /* output buffer too small                      */
+
+/* flags: the reference's optional -D defines (ideal.py:164-165, visc.py:111-121) */
+#define CLV_FLAG_RIEMANN_TEST 1
+#define CLV_FLAG_GUBSER_VISC_TEST 2
+#define CLV_FLAG_PIMN_OMEGA_COUPLING 4
+#define CLV_FLAG_OMEGA_OMEGA_COUPLING 8
+
+/* parts of a viscous stage (visc.py:287 IS_stepUpdate, visc.py:232 visc_stepUpdate) */
+#define CLV_PART_IS 1
+#define CLV_PART_KT 2
+
+/* Run constants: the reference's compile-time defines (ideal.py:146-171,
+ * eos.py:194-201, ideal.py:190-194). Floating constants are the float values
+ * of the "%sf" literals the reference host emits, in FP64 mode too. */
+typedef struct clv_params {
+  int nx, ny, nz;
+  long long ld; /* plane stride in elements, >= nx*ny*nz */
+  int precision; /* 4 = float32, 8 = float64 */
+  float dt, dx, dy, dz, tau0;
+  float etaos_xmin, etaos_ymin, etaos_left_slop, etaos_right_slop, lam1;
+  float efrz;
+  int nxskip, nyskip, nzskip;
+  float eos_ed_start, eos_ed_step;
+  int eos_num_ed, eos_nrow, eos_ncol;
+  const float *eos_table; /* device, eos_nrow*eos_ncol texels of (cs2, p, T, s) */
+  int flags;              /* CLV_FLAG_* */
+} clv_params;
+
+/* Buffers of one viscous Runge-Kutta stage. `step` is 1 or 2 as in
+ * visc.py:536-543; d_ev[], d_pi[] are the reference's three-slot buffers. */
+typedef struct clv_visc_buffers {
+  const void *ev_st;     /* d_ev[step]: stencil input, 4 planes                */
+  const void *pi_st;     /* d_pi[step]: stencil input, 10 planes               */
+  const void *ev1;       /* d_ev[1]                                            */
+  const void *ev2_ed;    /* plane 0 of d_ev[2] (read by step 1's pi update)    */
+  const void *pi1;       /* d_pi[1]: start point of the pi update              */
+  const void *pi_n;      /* pi at the start of the time step (d_pi[0])         */
+  const void *pi_new_in; /* d_pi[3-step]: read when CLV_PART_IS is not fused   */
+  void *ev_new;          /* d_ev[3-step]                                       */
+  void *pi_new;          /* d_pi[3-step]                                       */
+  void *src;             /* 14 planes: d_Src (4) then d_IS_src (10)            */
+  void *udiff;           /* 4 planes                                           */
+  unsigned char *goodcell; /* 1 byte per cell (the reference's d_goodcell)     */
+  void *edmax_key;       /* optional: running max of ev_new energy density     */
+  int write_src;         /* keep the accumulated sources (needed by step 2)    */
+  int write_udiff;       /* step 2 only: udiff = u(ev_new) - u(ev1)            */
+} clv_visc_buffers;
+
+/* Library version; the low 8 bits bump on any ABI change. */
+int clv_version(void);
+/* One-line description of the last error on this thread ("" if none). */
+const char *clv_last_error(void);
+/* Required alignment (bytes) of every field pointer and of ld*elem_size. */
+int clv_alignment(void);
+
+/* One ideal Runge-Kutta stage: kt_src_christoffel + kt_src_alongx/y/z +
+ * update_ev (kernel_ideal.cl:3-231, driven by ideal.py:211-255).
+ * ev_st = d_ev[step], ev1 = d_ev[1], ev_new = d_ev[3-step], src = d_Src (4
+ * planes; zeroed by step 1, accumulated by step 2). ev_new may equal ev1.
+ * edmax_key (nullable) receives the max of ev_new's energy density. */
+int clv_ideal_stage(const clv_params *p, int step, double tau, const void *ev_st, const void *ev1,
+                    void *ev_new, void *src, int write_src, void *edmax_key, void *stream);
+
+/* One viscous Runge-Kutta stage, any of CLV_PART_IS (visc_src_christoffel,
+ * visc_src_alongx/y/z, update_pimn: kernel_IS.cl:41-709) and CLV_PART_KT
+ * (kt_src_christoffel, kt_src_alongx/y/z, update_ev: kernel_visc.cl:11-393).
+ * With both parts the new pi feeds update_ev from registers. */
+int clv_visc_stage(const clv_params *p, int step, double tau, int parts, const clv_visc_buffers *b, void *stream);
+
+/* visc_initialize (kernel_IS.cl:10-36): Navier-Stokes pi from ev, udiff = 0,
+ * goodcell = 1. Components of pi1 other than 11, 22, 33 are left as they are. */
+int clv_visc_initialize(const clv_params *p, void *pi1, unsigned char *goodcell, void *udiff, const void *ev,
+                        double tau, void *stream);
+
+/* get_udiff (kernel_IS.cl:714-724): udiff = u(ev1) - u(ev0). */
+int clv_get_udiff(const clv_params *p, void *udiff, const void *ev0, const void *ev1, void *stream);
+
+/* reduction_stage1 + host max (kernel_reduction.cl:7-39, ideal.py:257-262):
+ * folds max(ed) over the first plane of ev into *key (device, an ordered
+ * integer of precision-sized width; set it to 0 first with clv_max_ed_reset).
+ * NaN values are ignored. */
+int clv_max_ed_reset(const clv_params *p, void *key, void *stream);
+int clv_max_ed(const clv_params *p, const void *ev, void *key, void *stream);
+/* Synchronous: decode *key into a double (-FLT_MAX if no value was seen). */
+int clv_max_ed_read(const clv_params *p, const void *key, double *out, void *stream);
+
+/* get_hypersf / visc_hypersf (kernel_hypersf.cl:404-660): append the freeze-out
+ * surface elements between (ev_old, tau_old) and (ev_new, tau_new) to the
+ * output arrays, in coarse-cube (i, j, k) order, after the *total elements
+ * already there (total: device long long, updated on the stream).
+ *   sf   : capacity x 8 reals (dSigma_0..3, vx, vy, veta, etas)  [real8]
+ *   txyz : capacity x 4 reals (tau cosh eta, x, y, tau sinh eta) [real4]
+ *   pisf : capacity x 10 reals (visc != 0 only; may be NULL)
+ * Elements beyond capacity are counted but not written; compare *total with
+ * capacity after the stream completes.
+ * scratch: device memory of clv_hypersf_scratch_bytes(p) bytes. */
+size_t clv_hypersf_scratch_bytes(const clv_params *p);
+int clv_hypersf_append(const clv_params *p, int visc, double tau_old, double tau_new, const void *ev_old,
+                       const void *ev_new, const void *pi_old, const void *pi_new, void *sf, void *txyz, void *pisf,
+                       long long capacity, long long *total, void *scratch, size_t scratch_bytes, void *stream);
+
+/* Host-boundary layout transposes: (n, w) row-major <-> w planes of ld. */
+int clv_aos_to_soa(const clv_params *p, const void *aos, void *soa, long long n, int w, void *stream);
+int clv_soa_to_aos(const clv_params *p, const void *soa, void *aos, long long n, int w, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CLVISC_B200_H */

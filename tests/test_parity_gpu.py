@@ -1,0 +1,177 @@
+"""CUDA kernels (through the C ABI) against the oracle on the same seeded
+inputs. The kernels are built without FMA contraction and with IEEE
+division/square root, like the oracle, so the expected agreement is exact:
+every field bit for bit, and hypersurface element counts equal. The only
+transcendental outputs (tau*cosh(eta), tau*sinh(eta) of sf_txyz) are compared
+to 4 ulp (rtol 5e-7 FP32, 1e-15 FP64)."""
+import numpy as np
+import pytest
+import torch
+
+from parity_util import assert_same, make_cfg, seeded_ic
+
+pytestmark = pytest.mark.gpu
+
+
+def _ref_order_step(v, loop):
+    """visc.py:527-544 with the separate IS / KT launches."""
+    v.d_pi[0].copy_(v.d_pi[1])
+    v.ideal.d_ev[0].copy_(v.ideal.d_ev[1])
+    v.IS_stepUpdate(1)
+    v.visc_stepUpdate(1)
+    v.update_time(loop)
+    v.IS_stepUpdate(2)
+    v.visc_stepUpdate(2)
+    v.update_udiff(v.ideal.d_ev[0], v.ideal.d_ev[1])
+
+
+def _compare_visc(v, o, tag):
+    assert_same(tag + ' ev[1]', v.ideal.field_to_host(v.ideal.d_ev[1]), o.ideal.d_ev[1])
+    assert_same(tag + ' pi[1]', v.ideal.field_to_host(v.d_pi[1]), o.d_pi[1])
+    assert_same(tag + ' ev[2]', v.ideal.field_to_host(v.ideal.d_ev[2]), o.ideal.d_ev[2])
+    assert_same(tag + ' pi[2]', v.ideal.field_to_host(v.d_pi[2]), o.d_pi[2])
+    assert_same(tag + ' udiff', v.ideal.field_to_host(v.d_udiff), o.d_udiff)
+    assert_same(tag + ' goodcell', v.d_goodcell[:v.size].cpu().numpy().astype(np.float64),
+                o.d_goodcell.astype(np.float64))
+
+
+@pytest.mark.parametrize('use_float32', [True, False])
+@pytest.mark.parametrize('grid', [(13, 11, 9), (17, 15, 1), (1, 9, 12)])
+def test_ideal_stage_parity(cuda_lib, oracle_mod, use_float32, grid):
+    from clvisc_b200.ideal import CLIdeal
+    cfg = make_cfg(*grid, use_float32=use_float32)
+    ic = seeded_ic(cfg, seed=3, flow=0.3)
+    g = CLIdeal(cfg)
+    o = oracle_mod.OracleIdeal(cfg)
+    g.load_ini(ic)
+    o.load_ini(ic)
+    for n in range(6):
+        g.stepUpdate(1)
+        o.stepUpdate(1)
+        assert_same('stage1 ev[2] n=%d' % n, g.field_to_host(g.d_ev[2]), o.d_ev[2])
+        assert_same('stage1 src n=%d' % n, g.field_to_host(g.d_Src), o.d_Src)
+        g.update_time(n)
+        o.update_time(n)
+        g.stepUpdate(2)
+        o.stepUpdate(2)
+        assert_same('stage2 ev[1] n=%d' % n, g.field_to_host(g.d_ev[1]), o.d_ev[1])
+    assert g.max_energy_density() == o.max_energy_density()
+
+
+@pytest.mark.parametrize('use_float32', [True, False])
+def test_visc_construction_parity(cuda_lib, oracle_mod, use_float32):
+    """IS_initialize on the empty state and the ideal prediction (visc.py:101-102)."""
+    from clvisc_b200.visc import CLVisc
+    cfg = make_cfg(11, 9, 7, use_float32=use_float32)
+    v = CLVisc(cfg)
+    o = oracle_mod.OracleVisc(cfg)
+    assert_same('pi[1]', v.ideal.field_to_host(v.d_pi[1]), o.d_pi[1])
+    assert_same('ev[2]', v.ideal.field_to_host(v.ideal.d_ev[2]), o.ideal.d_ev[2])
+    v.load_ini(seeded_ic(cfg))
+    o.load_ini(seeded_ic(cfg))
+    v.IS_initialize()
+    o.IS_initialize()
+    assert_same('pi[1] from ic', v.ideal.field_to_host(v.d_pi[1]), o.d_pi[1])
+
+
+@pytest.mark.parametrize('use_float32', [True, False])
+@pytest.mark.parametrize('grid', [(15, 13, 11), (19, 17, 1)])
+def test_visc_parts_parity(cuda_lib, oracle_mod, use_float32, grid):
+    """Separate IS_stepUpdate / visc_stepUpdate launches, reference order."""
+    from clvisc_b200.visc import CLVisc
+    cfg = make_cfg(*grid, use_float32=use_float32)
+    ic = seeded_ic(cfg, seed=5, flow=0.2)
+    v = CLVisc(cfg)
+    o = oracle_mod.OracleVisc(cfg)
+    v.load_ini(ic)
+    o.load_ini(ic)
+    v.IS_initialize()
+    o.IS_initialize()
+    for n in range(4):
+        _ref_order_step(v, n)
+        o.step(n)
+        _compare_visc(v, o, 'parts n=%d' % n)
+
+
+@pytest.mark.parametrize('use_float32', [True, False])
+@pytest.mark.parametrize('grid', [(15, 13, 11), (21, 19, 1), (9, 1, 13)])
+def test_visc_fused_step_parity(cuda_lib, oracle_mod, use_float32, grid):
+    """The fused per-stage kernel of evolve() against the reference order."""
+    from clvisc_b200.visc import CLVisc
+    cfg = make_cfg(*grid, use_float32=use_float32)
+    ic = seeded_ic(cfg, seed=9)
+    v = CLVisc(cfg)
+    o = oracle_mod.OracleVisc(cfg)
+    v.load_ini(ic)
+    o.load_ini(ic)
+    for n in range(8):
+        v.step(n, edmax=True)
+        o.step(n)
+        tag = 'fused n=%d' % n
+        assert_same(tag + ' ev[1]', v.ideal.field_to_host(v.ideal.d_ev[1]), o.ideal.d_ev[1])
+        assert_same(tag + ' pi[1]', v.ideal.field_to_host(v.d_pi[1]), o.d_pi[1])
+        assert_same(tag + ' ev[2]', v.ideal.field_to_host(v.ideal.d_ev[2]), o.ideal.d_ev[2])
+        assert_same(tag + ' udiff', v.ideal.field_to_host(v.d_udiff), o.d_udiff)
+        assert v.read_edmax_key() == o.ideal.max_energy_density()
+
+
+@pytest.mark.parametrize('use_float32', [True, False])
+def test_visc_evolve_hypersf_parity(cuda_lib, oracle_mod, use_float32, tmp_path):
+    """evolve() with freeze-out extraction: same history, same state, same
+    surface element count and element values."""
+    from clvisc_b200.visc import CLVisc
+    cfg = make_cfg(25, 23, 13, use_float32=use_float32, dt=0.04, ntskip=5, skip=(2, 2, 1), out=str(tmp_path))
+    ic = seeded_ic(cfg, seed=11, edmax=20.0)
+    v = CLVisc(cfg)
+    o = oracle_mod.OracleVisc(cfg)
+    v.load_ini(ic)
+    o.load_ini(ic)
+    v.evolve(max_loops=60, force_run_to_maxloop=True, save_hypersf=True)
+    o.evolve(max_loops=60, force_run_to_maxloop=True, save_hypersf=True)
+    assert_same('history', np.array(v.ideal.history, np.float64), np.array(o.ideal.history, np.float64))
+    assert_same('ev[1]', v.ideal.field_to_host(v.ideal.d_ev[1]), o.ideal.d_ev[1])
+    sf_o, tx_o, pi_o = o.hypersf()
+    n = v.ideal.read_num_of_sf()
+    assert n == len(sf_o) and n > 0
+    sf_g = v.ideal.d_hypersf[:n].cpu().numpy()
+    tx_g = v.ideal.d_sf_txyz[:n].cpu().numpy()
+    pi_g = v.d_pi_sf[:n].cpu().numpy()
+    assert_same('hypersf', sf_g, sf_o)
+    assert_same('pisf', pi_g, pi_o)
+    assert_same('sf x, y', tx_g[:, 1:3], tx_o[:, 1:3])
+    rtol = 5e-7 if use_float32 else 1e-15
+    np.testing.assert_allclose(tx_g[:, [0, 3]], tx_o[:, [0, 3]], rtol=rtol, atol=0)
+
+
+def test_ideal_config1_parity(cuda_lib, oracle_mod, tmp_path):
+    """The (2+1)D ideal case: 101x101x1, dx=0.16, dt=0.02, tau0=0.6, conformal
+    EOS, FP64, Gaussian 30*exp(-x^2/8 - y^2/12.5), evolved to tau = 10 fm."""
+    from clvisc_b200.ideal import CLIdeal
+    from clvisc_b200.initial import gaussian_2d
+    cfg = make_cfg(101, 101, 1, use_float32=False, eos_type='ideal_gas', dx=0.16, dt=0.02, ntskip=10,
+                   skip=(1, 1, 1), out=str(tmp_path))
+    ic = gaussian_2d(101, 101, 0.16, 0.16)
+    g = CLIdeal(cfg)
+    o = oracle_mod.OracleIdeal(cfg)
+    g.load_ini(ic)
+    o.load_ini(ic)
+    g.evolve(max_loops=470, save_hypersf=True, to_maxloop=True)
+    o.evolve(max_loops=470, save_hypersf=True, to_maxloop=True)
+    assert_same('history', np.array(g.history, np.float64), np.array(o.history, np.float64))
+    assert_same('ev', g.field_to_host(g.d_ev[1]), o.d_ev[1])
+    # kernel_hypersf.cl:422 needs (k+1)*nzskip < NZ: a one-cell eta grid has no surface
+    assert g.read_num_of_sf() == len(o.hypersf()[0]) == 0
+
+
+def test_layout_roundtrip_and_max(cuda_lib):
+    from clvisc_b200.ideal import CLIdeal
+    cfg = make_cfg(7, 5, 3)
+    g = CLIdeal(cfg)
+    x = np.random.default_rng(1).normal(size=(g.size, 4)).astype(np.float32)
+    g.load_ini(x)
+    np.testing.assert_array_equal(g.ev_to_host(), x)
+    assert g.max_energy_density() == x[:, 0].max()
+    x[:, 0] = -np.abs(x[:, 0]) - 1.0
+    g.load_ini(x)
+    assert g.max_energy_density() == x[:, 0].max()
+    torch.cuda.synchronize()
