@@ -39,10 +39,10 @@ ALG_BYTES_PER_CELL_UPDATE = 312
 SLAB_NZ = 16  # CPU-baseline sample: a 385 x 385 x 16 eta slab of the event
 
 
-def make_cfg(nz=NZ, out='/tmp/clv_bench'):
+def make_cfg(nz=NZ, out='/tmp/clv_bench', nx=NX, ny=NY):
     from clvisc_b200.config import read_config, set_real
     cfg = read_config([])
-    cfg.NX, cfg.NY, cfg.NZ = NX, NY, nz
+    cfg.NX, cfg.NY, cfg.NZ = nx, ny, nz
     cfg.DX = cfg.DY = DX
     cfg.DZ = DZ
     cfg.DT = DT
@@ -58,9 +58,9 @@ def make_cfg(nz=NZ, out='/tmp/clv_bench'):
     return set_real(cfg)
 
 
-def initial_condition(seed=5):
+def initial_condition(seed=5, nx=NX, ny=NY, nz=NZ):
     from clvisc_b200.initial import glauber_event
-    return glauber_event(NX, NY, NZ, DX, DX, DZ, b=8.0, seed=seed, edmax=50.0)
+    return glauber_event(nx, ny, nz, DX, DX, DZ, b=8.0, seed=seed, edmax=50.0)
 
 
 class ClockSampler(object):
@@ -187,12 +187,13 @@ def run_gpu(args, rank, world, dist):
     from clvisc_b200.visc import CLVisc
     dev = int(os.environ.get('LOCAL_RANK', 0))
     torch.cuda.set_device(dev)
-    cfg = make_cfg(out='/tmp/clv_bench_r%d' % rank)
-    ic = initial_condition(seed=5)
+    nx, ny, nz = args.grid
+    cfg = make_cfg(nz=nz, nx=nx, ny=ny, out='/tmp/clv_bench_r%d' % rank)
+    ic = initial_condition(seed=5, nx=nx, ny=ny, nz=nz)
     v = CLVisc(cfg, gpu_id=dev)
     v.load_ini(ic)
     stream = torch.cuda.current_stream()
-    cells = NX * NY * NZ
+    cells = nx * ny * nz
 
     def barrier():
         if dist is not None:
@@ -219,6 +220,11 @@ def run_gpu(args, rank, world, dist):
         ms = float(t.item())
     value = world * cells * args.steps / (ms * 1e-3)
 
+    if args.no_e2e:
+        if rank == 0:
+            print(json.dumps({'metric': METRIC, 'value': value, 'unit': UNIT, 'ms_per_step': ms / args.steps,
+                              'config': {'grid': [nx, ny, nz]}, 'gpu_launches': 2 * args.steps}), flush=True)
+        return
     # end to end through the public API with host buffers
     host_ic = torch.from_numpy(np.ascontiguousarray(ic)).pin_memory()
     v2 = CLVisc(cfg, gpu_id=dev)
@@ -276,6 +282,9 @@ def main():
     ap.add_argument('--warmup', type=int, default=3)
     ap.add_argument('--impl', default='b200', choices=['b200', 'reference'])
     ap.add_argument('--no-cpu-baseline', action='store_true')
+    ap.add_argument('--no-e2e', action='store_true', help='device-timed steps only (profiling runs)')
+    ap.add_argument('--grid', type=lambda s: tuple(int(x) for x in s.split(',')), default=(NX, NY, NZ),
+                    help='nx,ny,nz (default: the 385,385,115 workload)')
     args = ap.parse_args()
     world = int(os.environ.get('WORLD_SIZE', '1'))
     rank = int(os.environ.get('RANK', '0'))

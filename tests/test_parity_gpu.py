@@ -120,7 +120,8 @@ def test_visc_evolve_hypersf_parity(cuda_lib, oracle_mod, use_float32, tmp_path)
     """evolve() with freeze-out extraction: same history, same state, same
     surface element count and element values."""
     from clvisc_b200.visc import CLVisc
-    cfg = make_cfg(25, 23, 13, use_float32=use_float32, dt=0.04, ntskip=5, skip=(2, 2, 1), out=str(tmp_path))
+    cfg = make_cfg(25, 23, 13, use_float32=use_float32, dx=0.8, dz=0.6, dt=0.04, ntskip=5, skip=(2, 2, 1),
+                   out=str(tmp_path))
     ic = seeded_ic(cfg, seed=11, edmax=20.0)
     v = CLVisc(cfg)
     o = oracle_mod.OracleVisc(cfg)
