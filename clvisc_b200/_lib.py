@@ -16,6 +16,15 @@ CLV_FLAG_GUBSER_VISC_TEST = 2
 CLV_FLAG_PIMN_OMEGA_COUPLING = 4
 CLV_FLAG_OMEGA_OMEGA_COUPLING = 8
 
+CLV_OPT_STAGE_KERNEL = 1
+CLV_OPT_CHUNK = 2
+CLV_OPT_TILED_BLOCKS = 3
+
+
+def set_option(option, value):
+    """Process-wide tuning option of the CUDA library (clv_set_option)."""
+    check(load().clv_set_option(int(option), int(value)), 'clv_set_option')
+
 CLV_ERR = {-1: 'invalid argument', -2: 'CUDA error', -3: 'capacity exceeded'}
 
 
@@ -58,6 +67,7 @@ _SIGS = {
     'clv_version': ([], ctypes.c_int),
     'clv_last_error': ([], ctypes.c_char_p),
     'clv_alignment': ([], ctypes.c_int),
+    'clv_set_option': ([ctypes.c_int, ctypes.c_int], ctypes.c_int),
     'clv_ideal_stage': ([_P, ctypes.c_int, ctypes.c_double, _VP, _VP, _VP, _VP, ctypes.c_int, _VP, _VP], ctypes.c_int),
     'clv_visc_stage': ([_P, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.POINTER(ClvViscBuffers), _VP],
                        ctypes.c_int),

@@ -9,10 +9,14 @@
 #include "clv_hypersf.cuh"
 #include "clv_misc.cuh"
 #include "clv_stage.cuh"
+#include "clv_stage_tiled.cuh"
 
 namespace {
 
 thread_local std::string g_err;
+int g_stage_kernel = 0;  // CLV_OPT_STAGE_KERNEL: 0 tiled, 1 per-cell
+int g_chunk = 32;        // CLV_OPT_CHUNK: x planes per tiled CTA
+int g_minb = 2;          // CLV_OPT_TILED_BLOCKS: resident tiled CTAs per SM (FP32)
 
 int fail(int code, const char* fmt, const char* what = "") {
   char buf[256];
@@ -60,6 +64,34 @@ int to_params(const clv_params* in, clv::Params* out) {
 inline long long ncell(const clv::Params& p) { return (long long)p.nx * p.ny * p.nz; }
 inline unsigned int nblk(long long n, int bs) { return (unsigned int)((n + bs - 1) / bs); }
 
+template <class real, bool IS, bool KT, bool CPL, int MINB>
+int launch_tiled_b(const clv::Params& p, const clv::ViscBuffers<real>& v, int step, double tau, cudaStream_t s) {
+  constexpr int TJ = 8, TK = 32;
+  typedef clv::TileSmem<real, TJ, TK> SM;
+  auto kern = clv::visc_stage_tiled_kernel<real, IS, KT, CPL, TJ, TK, MINB>;
+  static bool configured = false;
+  if (!configured) {
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SM)) != cudaSuccess)
+      return cuda_check("cudaFuncSetAttribute(visc_stage_tiled_kernel)");
+    configured = true;
+  }
+  const int chunk = g_chunk;
+  dim3 grid((p.nz + TK - 1) / TK, (p.ny + TJ - 1) / TJ, (p.nx + chunk - 1) / chunk);
+  kern<<<grid, TJ * TK, sizeof(SM), s>>>(p, v, step, (real)tau, chunk);
+  return cuda_check("visc_stage_tiled_kernel");
+}
+
+template <class real, bool IS, bool KT>
+int launch_tiled(const clv::Params& p, const clv::ViscBuffers<real>& v, int step, double tau, cudaStream_t s) {
+  // the coupling terms (GUBSER_VISC_TEST, PIMUNU_OMEGA_COUPLING,
+  // OMEGA_OMEGA_COUPLING) live in a separate instantiation so that the
+  // default kernel does not carry their code
+  const bool cpl = IS && (p.flags & (clv::FLAG_GUBSER_VISC | clv::FLAG_PIMN_OMEGA | clv::FLAG_OMEGA_OMEGA));
+  if (cpl) return launch_tiled_b<real, IS, KT, IS, 1>(p, v, step, tau, s);
+  if (sizeof(real) == 8 || g_minb == 1) return launch_tiled_b<real, IS, KT, false, 1>(p, v, step, tau, s);
+  return launch_tiled_b<real, IS, KT, false, 2>(p, v, step, tau, s);
+}
+
 template <class real>
 int visc_stage_t(const clv::Params& p, int step, double tau, int parts, const clv_visc_buffers* b, cudaStream_t s) {
   clv::ViscBuffers<real> v;
@@ -76,12 +108,20 @@ int visc_stage_t(const clv::Params& p, int step, double tau, int parts, const cl
     return fail(CLV_ERR_INVALID, "visc stage: null buffer for the pi update%s");
   if (kt && (!v.evnew || !v.pin || (!is && !v.pi2in))) return fail(CLV_ERR_INVALID, "visc stage: null buffer for update_ev%s");
   if (v.write_udiff && (!kt || !v.udiff)) return fail(CLV_ERR_INVALID, "visc stage: write_udiff needs CLV_PART_KT%s");
+  if (g_stage_kernel == 0) {
+    if (is && kt) return launch_tiled<real, true, true>(p, v, step, tau, s);
+    if (is) return launch_tiled<real, true, false>(p, v, step, tau, s);
+    return launch_tiled<real, false, true>(p, v, step, tau, s);
+  }
   const int bs = 128;
   dim3 grid(nblk(ncell(p), bs));
   real t = (real)tau;
-  if (is && kt) clv::visc_stage_kernel<real, true, true><<<grid, bs, 0, s>>>(p, v, step, t);
-  else if (is) clv::visc_stage_kernel<real, true, false><<<grid, bs, 0, s>>>(p, v, step, t);
-  else clv::visc_stage_kernel<real, false, true><<<grid, bs, 0, s>>>(p, v, step, t);
+  const bool cpl = p.flags & (clv::FLAG_GUBSER_VISC | clv::FLAG_PIMN_OMEGA | clv::FLAG_OMEGA_OMEGA);
+  if (is && kt && cpl) clv::visc_stage_kernel<real, true, true, true><<<grid, bs, 0, s>>>(p, v, step, t);
+  else if (is && kt) clv::visc_stage_kernel<real, true, true, false><<<grid, bs, 0, s>>>(p, v, step, t);
+  else if (is && cpl) clv::visc_stage_kernel<real, true, false, true><<<grid, bs, 0, s>>>(p, v, step, t);
+  else if (is) clv::visc_stage_kernel<real, true, false, false><<<grid, bs, 0, s>>>(p, v, step, t);
+  else clv::visc_stage_kernel<real, false, true, false><<<grid, bs, 0, s>>>(p, v, step, t);
   return cuda_check("visc_stage_kernel");
 }
 
@@ -141,6 +181,22 @@ extern "C" {
 int clv_version(void) { return 0x000101; }
 const char* clv_last_error(void) { return g_err.c_str(); }
 int clv_alignment(void) { return kAlign; }
+
+int clv_set_option(int option, int value) {
+  if (option == CLV_OPT_STAGE_KERNEL && (value == 0 || value == 1)) {
+    g_stage_kernel = value;
+    return CLV_OK;
+  }
+  if (option == CLV_OPT_TILED_BLOCKS && (value == 1 || value == 2)) {
+    g_minb = value;
+    return CLV_OK;
+  }
+  if (option == CLV_OPT_CHUNK && value >= 1 && value <= 4096) {
+    g_chunk = value;
+    return CLV_OK;
+  }
+  return fail(CLV_ERR_INVALID, "clv_set_option: unknown option or value%s");
+}
 
 int clv_ideal_stage(const clv_params* pp, int step, double tau, const void* ev_st, const void* ev1, void* ev_new,
                     void* src, int write_src, void* edmax_key, void* stream) {

@@ -47,6 +47,13 @@ template <class real> __device__ __forceinline__ real csign(real x) {
   return x > (real)0 ? (real)1 : (x < (real)0 ? (real)-1 : (x != x ? (real)0 : x));
 }
 
+// x / step for the Runge-Kutta stage index step (1 or 2): dividing by 1 or 2
+// is exact, as is multiplying by 1 or 0.5, so this equals the division bit for
+// bit (subnormal results included)
+template <class real> __device__ __forceinline__ real div_step(real x, int step) {
+  return step == 2 ? x * (real)0.5f : x;
+}
+
 // ------------------------------------------------------------------ EOS
 // Table lookup of eos_table.h:39-62: row/col from the energy density, two
 // nearest texels (the second wraps to the next row), clamp-to-edge, lerp.

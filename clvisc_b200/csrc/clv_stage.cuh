@@ -60,8 +60,184 @@ __device__ __forceinline__ Stencil make_stencil(int q, int L, long long stride) 
   return s;
 }
 
+// update_pimn (kernel_IS.cl:501-709) for cell I: e0 and pc are the stage
+// input ev and pi at the cell, grad the velocity gradients, S10 the IS sources
+// (updated in place); writes pi_new and goodcell, returns the new pi in pinew.
+template <class real, bool COUPLED>
+__device__ __forceinline__ void pi_update(const Params& p, const ViscBuffers<real>& b, int step, real tau,
+                                          long long I, const real e0[4], const real pc[10], const real grad[3][4],
+                                          real S10[10], real pinew[10]) {
+  const long long ld = p.ld;
+  const real acu = Acu<real>::v;
+  real e1[4];
+#pragma unroll
+  for (int c = 0; c < 4; c++) e1[c] = b.ev1[c * ld + I];
+  real g1 = gamma3<real>(e1[1], e1[2], e1[3]);
+  real u_old[4] = {g1 * 1.0f, g1 * e1[1], g1 * e1[2], g1 * e1[3]};
+  real u_new[4], udt[4];
+  real e2s0;
+  if (step == 1) {
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+      real ud = b.udiff[c * ld + I];
+      udt[c] = ud / (real)p.DT;
+      u_new[c] = u_old[c] + ud;
+    }
+    e2s0 = b.ev2e[I];
+  } else {
+    real g2 = gamma3<real>(e0[1], e0[2], e0[3]);
+    u_new[0] = g2 * 1.0f;
+    u_new[1] = g2 * e0[1];
+    u_new[2] = g2 * e0[2];
+    u_new[3] = g2 * e0[3];
+#pragma unroll
+    for (int c = 0; c < 4; c++) udt[c] = (u_new[c] - u_old[c]) / (real)p.DT;
+    e2s0 = e0[0];
+  }
+  real da[4][4];
+#pragma unroll
+  for (int c = 0; c < 4; c++) {
+    da[c][0] = udt[c];
+    da[c][1] = grad[0][c];
+    da[c][2] = grad[1][c];
+    da[c][3] = grad[2][c];
+  }
+  real u[4], DU[4];
+#pragma unroll
+  for (int c = 0; c < 4; c++) u[c] = (step == 1) ? u_old[c] : u_new[c];
+#pragma unroll
+  for (int c = 0; c < 4; c++) DU[c] = dot4<real>(u, da[c]);
+  real ed_step = (step == 1) ? e1[0] : e2s0;
+  real theta = udt[0] + grad[0][1] + grad[1][2] + grad[2][3];
+  real temperature = eos_comp<real>(p, ed_step, 2);
+  real sdens = eos_comp<real>(p, ed_step, 3);
+  real local_etaos = etaos<real>(p, temperature);
+  real etav = local_etaos * sdens * CLV_HBARC;
+  real one_over_taupi = temperature / (3.0f * cmax<real>(acu, local_etaos) * CLV_HBARC);
+  real coef_pipi = 0.0f;
+  if (COUPLED && (p.flags & FLAG_GUBSER_VISC)) {  // kernel_IS.cl:581-590
+    real ETAOS = p.ETAOS_YMIN;
+    real etavH = ETAOS * 4.0f / 3.0f;
+    real taupiH = p.LAM1 * p.LAM1 * etavH / 3.0f;
+    one_over_taupi = 1.0f / (taupiH * pow(ed_step, (real)-0.25f));
+    coef_pipi = p.LAM1 / ed_step;
+    etav = ETAOS * 4.0f / 3.0f * pow(ed_step, (real)0.75f);
+  }
+  real Omega[6] = {0, 0, 0, 0, 0, 0};
+  if (COUPLED && (p.flags & (FLAG_PIMN_OMEGA | FLAG_OMEGA_OMEGA))) omega_tensor<real>(udt, grad, u, Omega);
+
+  real max_pimn_abs = 0.0f;
+#pragma unroll
+  for (int mu = 0; mu < 4; mu++)
+#pragma unroll
+    for (int nu = mu; nu < 4; nu++) {
+      real gmu[4] = {gmn<real>(mu, 0), gmn<real>(mu, 1), gmn<real>(mu, 2), gmn<real>(mu, 3)};
+      real gnu[4] = {gmn<real>(nu, 0), gmn<real>(nu, 1), gmn<real>(nu, 2), gmn<real>(nu, 3)};
+      real sigma = dot4<real>(gmu, da[nu]) + dot4<real>(gnu, da[mu]) - (u[mu] * DU[nu] + u[nu] * DU[mu]) -
+                   2.0f / 3.0f * (gmn<real>(mu, nu) - u[mu] * u[nu]) * theta;
+      const int mn = pidx(mu, nu);
+      if (u[0] > 10000.0f) sigma = 0.0f;
+      real piNS = etav * sigma;
+      real pi_old = b.pi1[mn * ld + I] * u_old[0];
+      real src = -pc[mn] * theta / 3.0f - pc[mn] * u[0] / tau;
+      src -= (u[mu] * pc[pidx(nu, 0)] + u[nu] * pc[pidx(mu, 0)]) * DU[0] * gmn<real>(0, 0);
+      src -= (u[mu] * pc[pidx(nu, 1)] + u[nu] * pc[pidx(mu, 1)]) * DU[1] * gmn<real>(1, 1);
+      src -= (u[mu] * pc[pidx(nu, 2)] + u[nu] * pc[pidx(mu, 2)]) * DU[2] * gmn<real>(2, 2);
+      src -= (u[mu] * pc[pidx(nu, 3)] + u[nu] * pc[pidx(mu, 3)]) * DU[3] * gmn<real>(3, 3);
+      if (COUPLED && (p.flags & FLAG_GUBSER_VISC))
+        src -= one_over_taupi * coef_pipi *
+               (pipi<real>(0, mu, nu, pc, u) - pipi<real>(1, mu, nu, pc, u) - pipi<real>(2, mu, nu, pc, u) -
+                pipi<real>(3, mu, nu, pc, u));
+      if (COUPLED && (p.flags & FLAG_PIMN_OMEGA))
+        src += 2.0f * (pi_omega<real>(0, mu, nu, pc, Omega, u) - pi_omega<real>(1, mu, nu, pc, Omega, u) -
+                       pi_omega<real>(2, mu, nu, pc, Omega, u) - pi_omega<real>(3, mu, nu, pc, Omega, u));
+      if (COUPLED && (p.flags & FLAG_OMEGA_OMEGA))
+        src -= 1.0f * one_over_taupi *
+               (omega_omega<real>(0, mu, nu, Omega, u) - omega_omega<real>(1, mu, nu, Omega, u) -
+                omega_omega<real>(2, mu, nu, Omega, u) - omega_omega<real>(3, mu, nu, Omega, u));
+      S10[mn] += src;
+      pi_old = (pi_old + div_step(S10[mn] * p.DT, step) + p.DT * one_over_taupi * piNS) /
+               (u_new[0] + p.DT * one_over_taupi);
+      if (fabs(pi_old) > max_pimn_abs) max_pimn_abs = fabs(pi_old);
+      pinew[mn] = pi_old;
+    }
+  real pre = eosP<real>(p, e2s0);
+  real T00 = (e2s0 + pre) * u_new[0] * u_new[0] - pre;
+  uint8_t good = 1;
+  if (max_pimn_abs > T00) {
+#pragma unroll
+    for (int m = 0; m < 10; m++) pinew[m] = 0.0f;
+    good = 0;
+  }
+#pragma unroll
+  for (int m = 0; m < 10; m++) b.pinew[m * ld + I] = pinew[m];
+  b.goodcell[I] = good;
+}
+
+// update_ev (kernel_visc.cl:322-393) for cell I: pin = pi^{tau mu} at the
+// start of the step, S4 the KT sources; the new pi^{tau mu} comes from pinew
+// (fused pi update) or from pi_new_in. Also get_udiff and the edmax key.
+template <class real, bool FUSED_PI>
+__device__ __forceinline__ void ev_update(const Params& p, const ViscBuffers<real>& b, int step, real tau,
+                                          long long I, const real pin[4], const real S4[4], const real pinew[10]) {
+  const long long ld = p.ld;
+  const real acu = Acu<real>::v;
+  real e1[4];
+#pragma unroll
+  for (int c = 0; c < 4; c++) e1[c] = b.ev1[c * ld + I];
+  real ed = e1[0], vx = e1[1], vy = e1[2], vz = e1[3];
+  real pressure = eosP<real>(p, ed);
+  real u0 = gamma3<real>(vx, vy, vz);
+  real umu[4] = {u0 * 1.0f, u0 * vx, u0 * vy, u0 * vz};
+  real old_time = tau - (step - 1) * p.DT;
+  real T0m[4];
+#pragma unroll
+  for (int c = 0; c < 4; c++) {
+    real g0 = c == 0 ? (real)1.0f : (real)0.0f;
+    T0m[c] = ((ed + pressure) * u0 * umu[c] - pressure * g0 + pin[c]) * old_time;
+  }
+#pragma unroll
+  for (int c = 0; c < 4; c++) {
+    real pim2 = FUSED_PI ? pinew[c] : b.pi2in[c * ld + I];
+    T0m[c] = T0m[c] + div_step(S4[c] * p.DT, step) - pim2 * tau;
+  }
+  real T00 = cmax<real>(acu, T0m[0]) / tau;
+  real T01 = (fabs(T0m[1]) < acu) ? (real)0.0f : T0m[1] / tau;
+  real T02 = (fabs(T0m[2]) < acu) ? (real)0.0f : T0m[2] / tau;
+  real T03 = (fabs(T0m[3]) < acu) ? (real)0.0f : T0m[3] / tau;
+  real M = sqrt(T01 * T01 + T02 * T02 + T03 * T03);
+  real SCALE_COEF = 0.999f;
+  if (M > T00) {
+    T01 *= SCALE_COEF * T00 / M;
+    T02 *= SCALE_COEF * T00 / M;
+    T03 *= SCALE_COEF * T00 / M;
+    M = SCALE_COEF * T00;
+  }
+  real ed_find = root_newton<real>(p, T00, M);
+  if (ed_find < acu) {
+    T01 = 0.0f;
+    T02 = 0.0f;
+    T03 = 0.0f;
+  }
+  ed_find = cmax<real>(0.0f, ed_find);
+  real pr = eosP<real>(p, ed_find);
+  real epv = cmax<real>(acu, T00 + pr);
+  real en[4] = {ed_find, T01 / epv, T02 / epv, T03 / epv};
+#pragma unroll
+  for (int c = 0; c < 4; c++) b.evnew[c * ld + I] = en[c];
+  if (b.write_udiff) {  // get_udiff, kernel_IS.cl:714-724
+    real gn = gamma3<real>(en[1], en[2], en[3]);
+    real go = gamma3<real>(e1[1], e1[2], e1[3]);
+    b.udiff[0 * ld + I] = gn * 1.0f - go * 1.0f;
+    b.udiff[1 * ld + I] = gn * en[1] - go * e1[1];
+    b.udiff[2 * ld + I] = gn * en[2] - go * e1[2];
+    b.udiff[3 * ld + I] = gn * en[3] - go * e1[3];
+  }
+  if (b.edmax_key && en[0] == en[0]) atomicMax(b.edmax_key, fkey(en[0]));
+}
+
 // --------------------------------------------------------------- viscous
-template <class real, bool DO_IS, bool DO_KT>
+template <class real, bool DO_IS, bool DO_KT, bool COUPLED>
 __global__ void __launch_bounds__(128) visc_stage_kernel(Params p, ViscBuffers<real> b, int step, real tau) {
   const long long N = (long long)p.nx * p.ny * p.nz;
   const long long I = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -258,168 +434,9 @@ __global__ void __launch_bounds__(128) visc_stage_kernel(Params p, ViscBuffers<r
     }
   }
 
-  // ------------------------------------------------ pi update (update_pimn)
   real pinew[10];
-  if (DO_IS) {
-    real e1[4];
-#pragma unroll
-    for (int c = 0; c < 4; c++) e1[c] = b.ev1[c * ld + I];
-    real g1 = gamma3<real>(e1[1], e1[2], e1[3]);
-    real u_old[4] = {g1 * 1.0f, g1 * e1[1], g1 * e1[2], g1 * e1[3]};
-    real u_new[4], udt[4];
-    real e2s0;
-    if (step == 1) {
-#pragma unroll
-      for (int c = 0; c < 4; c++) {
-        real ud = b.udiff[c * ld + I];
-        udt[c] = ud / (real)p.DT;
-        u_new[c] = u_old[c] + ud;
-      }
-      e2s0 = b.ev2e[I];
-    } else {
-      real g2 = gamma3<real>(e0[1], e0[2], e0[3]);
-      u_new[0] = g2 * 1.0f;
-      u_new[1] = g2 * e0[1];
-      u_new[2] = g2 * e0[2];
-      u_new[3] = g2 * e0[3];
-#pragma unroll
-      for (int c = 0; c < 4; c++) udt[c] = (u_new[c] - u_old[c]) / (real)p.DT;
-      e2s0 = e0[0];
-    }
-    real da[4][4];
-#pragma unroll
-    for (int c = 0; c < 4; c++) {
-      da[c][0] = udt[c];
-      da[c][1] = grad[0][c];
-      da[c][2] = grad[1][c];
-      da[c][3] = grad[2][c];
-    }
-    real u[4], DU[4];
-#pragma unroll
-    for (int c = 0; c < 4; c++) u[c] = (step == 1) ? u_old[c] : u_new[c];
-#pragma unroll
-    for (int c = 0; c < 4; c++) DU[c] = dot4<real>(u, da[c]);
-    real ed_step = (step == 1) ? e1[0] : e2s0;
-    real theta = udt[0] + grad[0][1] + grad[1][2] + grad[2][3];
-    real temperature = eos_comp<real>(p, ed_step, 2);
-    real sdens = eos_comp<real>(p, ed_step, 3);
-    real local_etaos = etaos<real>(p, temperature);
-    real etav = local_etaos * sdens * CLV_HBARC;
-    real one_over_taupi = temperature / (3.0f * cmax<real>(acu, local_etaos) * CLV_HBARC);
-    real coef_pipi = 0.0f;
-    if (p.flags & FLAG_GUBSER_VISC) {  // kernel_IS.cl:581-590
-      real ETAOS = p.ETAOS_YMIN;
-      real etavH = ETAOS * 4.0f / 3.0f;
-      real taupiH = p.LAM1 * p.LAM1 * etavH / 3.0f;
-      one_over_taupi = 1.0f / (taupiH * pow(ed_step, (real)-0.25f));
-      coef_pipi = p.LAM1 / ed_step;
-      etav = ETAOS * 4.0f / 3.0f * pow(ed_step, (real)0.75f);
-    }
-    real Omega[6] = {0, 0, 0, 0, 0, 0};
-    if (p.flags & (FLAG_PIMN_OMEGA | FLAG_OMEGA_OMEGA)) omega_tensor<real>(udt, grad, u, Omega);
-
-    real max_pimn_abs = 0.0f;
-#pragma unroll
-    for (int mu = 0; mu < 4; mu++)
-#pragma unroll
-      for (int nu = mu; nu < 4; nu++) {
-        real gmu[4] = {gmn<real>(mu, 0), gmn<real>(mu, 1), gmn<real>(mu, 2), gmn<real>(mu, 3)};
-        real gnu[4] = {gmn<real>(nu, 0), gmn<real>(nu, 1), gmn<real>(nu, 2), gmn<real>(nu, 3)};
-        real sigma = dot4<real>(gmu, da[nu]) + dot4<real>(gnu, da[mu]) - (u[mu] * DU[nu] + u[nu] * DU[mu]) -
-                     2.0f / 3.0f * (gmn<real>(mu, nu) - u[mu] * u[nu]) * theta;
-        const int mn = pidx(mu, nu);
-        if (u[0] > 10000.0f) sigma = 0.0f;
-        real piNS = etav * sigma;
-        real pi_old = b.pi1[mn * ld + I] * u_old[0];
-        real src = -pc[mn] * theta / 3.0f - pc[mn] * u[0] / tau;
-        src -= (u[mu] * pc[pidx(nu, 0)] + u[nu] * pc[pidx(mu, 0)]) * DU[0] * gmn<real>(0, 0);
-        src -= (u[mu] * pc[pidx(nu, 1)] + u[nu] * pc[pidx(mu, 1)]) * DU[1] * gmn<real>(1, 1);
-        src -= (u[mu] * pc[pidx(nu, 2)] + u[nu] * pc[pidx(mu, 2)]) * DU[2] * gmn<real>(2, 2);
-        src -= (u[mu] * pc[pidx(nu, 3)] + u[nu] * pc[pidx(mu, 3)]) * DU[3] * gmn<real>(3, 3);
-        if (p.flags & FLAG_GUBSER_VISC)
-          src -= one_over_taupi * coef_pipi *
-                 (pipi<real>(0, mu, nu, pc, u) - pipi<real>(1, mu, nu, pc, u) - pipi<real>(2, mu, nu, pc, u) -
-                  pipi<real>(3, mu, nu, pc, u));
-        if (p.flags & FLAG_PIMN_OMEGA)
-          src += 2.0f * (pi_omega<real>(0, mu, nu, pc, Omega, u) - pi_omega<real>(1, mu, nu, pc, Omega, u) -
-                         pi_omega<real>(2, mu, nu, pc, Omega, u) - pi_omega<real>(3, mu, nu, pc, Omega, u));
-        if (p.flags & FLAG_OMEGA_OMEGA)
-          src -= 1.0f * one_over_taupi *
-                 (omega_omega<real>(0, mu, nu, Omega, u) - omega_omega<real>(1, mu, nu, Omega, u) -
-                  omega_omega<real>(2, mu, nu, Omega, u) - omega_omega<real>(3, mu, nu, Omega, u));
-        S10[mn] += src;
-        pi_old = (pi_old + S10[mn] * p.DT / step + p.DT * one_over_taupi * piNS) / (u_new[0] + p.DT * one_over_taupi);
-        if (fabs(pi_old) > max_pimn_abs) max_pimn_abs = fabs(pi_old);
-        pinew[mn] = pi_old;
-      }
-    real pre = eosP<real>(p, e2s0);
-    real T00 = (e2s0 + pre) * u_new[0] * u_new[0] - pre;
-    uint8_t good = 1;
-    if (max_pimn_abs > T00) {
-#pragma unroll
-      for (int m = 0; m < 10; m++) pinew[m] = 0.0f;
-      good = 0;
-    }
-#pragma unroll
-    for (int m = 0; m < 10; m++) b.pinew[m * ld + I] = pinew[m];
-    b.goodcell[I] = good;
-  }
-
-  // ------------------------------------------- T^{tau mu} update (update_ev)
-  if (DO_KT) {
-    real e1[4];
-#pragma unroll
-    for (int c = 0; c < 4; c++) e1[c] = b.ev1[c * ld + I];
-    real ed = e1[0], vx = e1[1], vy = e1[2], vz = e1[3];
-    real pressure = eosP<real>(p, ed);
-    real u0 = gamma3<real>(vx, vy, vz);
-    real umu[4] = {u0 * 1.0f, u0 * vx, u0 * vy, u0 * vz};
-    real old_time = tau - (step - 1) * p.DT;
-    real T0m[4];
-#pragma unroll
-    for (int c = 0; c < 4; c++) {
-      real g0 = c == 0 ? (real)1.0f : (real)0.0f;
-      T0m[c] = ((ed + pressure) * u0 * umu[c] - pressure * g0 + pin[c]) * old_time;
-    }
-#pragma unroll
-    for (int c = 0; c < 4; c++) {
-      real pim2 = DO_IS ? pinew[c] : b.pi2in[c * ld + I];
-      T0m[c] = T0m[c] + S4[c] * p.DT / step - pim2 * tau;
-    }
-    real T00 = cmax<real>(acu, T0m[0]) / tau;
-    real T01 = (fabs(T0m[1]) < acu) ? (real)0.0f : T0m[1] / tau;
-    real T02 = (fabs(T0m[2]) < acu) ? (real)0.0f : T0m[2] / tau;
-    real T03 = (fabs(T0m[3]) < acu) ? (real)0.0f : T0m[3] / tau;
-    real M = sqrt(T01 * T01 + T02 * T02 + T03 * T03);
-    real SCALE_COEF = 0.999f;
-    if (M > T00) {
-      T01 *= SCALE_COEF * T00 / M;
-      T02 *= SCALE_COEF * T00 / M;
-      T03 *= SCALE_COEF * T00 / M;
-      M = SCALE_COEF * T00;
-    }
-    real ed_find = root_newton<real>(p, T00, M);
-    if (ed_find < acu) {
-      T01 = 0.0f;
-      T02 = 0.0f;
-      T03 = 0.0f;
-    }
-    ed_find = cmax<real>(0.0f, ed_find);
-    real pr = eosP<real>(p, ed_find);
-    real epv = cmax<real>(acu, T00 + pr);
-    real en[4] = {ed_find, T01 / epv, T02 / epv, T03 / epv};
-#pragma unroll
-    for (int c = 0; c < 4; c++) b.evnew[c * ld + I] = en[c];
-    if (b.write_udiff) {  // get_udiff, kernel_IS.cl:714-724
-      real gn = gamma3<real>(en[1], en[2], en[3]);
-      real go = gamma3<real>(e1[1], e1[2], e1[3]);
-      b.udiff[0 * ld + I] = gn * 1.0f - go * 1.0f;
-      b.udiff[1 * ld + I] = gn * en[1] - go * e1[1];
-      b.udiff[2 * ld + I] = gn * en[2] - go * e1[2];
-      b.udiff[3 * ld + I] = gn * en[3] - go * e1[3];
-    }
-    if (b.edmax_key && en[0] == en[0]) atomicMax(b.edmax_key, fkey(en[0]));
-  }
+  if (DO_IS) pi_update<real, COUPLED>(p, b, step, tau, I, e0, pc, grad, S10, pinew);
+  if (DO_KT) ev_update<real, DO_IS>(p, b, step, tau, I, pin, S4, pinew);
 
   if (b.write_src) {
     if (DO_KT)
@@ -536,7 +553,7 @@ __global__ void __launch_bounds__(128) ideal_stage_kernel(Params p, IdealBuffers
     real g0 = c == 0 ? (real)1.0f : (real)0.0f;
     T0m[c] = (ed + pressure) * u0 * umu[c] - pressure * g0;
     if (!riemann) T0m[c] = T0m[c] * old_time;
-    T0m[c] = T0m[c] + S[c] * p.DT / step;
+    T0m[c] = T0m[c] + div_step(S[c] * p.DT, step);
   }
   real T00, T01, T02, T03;
   if (riemann) {

@@ -81,6 +81,16 @@ typedef struct clv_visc_buffers {
   int write_udiff;       /* step 2 only: udiff = u(ev_new) - u(ev1)            */
 } clv_visc_buffers;
 
+/* Tuning options (process-wide): the viscous-stage kernel variant
+ * (0 = tiled, the default; 1 = one thread per cell without shared memory),
+ * the number of x planes a tiled thread block marches through, and the
+ * number of tiled blocks kept resident per SM in FP32 (1 or 2; FP64 uses 1).
+ * Every variant computes the same values bit for bit. */
+#define CLV_OPT_STAGE_KERNEL 1
+#define CLV_OPT_CHUNK 2
+#define CLV_OPT_TILED_BLOCKS 3
+int clv_set_option(int option, int value);
+
 /* Library version; the low 8 bits bump on any ABI change. */
 int clv_version(void);
 /* One-line description of the last error on this thread ("" if none). */

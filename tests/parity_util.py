@@ -22,6 +22,7 @@ def make_cfg(nx, ny, nz, use_float32=True, eos_type='lattice_pce165', dx=0.3, dz
     cfg.fPathOut = out
     for k, v in extra.items():
         setattr(cfg, k, v)
+    cfg.BSZ = 64
     from clvisc_b200.config import set_real
     return set_real(cfg)
 

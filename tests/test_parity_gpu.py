@@ -75,8 +75,8 @@ def test_visc_construction_parity(cuda_lib, oracle_mod, use_float32):
 
 
 @pytest.mark.parametrize('use_float32', [True, False])
-@pytest.mark.parametrize('grid', [(15, 13, 11), (19, 17, 1)])
-def test_visc_parts_parity(cuda_lib, oracle_mod, use_float32, grid):
+@pytest.mark.parametrize('grid', [(15, 13, 11), (19, 17, 1), (34, 9, 41)])
+def test_visc_parts_parity(cuda_lib, oracle_mod, use_float32, grid, stage_variant):
     """Separate IS_stepUpdate / visc_stepUpdate launches, reference order."""
     from clvisc_b200.visc import CLVisc
     cfg = make_cfg(*grid, use_float32=use_float32)
@@ -93,9 +93,23 @@ def test_visc_parts_parity(cuda_lib, oracle_mod, use_float32, grid):
         _compare_visc(v, o, 'parts n=%d' % n)
 
 
+@pytest.fixture(params=['tiled', 'tiled-1blk', 'tiled-chunk5', 'per-cell'])
+def stage_variant(request, cuda_lib):
+    """Every viscous-stage kernel variant; restores the default afterwards."""
+    from clvisc_b200 import _lib
+    opts = {'tiled': [], 'tiled-1blk': [(_lib.CLV_OPT_TILED_BLOCKS, 1)], 'tiled-chunk5': [(_lib.CLV_OPT_CHUNK, 5)],
+            'per-cell': [(_lib.CLV_OPT_STAGE_KERNEL, 1)]}[request.param]
+    for o, v in opts:
+        _lib.set_option(o, v)
+    yield request.param
+    _lib.set_option(_lib.CLV_OPT_STAGE_KERNEL, 0)
+    _lib.set_option(_lib.CLV_OPT_CHUNK, 32)
+    _lib.set_option(_lib.CLV_OPT_TILED_BLOCKS, 2)
+
+
 @pytest.mark.parametrize('use_float32', [True, False])
-@pytest.mark.parametrize('grid', [(15, 13, 11), (21, 19, 1), (9, 1, 13)])
-def test_visc_fused_step_parity(cuda_lib, oracle_mod, use_float32, grid):
+@pytest.mark.parametrize('grid', [(15, 13, 11), (21, 19, 1), (9, 1, 13), (40, 37, 35)])
+def test_visc_fused_step_parity(cuda_lib, oracle_mod, use_float32, grid, stage_variant):
     """The fused per-stage kernel of evolve() against the reference order."""
     from clvisc_b200.visc import CLVisc
     cfg = make_cfg(*grid, use_float32=use_float32)
@@ -176,3 +190,45 @@ def test_layout_roundtrip_and_max(cuda_lib):
     g.load_ini(x)
     assert g.max_energy_density() == x[:, 0].max()
     torch.cuda.synchronize()
+
+
+@pytest.mark.parametrize('use_float32', [True, False])
+def test_visc_couplings_parity(cuda_lib, oracle_mod, use_float32, stage_variant):
+    """PIMUNU_OMEGA_COUPLING and OMEGA_OMEGA_COUPLING (kernel_IS.cl:636-683):
+    rational arithmetic only, so bit for bit."""
+    from clvisc_b200.visc import CLVisc
+    cfg = make_cfg(17, 15, 13, use_float32=use_float32, pimn_omega_coupling=True, omega_omega_coupling=True)
+    ic = seeded_ic(cfg, seed=21, flow=0.3)
+    v = CLVisc(cfg)
+    o = oracle_mod.OracleVisc(cfg)
+    v.load_ini(ic)
+    o.load_ini(ic)
+    for n in range(4):
+        v.step(n)
+        o.step(n)
+    assert_same('ev[1]', v.ideal.field_to_host(v.ideal.d_ev[1]), o.ideal.d_ev[1])
+    assert_same('pi[1]', v.ideal.field_to_host(v.d_pi[1]), o.d_pi[1])
+
+
+@pytest.mark.parametrize('use_float32', [True, False])
+def test_visc_gubser_flag_parity(cuda_lib, oracle_mod, use_float32):
+    """GUBSER_VISC_TEST terms (kernel_IS.cl:581-590, 629-634) use pow(), whose
+    last bit differs between the device and host libraries: fields agree to
+    1e-5 (FP32) / 1e-11 (FP64) relative after 4 steps."""
+    from clvisc_b200.visc import CLVisc
+    cfg = make_cfg(17, 15, 1, use_float32=use_float32, eos_type='ideal_gas', gubser_visc_test=True, LAM1=-10.0,
+                   etaos=0.2)
+    ic = seeded_ic(cfg, seed=23)
+    v = CLVisc(cfg)
+    o = oracle_mod.OracleVisc(cfg)
+    v.load_ini(ic)
+    o.load_ini(ic)
+    for n in range(4):
+        v.step(n)
+        o.step(n)
+    rtol = 1e-5 if use_float32 else 1e-11
+    for name, g, w in (('ev', v.ideal.field_to_host(v.ideal.d_ev[1]), o.ideal.d_ev[1]),
+                       ('pi', v.ideal.field_to_host(v.d_pi[1]), o.d_pi[1])):
+        scale = np.abs(w).max(axis=0, keepdims=True) + 1e-30
+        err = np.abs(g.astype(np.float64) - w) / scale
+        assert err.max() <= rtol, (name, err.max())
