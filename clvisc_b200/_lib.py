@@ -79,6 +79,8 @@ _SIGS = {
     'clv_hypersf_scratch_bytes': ([_P], ctypes.c_size_t),
     'clv_hypersf_append': ([_P, ctypes.c_int, ctypes.c_double, ctypes.c_double, _VP, _VP, _VP, _VP, _VP, _VP, _VP,
                             ctypes.c_longlong, _VP, _VP, ctypes.c_size_t, _VP], ctypes.c_int),
+    'clv_hypersf_append_noalloc': ([_P, ctypes.c_int, ctypes.c_double, ctypes.c_double, _VP, _VP, _VP, _VP, _VP,
+                                    _VP, _VP, ctypes.c_longlong, _VP, _VP], ctypes.c_int),
     'clv_aos_to_soa': ([_P, _VP, _VP, ctypes.c_longlong, ctypes.c_int, _VP], ctypes.c_int),
     'clv_soa_to_aos': ([_P, _VP, _VP, ctypes.c_longlong, ctypes.c_int, _VP], ctypes.c_int),
 }

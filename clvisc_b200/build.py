@@ -14,8 +14,9 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, 'libclvisc_b200.so')
-SOURCES = ['csrc/clv_capi.cu']
-DEPS = ['csrc/clv_device.cuh', 'csrc/clv_stage.cuh', 'csrc/clv_misc.cuh', 'csrc/clv_hypersf.cuh',
+SOURCES = ['csrc/clv_capi.cu', 'csrc/clv_noalloc.cu']
+DEPS = ['csrc/clv_device.cuh', 'csrc/clv_stage.cuh', 'csrc/clv_stage_tiled.cuh', 'csrc/clv_misc.cuh',
+        'csrc/clv_hypersf.cuh',
         '../include/clvisc_b200.h']
 
 NVCC_FLAGS = [

@@ -11,9 +11,13 @@
 #include "clv_stage.cuh"
 #include "clv_stage_tiled.cuh"
 
+namespace clv_host {
+thread_local std::string g_err;  // message behind clv_last_error()
+}
+using clv_host::g_err;
+
 namespace {
 
-thread_local std::string g_err;
 int g_stage_kernel = 0;  // CLV_OPT_STAGE_KERNEL: 0 tiled, 1 per-cell
 int g_chunk = 32;        // CLV_OPT_CHUNK: x planes per tiled CTA
 int g_minb = 2;          // CLV_OPT_TILED_BLOCKS: resident tiled CTAs per SM (FP32)

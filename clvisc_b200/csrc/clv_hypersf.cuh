@@ -249,6 +249,7 @@ __global__ void hsf_mark_kernel(Params p, const real* ev_old, const real* ev_new
   if (threadIdx.x == 0) block_count[blockIdx.x] = c;
 }
 
+#ifndef CLV_HSF_NO_SHARED_KERNELS
 // pass 2: exclusive scan of the block counts in one block; total -> *total
 __global__ void hsf_scan_kernel(int* block_count, int nblocks, long long* total) {
   __shared__ long long warp_sum[32];
@@ -300,6 +301,8 @@ __global__ void hsf_compact_kernel(long long ncube, const uint8_t* mark, const i
   for (int u = 0; u < w; u++) wbase += warp_tot[u];
   if (m) list[block_offset[blockIdx.x] + wbase + before] = (int)q;
 }
+
+#endif  // CLV_HSF_NO_SHARED_KERNELS
 
 // pass 4: one thread per emitted element
 template <class real>
@@ -374,6 +377,8 @@ __global__ void hsf_element_kernel(Params p, const real* ev_old, const real* ev_
   }
 }
 
+#ifndef CLV_HSF_NO_SHARED_KERNELS
 __global__ void hsf_advance_kernel(const long long* count, long long* total_inout) { *total_inout += *count; }
+#endif
 
 }  // namespace clv

@@ -144,6 +144,23 @@ int clv_hypersf_append(const clv_params *p, int visc, double tau_old, double tau
                        const void *ev_new, const void *pi_old, const void *pi_new, void *sf, void *txyz, void *pisf,
                        long long capacity, long long *total, void *scratch, size_t scratch_bytes, void *stream);
 
+/* clv_hypersf_append without the scratch argument, for callers that cannot
+ * allocate device memory: an application whose memory pool owns the device
+ * and lets no library allocate, or a time-critical loop where a cudaMalloc
+ * (which may synchronise the device) is not acceptable. It has no counterpart
+ * in the reference. Its scratch is a fixed array inside the library (about
+ * 1 MB, held on every GPU that loads the library until the process exits),
+ * which limits a call to 2^26 coarse cubes, ((NX-1)/nxskip+1) *
+ * ((NY-1)/nyskip+1) * ((NZ-1)/nzskip+1); larger grids return
+ * CLV_ERR_INVALID. It appends the same elements, in the same order, as
+ * clv_hypersf_append. All calls share that array: calls whose launches overlap
+ * on the GPU race, so serialise them. The first call on each device looks up
+ * the array's device address (with that device current); make that first call
+ * before any stream capture. Nothing is allocated or freed. */
+int clv_hypersf_append_noalloc(const clv_params *p, int visc, double tau_old, double tau_new, const void *ev_old,
+                               const void *ev_new, const void *pi_old, const void *pi_new, void *sf, void *txyz,
+                               void *pisf, long long capacity, long long *total, void *stream);
+
 /* Host-boundary layout transposes: (n, w) row-major <-> w planes of ld. */
 int clv_aos_to_soa(const clv_params *p, const void *aos, void *soa, long long n, int w, void *stream);
 int clv_soa_to_aos(const clv_params *p, const void *soa, void *aos, long long n, int w, void *stream);
