@@ -63,7 +63,38 @@ int to_params(const clv_params* in, clv::Params* out) {
   p.eos_num = in->eos_num_ed; p.eos_nrow = in->eos_nrow; p.eos_ncol = in->eos_ncol;
   p.eos = in->eos_table;
   p.flags = in->flags;
+  // correctly rounded reciprocals in each precision (host IEEE arithmetic, no
+  // contraction): the kernels divide by these constants with clv::div_by
+  const float epr = in->eos_ed_step * in->eos_ncol;  // as the kernels form it
+  p.rf.eos_step = 1.0f / in->eos_ed_step;
+  p.rf.eos_epr = 1.0f / epr;
+  p.rf.DT = 1.0f / in->dt;
+  p.rf.DX = 1.0f / in->dx;
+  p.rf.DY = 1.0f / in->dy;
+  p.rf.DZ = 1.0f / in->dz;
+  p.rf.three = 1.0f / 3.0f;
+  p.rd.eos_step = 1.0 / (double)in->eos_ed_step;
+  p.rd.eos_epr = 1.0 / (double)epr;
+  p.rd.DT = 1.0 / (double)in->dt;
+  p.rd.DX = 1.0 / (double)in->dx;
+  p.rd.DY = 1.0 / (double)in->dy;
+  p.rd.DZ = 1.0 / (double)in->dz;
+  p.rd.three = 1.0 / 3.0;
+  if (!(in->dt > 0.0f) || !(in->dx > 0.0f) || !(in->dy > 0.0f) || !(in->dz > 0.0f))
+    return fail(CLV_ERR_INVALID, "dt, dx, dy, dz must be > 0%s");
   return CLV_OK;
+}
+
+// tau of a stage launch in the run precision, DZ*tau as the kernels form it,
+// and the correctly rounded reciprocals of both
+template <class real>
+clv::TauConst<real> tau_const(const clv::Params& p, double tau_d) {
+  clv::TauConst<real> t;
+  t.tau = (real)tau_d;
+  t.rtau = (real)1 / t.tau;
+  t.dzt = (real)p.DZ * t.tau;
+  t.rdzt = (real)1 / t.dzt;
+  return t;
 }
 inline long long ncell(const clv::Params& p) { return (long long)p.nx * p.ny * p.nz; }
 inline unsigned int nblk(long long n, int bs) { return (unsigned int)((n + bs - 1) / bs); }
@@ -81,7 +112,7 @@ int launch_tiled_b(const clv::Params& p, const clv::ViscBuffers<real>& v, int st
   }
   const int chunk = g_chunk;
   dim3 grid((p.nz + TK - 1) / TK, (p.ny + TJ - 1) / TJ, (p.nx + chunk - 1) / chunk);
-  kern<<<grid, TJ * TK, sizeof(SM), s>>>(p, v, step, (real)tau, chunk);
+  kern<<<grid, TJ * TK, sizeof(SM), s>>>(p, v, step, tau_const<real>(p, tau), chunk);
   return cuda_check("visc_stage_tiled_kernel");
 }
 
@@ -119,7 +150,7 @@ int visc_stage_t(const clv::Params& p, int step, double tau, int parts, const cl
   }
   const int bs = 128;
   dim3 grid(nblk(ncell(p), bs));
-  real t = (real)tau;
+  const clv::TauConst<real> t = tau_const<real>(p, tau);
   const bool cpl = p.flags & (clv::FLAG_GUBSER_VISC | clv::FLAG_PIMN_OMEGA | clv::FLAG_OMEGA_OMEGA);
   if (is && kt && cpl) clv::visc_stage_kernel<real, true, true, true><<<grid, bs, 0, s>>>(p, v, step, t);
   else if (is && kt) clv::visc_stage_kernel<real, true, true, false><<<grid, bs, 0, s>>>(p, v, step, t);
@@ -136,7 +167,7 @@ int ideal_stage_t(const clv::Params& p, int step, double tau, const void* ev_st,
   b.ev_st = (const real*)ev_st; b.ev1 = (const real*)ev1; b.evnew = (real*)ev_new; b.src = (real*)src;
   b.edmax_key = (typename clv::KeyT<real>::type*)key; b.write_src = write_src;
   const int bs = 128;
-  clv::ideal_stage_kernel<real><<<nblk(ncell(p), bs), bs, 0, s>>>(p, b, step, (real)tau);
+  clv::ideal_stage_kernel<real><<<nblk(ncell(p), bs), bs, 0, s>>>(p, b, step, tau_const<real>(p, tau));
   return cuda_check("ideal_stage_kernel");
 }
 

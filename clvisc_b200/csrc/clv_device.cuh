@@ -12,6 +12,13 @@
 
 namespace clv {
 
+// correctly rounded reciprocals of run constants in one precision
+template <class real> struct Recips {
+  real eos_step, eos_epr;  // EOS grid step and energy density per image row
+  real DT, DX, DY, DZ;     // DT, DX, DY, DZ as reals
+  real three;              // 3
+};
+
 // run constants, passed by value to every kernel
 struct Params {
   int nx, ny, nz;
@@ -24,6 +31,17 @@ struct Params {
   int eos_num, eos_nrow, eos_ncol;
   const float* eos;  // nrow*ncol texels of (cs2, p, T, s)
   int flags;
+  Recips<float> rf;   // reciprocals for float kernels
+  Recips<double> rd;  // reciprocals for double kernels
+};
+template <class real> __device__ __forceinline__ const Recips<real>& recips(const Params& p);
+template <> __device__ __forceinline__ const Recips<float>& recips<float>(const Params& p) { return p.rf; }
+template <> __device__ __forceinline__ const Recips<double>& recips<double>(const Params& p) { return p.rd; }
+
+// tau-dependent divisors of one stage launch and their reciprocals
+template <class real> struct TauConst {
+  real tau, rtau;  // tau, 1/tau
+  real dzt, rdzt;  // DZ*tau, 1/(DZ*tau)
 };
 
 enum : int {
@@ -47,6 +65,36 @@ template <class real> __device__ __forceinline__ real csign(real x) {
   return x > (real)0 ? (real)1 : (x < (real)0 ? (real)-1 : (x != x ? (real)0 : x));
 }
 
+// ------------------------------------------------------- exact division
+// a/b rounded to nearest (the IEEE quotient) from y = RN(1/b), by Markstein's
+// method (P. Markstein, IBM J. Res. Dev. 34 (1990) 111): q = RN(a*y) is within
+// a few ulps of a/b, r = a - b*q is formed exactly with a fused multiply-add,
+// and q + r*y rounded once corrects q; applied twice, the second correction
+// starts from a faithful quotient, for which the theorem gives the correctly
+// rounded a/b when nothing under- or overflows. Outside the range where that
+// holds (|a| below 2^-80 / 2^-900 or above 2^80 / 2^900, infinities, NaN) the
+// IEEE division is used; a = 0 gives a*y, the correctly signed zero. Only used
+// with divisors and reciprocals that are normal numbers well inside the range.
+template <class real> struct DivRange;
+template <> struct DivRange<float> {
+  static constexpr float lo = 0x1p-80f, hi = 0x1p+80f;
+};
+template <> struct DivRange<double> {
+  static constexpr double lo = 0x1p-900, hi = 0x1p+900;
+};
+static __device__ __noinline__ float ieee_div(float a, float b) { return a / b; }
+static __device__ __noinline__ double ieee_div(double a, double b) { return a / b; }
+template <class real> __device__ __forceinline__ real div_by(real a, real b, real y) {
+  real q0 = a * y;
+  real r = fma(-q0, b, a);
+  real q = fma(r, y, q0);
+  r = fma(-q, b, a);
+  q = fma(r, y, q);
+  real aa = fabs(a);
+  if (!(aa >= DivRange<real>::lo && aa <= DivRange<real>::hi)) q = (a == (real)0) ? q0 : ieee_div(a, b);
+  return q;
+}
+
 // x / step for the Runge-Kutta stage index step (1 or 2): dividing by 1 or 2
 // is exact, as is multiplying by 1 or 0.5, so this equals the division bit for
 // bit (subnormal results included)
@@ -59,9 +107,10 @@ template <class real> __device__ __forceinline__ real div_step(real x, int step)
 // nearest texels (the second wraps to the next row), clamp-to-edge, lerp.
 template <class real>
 __device__ __forceinline__ real eos_comp(const Params& p, real eps, int c) {
+  const Recips<real>& rc = recips<real>(p);
   real ed_per_row = p.eos_step * p.eos_ncol;
-  int row = (int)(eps / ed_per_row);
-  int col = (int)((eps - p.eos_start - row * ed_per_row) / p.eos_step);
+  int row = (int)div_by<real>(eps, ed_per_row, rc.eos_epr);
+  int col = (int)div_by<real>(eps - p.eos_start - row * ed_per_row, (real)p.eos_step, rc.eos_step);
   real eps_low = p.eos_start + row * ed_per_row + col * p.eos_step;
   int col2 = col + 1, row2 = row;
   if (col2 == p.eos_ncol) {
@@ -72,7 +121,7 @@ __device__ __forceinline__ real eos_comp(const Params& p, real eps, int c) {
   int c1 = min(max(col2, 0), p.eos_ncol - 1), r1 = min(max(row2, 0), p.eos_nrow - 1);
   float lo = __ldg(p.eos + 4 * ((long long)r0 * p.eos_ncol + c0) + c);
   float hi = __ldg(p.eos + 4 * ((long long)r1 * p.eos_ncol + c1) + c);
-  real r = (eps - eps_low) / p.eos_step;
+  real r = div_by<real>(eps - eps_low, (real)p.eos_step, rc.eos_step);
   return (real)(1.0f - r) * (real)lo + r * (real)hi;
 }
 template <class real> __device__ __forceinline__ bool eos_in_table(const Params& p, real eps) {

@@ -64,11 +64,13 @@ __device__ __forceinline__ Stencil make_stencil(int q, int L, long long stride) 
 // input ev and pi at the cell, grad the velocity gradients, S10 the IS sources
 // (updated in place); writes pi_new and goodcell, returns the new pi in pinew.
 template <class real, bool COUPLED>
-__device__ __forceinline__ void pi_update(const Params& p, const ViscBuffers<real>& b, int step, real tau,
-                                          long long I, const real e0[4], const real pc[10], const real grad[3][4],
-                                          real S10[10], real pinew[10]) {
+__device__ __forceinline__ void pi_update(const Params& p, const ViscBuffers<real>& b, int step,
+                                          const TauConst<real>& tc, long long I, const real e0[4], const real pc[10],
+                                          const real grad[3][4], real S10[10], real pinew[10]) {
   const long long ld = p.ld;
   const real acu = Acu<real>::v;
+  const real tau = tc.tau;
+  const Recips<real>& rc = recips<real>(p);
   real e1[4];
 #pragma unroll
   for (int c = 0; c < 4; c++) e1[c] = b.ev1[c * ld + I];
@@ -80,7 +82,7 @@ __device__ __forceinline__ void pi_update(const Params& p, const ViscBuffers<rea
 #pragma unroll
     for (int c = 0; c < 4; c++) {
       real ud = b.udiff[c * ld + I];
-      udt[c] = ud / (real)p.DT;
+      udt[c] = div_by<real>(ud, (real)p.DT, rc.DT);
       u_new[c] = u_old[c] + ud;
     }
     e2s0 = b.ev2e[I];
@@ -91,7 +93,7 @@ __device__ __forceinline__ void pi_update(const Params& p, const ViscBuffers<rea
     u_new[2] = g2 * e0[2];
     u_new[3] = g2 * e0[3];
 #pragma unroll
-    for (int c = 0; c < 4; c++) udt[c] = (u_new[c] - u_old[c]) / (real)p.DT;
+    for (int c = 0; c < 4; c++) udt[c] = div_by<real>(u_new[c] - u_old[c], (real)p.DT, rc.DT);
     e2s0 = e0[0];
   }
   real da[4][4];
@@ -126,6 +128,9 @@ __device__ __forceinline__ void pi_update(const Params& p, const ViscBuffers<rea
   real Omega[6] = {0, 0, 0, 0, 0, 0};
   if (COUPLED && (p.flags & (FLAG_PIMN_OMEGA | FLAG_OMEGA_OMEGA))) omega_tensor<real>(udt, grad, u, Omega);
 
+  // the implicit update's denominator, shared by the ten components
+  const real den = u_new[0] + p.DT * one_over_taupi;
+  const real rden = (real)1.0f / den;
   real max_pimn_abs = 0.0f;
 #pragma unroll
   for (int mu = 0; mu < 4; mu++)
@@ -139,7 +144,7 @@ __device__ __forceinline__ void pi_update(const Params& p, const ViscBuffers<rea
       if (u[0] > 10000.0f) sigma = 0.0f;
       real piNS = etav * sigma;
       real pi_old = b.pi1[mn * ld + I] * u_old[0];
-      real src = -pc[mn] * theta / 3.0f - pc[mn] * u[0] / tau;
+      real src = div_by<real>(-pc[mn] * theta, (real)3.0f, rc.three) - div_by<real>(pc[mn] * u[0], tau, tc.rtau);
       src -= (u[mu] * pc[pidx(nu, 0)] + u[nu] * pc[pidx(mu, 0)]) * DU[0] * gmn<real>(0, 0);
       src -= (u[mu] * pc[pidx(nu, 1)] + u[nu] * pc[pidx(mu, 1)]) * DU[1] * gmn<real>(1, 1);
       src -= (u[mu] * pc[pidx(nu, 2)] + u[nu] * pc[pidx(mu, 2)]) * DU[2] * gmn<real>(2, 2);
@@ -156,8 +161,7 @@ __device__ __forceinline__ void pi_update(const Params& p, const ViscBuffers<rea
                (omega_omega<real>(0, mu, nu, Omega, u) - omega_omega<real>(1, mu, nu, Omega, u) -
                 omega_omega<real>(2, mu, nu, Omega, u) - omega_omega<real>(3, mu, nu, Omega, u));
       S10[mn] += src;
-      pi_old = (pi_old + div_step(S10[mn] * p.DT, step) + p.DT * one_over_taupi * piNS) /
-               (u_new[0] + p.DT * one_over_taupi);
+      pi_old = div_by<real>(pi_old + div_step(S10[mn] * p.DT, step) + p.DT * one_over_taupi * piNS, den, rden);
       if (fabs(pi_old) > max_pimn_abs) max_pimn_abs = fabs(pi_old);
       pinew[mn] = pi_old;
     }
@@ -178,10 +182,12 @@ __device__ __forceinline__ void pi_update(const Params& p, const ViscBuffers<rea
 // start of the step, S4 the KT sources; the new pi^{tau mu} comes from pinew
 // (fused pi update) or from pi_new_in. Also get_udiff and the edmax key.
 template <class real, bool FUSED_PI>
-__device__ __forceinline__ void ev_update(const Params& p, const ViscBuffers<real>& b, int step, real tau,
-                                          long long I, const real pin[4], const real S4[4], const real pinew[10]) {
+__device__ __forceinline__ void ev_update(const Params& p, const ViscBuffers<real>& b, int step,
+                                          const TauConst<real>& tc, long long I, const real pin[4], const real S4[4],
+                                          const real pinew[10]) {
   const long long ld = p.ld;
   const real acu = Acu<real>::v;
+  const real tau = tc.tau;
   real e1[4];
 #pragma unroll
   for (int c = 0; c < 4; c++) e1[c] = b.ev1[c * ld + I];
@@ -201,10 +207,10 @@ __device__ __forceinline__ void ev_update(const Params& p, const ViscBuffers<rea
     real pim2 = FUSED_PI ? pinew[c] : b.pi2in[c * ld + I];
     T0m[c] = T0m[c] + div_step(S4[c] * p.DT, step) - pim2 * tau;
   }
-  real T00 = cmax<real>(acu, T0m[0]) / tau;
-  real T01 = (fabs(T0m[1]) < acu) ? (real)0.0f : T0m[1] / tau;
-  real T02 = (fabs(T0m[2]) < acu) ? (real)0.0f : T0m[2] / tau;
-  real T03 = (fabs(T0m[3]) < acu) ? (real)0.0f : T0m[3] / tau;
+  real T00 = div_by<real>(cmax<real>(acu, T0m[0]), tau, tc.rtau);
+  real T01 = (fabs(T0m[1]) < acu) ? (real)0.0f : div_by<real>(T0m[1], tau, tc.rtau);
+  real T02 = (fabs(T0m[2]) < acu) ? (real)0.0f : div_by<real>(T0m[2], tau, tc.rtau);
+  real T03 = (fabs(T0m[3]) < acu) ? (real)0.0f : div_by<real>(T0m[3], tau, tc.rtau);
   real M = sqrt(T01 * T01 + T02 * T02 + T03 * T03);
   real SCALE_COEF = 0.999f;
   if (M > T00) {
@@ -222,7 +228,8 @@ __device__ __forceinline__ void ev_update(const Params& p, const ViscBuffers<rea
   ed_find = cmax<real>(0.0f, ed_find);
   real pr = eosP<real>(p, ed_find);
   real epv = cmax<real>(acu, T00 + pr);
-  real en[4] = {ed_find, T01 / epv, T02 / epv, T03 / epv};
+  const real repv = (real)1.0f / epv;
+  real en[4] = {ed_find, div_by<real>(T01, epv, repv), div_by<real>(T02, epv, repv), div_by<real>(T03, epv, repv)};
 #pragma unroll
   for (int c = 0; c < 4; c++) b.evnew[c * ld + I] = en[c];
   if (b.write_udiff) {  // get_udiff, kernel_IS.cl:714-724
@@ -238,7 +245,9 @@ __device__ __forceinline__ void ev_update(const Params& p, const ViscBuffers<rea
 
 // --------------------------------------------------------------- viscous
 template <class real, bool DO_IS, bool DO_KT, bool COUPLED>
-__global__ void __launch_bounds__(128) visc_stage_kernel(Params p, ViscBuffers<real> b, int step, real tau) {
+__global__ void __launch_bounds__(128) visc_stage_kernel(Params p, ViscBuffers<real> b, int step, TauConst<real> tc) {
+  const real tau = tc.tau;
+  const Recips<real>& rc = recips<real>(p);
   const long long N = (long long)p.nx * p.ny * p.nz;
   const long long I = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (I >= N) return;
@@ -278,13 +287,13 @@ __global__ void __launch_bounds__(128) visc_stage_kernel(Params p, ViscBuffers<r
   // Christoffel terms
   if (DO_IS) {  // kernel_IS.cl:56-65
     real uz = e0[3] * gamma3<real>(e0[1], e0[2], e0[3]);
-    S10[0] -= 2.0f * uz * pc[pidx(0, 3)] / tau;
-    S10[1] -= uz * pc[pidx(1, 3)] / tau;
-    S10[2] -= uz * pc[pidx(2, 3)] / tau;
-    S10[3] -= uz * (pc[pidx(0, 0)] + pc[pidx(3, 3)]) / tau;
-    S10[6] -= uz * pc[pidx(0, 1)] / tau;
-    S10[8] -= uz * pc[pidx(0, 2)] / tau;
-    S10[9] -= 2.0f * uz * pc[pidx(0, 3)] / tau;
+    S10[0] -= div_by<real>(2.0f * uz * pc[pidx(0, 3)], tau, tc.rtau);
+    S10[1] -= div_by<real>(uz * pc[pidx(1, 3)], tau, tc.rtau);
+    S10[2] -= div_by<real>(uz * pc[pidx(2, 3)], tau, tc.rtau);
+    S10[3] -= div_by<real>(uz * (pc[pidx(0, 0)] + pc[pidx(3, 3)]), tau, tc.rtau);
+    S10[6] -= div_by<real>(uz * pc[pidx(0, 1)], tau, tc.rtau);
+    S10[8] -= div_by<real>(uz * pc[pidx(0, 2)], tau, tc.rtau);
+    S10[9] -= div_by<real>(2.0f * uz * pc[pidx(0, 3)], tau, tc.rtau);
   }
   if (DO_KT) {  // kernel_visc.cl:24-50
     real ed = e0[0], vx = e0[1], vy = e0[2], vz = e0[3];
@@ -316,7 +325,8 @@ __global__ void __launch_bounds__(128) visc_stage_kernel(Params p, ViscBuffers<r
     const int L = a == 0 ? p.nx : (a == 1 ? p.ny : p.nz);
     const long long stride = a == 0 ? (long long)p.ny * p.nz : (a == 1 ? (long long)p.nz : 1ll);
     const Stencil st = make_stencil(q, L, stride);
-    const real D = a == 0 ? (real)p.DX : (a == 1 ? (real)p.DY : tau * p.DZ);
+    const real D = a == 0 ? (real)p.DX : (a == 1 ? (real)p.DY : tc.dzt);
+    const real rD = a == 0 ? rc.DX : (a == 1 ? rc.DY : tc.rdzt);
 
     real E[5][4];
 #pragma unroll
@@ -386,7 +396,7 @@ __global__ void __launch_bounds__(128) visc_stage_kernel(Params p, ViscBuffers<r
       for (int c = 0; c < 4; c++) {
         real src = F[1][c];
         src -= F[0][c];
-        S4[c] = S4[c] - src / D;
+        S4[c] = S4[c] - div_by<real>(src, D, rD);
       }
     }
 
@@ -400,14 +410,13 @@ __global__ void __launch_bounds__(128) visc_stage_kernel(Params p, ViscBuffers<r
         um[d][2] = u0[d + 1] * E[d + 1][2];
         um[d][3] = u0[d + 1] * E[d + 1][3];
       }
-      const real Dg = a == 2 ? (real)(p.DZ * tau) : D;
 #pragma unroll
-      for (int c = 0; c < 4; c++) grad[a][c] = grad_limit<real>(um[0][c], um[1][c], um[2][c]) / Dg;
+      for (int c = 0; c < 4; c++) grad[a][c] = div_by<real>(grad_limit<real>(um[0][c], um[1][c], um[2][c]), D, rD);
       if (a == 2) {
-        grad[2][0] = grad[2][0] + E[2][3] * u0[2] / tau;
-        grad[2][1] = grad[2][1] + (real)0.0f * u0[2] / tau;
-        grad[2][2] = grad[2][2] + (real)0.0f * u0[2] / tau;
-        grad[2][3] = grad[2][3] + (real)1.0f * u0[2] / tau;
+        grad[2][0] = grad[2][0] + div_by<real>(E[2][3] * u0[2], tau, tc.rtau);
+        grad[2][1] = grad[2][1] + div_by<real>((real)0.0f * u0[2], tau, tc.rtau);
+        grad[2][2] = grad[2][2] + div_by<real>((real)0.0f * u0[2], tau, tc.rtau);
+        grad[2][3] = grad[2][3] + div_by<real>((real)1.0f * u0[2], tau, tc.rtau);
       }
       // KT flux of u0*pi^{mn}, kt1d_real (helper.h:249-285)
 #pragma unroll 2
@@ -429,14 +438,14 @@ __global__ void __launch_bounds__(128) visc_stage_kernel(Params p, ViscBuffers<r
         }
         real src = Fm[1];
         src -= Fm[0];
-        S10[m] = S10[m] - src / D;
+        S10[m] = S10[m] - div_by<real>(src, D, rD);
       }
     }
   }
 
   real pinew[10];
-  if (DO_IS) pi_update<real, COUPLED>(p, b, step, tau, I, e0, pc, grad, S10, pinew);
-  if (DO_KT) ev_update<real, DO_IS>(p, b, step, tau, I, pin, S4, pinew);
+  if (DO_IS) pi_update<real, COUPLED>(p, b, step, tc, I, e0, pc, grad, S10, pinew);
+  if (DO_KT) ev_update<real, DO_IS>(p, b, step, tc, I, pin, S4, pinew);
 
   if (b.write_src) {
     if (DO_KT)
@@ -450,7 +459,9 @@ __global__ void __launch_bounds__(128) visc_stage_kernel(Params p, ViscBuffers<r
 
 // ----------------------------------------------------------------- ideal
 template <class real>
-__global__ void __launch_bounds__(128) ideal_stage_kernel(Params p, IdealBuffers<real> b, int step, real tau) {
+__global__ void __launch_bounds__(128) ideal_stage_kernel(Params p, IdealBuffers<real> b, int step, TauConst<real> tc) {
+  const real tau = tc.tau;
+  const Recips<real>& rc = recips<real>(p);
   const long long N = (long long)p.nx * p.ny * p.nz;
   const long long I = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (I >= N) return;
@@ -528,13 +539,14 @@ __global__ void __launch_bounds__(128) ideal_stage_kernel(Params p, IdealBuffers
       }
     }
     const real D = a == 0 ? (real)p.DX : (a == 1 ? (real)p.DY : (real)p.DZ);
+    const real rD = a == 0 ? rc.DX : (a == 1 ? rc.DY : rc.DZ);
 #pragma unroll
     for (int c = 0; c < 4; c++) {
       real src = F[1][c];
       src -= F[0][c];
-      if (riemann) S[c] = S[c] - src / D;
-      else if (a < 2) S[c] = S[c] - tau * src / D;
-      else S[c] = S[c] - tau * src / (tau * p.DZ);
+      if (riemann) S[c] = S[c] - div_by<real>(src, D, rD);
+      else if (a < 2) S[c] = S[c] - div_by<real>(tau * src, D, rD);
+      else S[c] = S[c] - div_by<real>(tau * src, tc.dzt, tc.rdzt);
     }
   }
 
@@ -562,10 +574,10 @@ __global__ void __launch_bounds__(128) ideal_stage_kernel(Params p, IdealBuffers
     T02 = (fabs(T0m[2]) < acu) ? (real)0.0f : T0m[2];
     T03 = (fabs(T0m[3]) < acu) ? (real)0.0f : T0m[3];
   } else {
-    T00 = cmax<real>(acu, T0m[0]) / tau;
-    T01 = (fabs(T0m[1]) < acu) ? (real)0.0f : T0m[1] / tau;
-    T02 = (fabs(T0m[2]) < acu) ? (real)0.0f : T0m[2] / tau;
-    T03 = (fabs(T0m[3]) < acu) ? (real)0.0f : T0m[3] / tau;
+    T00 = div_by<real>(cmax<real>(acu, T0m[0]), tau, tc.rtau);
+    T01 = (fabs(T0m[1]) < acu) ? (real)0.0f : div_by<real>(T0m[1], tau, tc.rtau);
+    T02 = (fabs(T0m[2]) < acu) ? (real)0.0f : div_by<real>(T0m[2], tau, tc.rtau);
+    T03 = (fabs(T0m[3]) < acu) ? (real)0.0f : div_by<real>(T0m[3], tau, tc.rtau);
   }
   real M = sqrt(T01 * T01 + T02 * T02 + T03 * T03);
   real SCALE_COEF = 0.999f;
@@ -579,7 +591,8 @@ __global__ void __launch_bounds__(128) ideal_stage_kernel(Params p, IdealBuffers
   ed_find = cmax<real>(0.0f, ed_find);
   real pr = eosP<real>(p, ed_find);
   real epv = cmax<real>(acu, T00 + pr);
-  real en[4] = {ed_find, T01 / epv, T02 / epv, T03 / epv};
+  const real repv = (real)1.0f / epv;
+  real en[4] = {ed_find, div_by<real>(T01, epv, repv), div_by<real>(T02, epv, repv), div_by<real>(T03, epv, repv)};
 #pragma unroll
   for (int c = 0; c < 4; c++) b.evnew[c * ld + I] = en[c];
   if (b.write_src)

@@ -132,7 +132,9 @@ __device__ __forceinline__ void face_flux(const Params& p, real tau, int a, cons
 
 template <class real, bool DO_IS, bool DO_KT, bool COUPLED, int TJ, int TK, int MINB>
 __global__ void __launch_bounds__(TJ * TK, MINB)
-    visc_stage_tiled_kernel(Params p, ViscBuffers<real> b, int step, real tau, int chunk) {
+    visc_stage_tiled_kernel(Params p, ViscBuffers<real> b, int step, TauConst<real> tc, int chunk) {
+  const real tau = tc.tau;
+  const Recips<real>& rc = recips<real>(p);
   typedef TileGeom<TJ, TK> G;
   typedef TileSmem<real, TJ, TK> SM;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -254,13 +256,13 @@ __global__ void __launch_bounds__(TJ * TK, MINB)
       }
       if (DO_IS) {  // kernel_IS.cl:56-65
         real uz = e0[3] * gamma3<real>(e0[1], e0[2], e0[3]);
-        S10[0] -= 2.0f * uz * pc[pidx(0, 3)] / tau;
-        S10[1] -= uz * pc[pidx(1, 3)] / tau;
-        S10[2] -= uz * pc[pidx(2, 3)] / tau;
-        S10[3] -= uz * (pc[pidx(0, 0)] + pc[pidx(3, 3)]) / tau;
-        S10[6] -= uz * pc[pidx(0, 1)] / tau;
-        S10[8] -= uz * pc[pidx(0, 2)] / tau;
-        S10[9] -= 2.0f * uz * pc[pidx(0, 3)] / tau;
+        S10[0] -= div_by<real>(2.0f * uz * pc[pidx(0, 3)], tau, tc.rtau);
+        S10[1] -= div_by<real>(uz * pc[pidx(1, 3)], tau, tc.rtau);
+        S10[2] -= div_by<real>(uz * pc[pidx(2, 3)], tau, tc.rtau);
+        S10[3] -= div_by<real>(uz * (pc[pidx(0, 0)] + pc[pidx(3, 3)]), tau, tc.rtau);
+        S10[6] -= div_by<real>(uz * pc[pidx(0, 1)], tau, tc.rtau);
+        S10[8] -= div_by<real>(uz * pc[pidx(0, 2)], tau, tc.rtau);
+        S10[9] -= div_by<real>(2.0f * uz * pc[pidx(0, 3)], tau, tc.rtau);
       }
       if (DO_KT) {  // kernel_visc.cl:24-50
         real ed = e0[0], vx = e0[1], vy = e0[2], vz = e0[3];
@@ -286,7 +288,8 @@ __global__ void __launch_bounds__(TJ * TK, MINB)
       // flux differences in the reference's order x, y, z
 #pragma unroll
       for (int a = 0; a < 3; a++) {
-        const real D = a == 0 ? (real)p.DX : (a == 1 ? (real)p.DY : tau * p.DZ);
+        const real D = a == 0 ? (real)p.DX : (a == 1 ? (real)p.DY : tc.dzt);
+        const real rD = a == 0 ? rc.DX : (a == 1 ? rc.DY : tc.rdzt);
 #pragma unroll
         for (int c = 0; c < NCOMP; c++) {
           if (c < 4 && !DO_KT) continue;
@@ -295,8 +298,8 @@ __global__ void __launch_bounds__(TJ * TK, MINB)
           real fm = a == 0 ? F_prev[c] : (a == 1 ? s.SY[c][tj * TK + tk] : s.SZ[c][tj * (TK + 2) + tk]);
           real src = fp;
           src -= fm;
-          if (c < 4) S4[c] = S4[c] - src / D;
-          else S10[c - 4] = S10[c - 4] - src / D;
+          if (c < 4) S4[c] = S4[c] - div_by<real>(src, D, rD);
+          else S10[c - 4] = S10[c - 4] - div_by<real>(src, D, rD);
         }
       }
 
@@ -318,21 +321,20 @@ __global__ void __launch_bounds__(TJ * TK, MINB)
           real umy1[4] = {uy1 * 1.0f, uy1 * Cy1[RF_VX * G::NC], uy1 * Cy1[RF_VY * G::NC], uy1 * Cy1[RF_VZ * G::NC]};
           real umz0[4] = {uz0 * 1.0f, uz0 * Cz0[RF_VX * G::NC], uz0 * Cz0[RF_VY * G::NC], uz0 * Cz0[RF_VZ * G::NC]};
           real umz1[4] = {uz1 * 1.0f, uz1 * Cz1[RF_VX * G::NC], uz1 * Cz1[RF_VY * G::NC], uz1 * Cz1[RF_VZ * G::NC]};
-          const real DZt = (real)(p.DZ * tau);
 #pragma unroll
           for (int c = 0; c < 4; c++) {
-            grad[0][c] = grad_limit<real>(umu_prev[c], umc[c], umx1[c]) / (real)p.DX;
-            grad[1][c] = grad_limit<real>(umy0[c], umc[c], umy1[c]) / (real)p.DY;
-            grad[2][c] = grad_limit<real>(umz0[c], umc[c], umz1[c]) / DZt;
+            grad[0][c] = div_by<real>(grad_limit<real>(umu_prev[c], umc[c], umx1[c]), (real)p.DX, rc.DX);
+            grad[1][c] = div_by<real>(grad_limit<real>(umy0[c], umc[c], umy1[c]), (real)p.DY, rc.DY);
+            grad[2][c] = div_by<real>(grad_limit<real>(umz0[c], umc[c], umz1[c]), tc.dzt, tc.rdzt);
           }
-          grad[2][0] = grad[2][0] + e0[3] * u0c / tau;
-          grad[2][1] = grad[2][1] + (real)0.0f * u0c / tau;
-          grad[2][2] = grad[2][2] + (real)0.0f * u0c / tau;
-          grad[2][3] = grad[2][3] + (real)1.0f * u0c / tau;
+          grad[2][0] = grad[2][0] + div_by<real>(e0[3] * u0c, tau, tc.rtau);
+          grad[2][1] = grad[2][1] + div_by<real>((real)0.0f * u0c, tau, tc.rtau);
+          grad[2][2] = grad[2][2] + div_by<real>((real)0.0f * u0c, tau, tc.rtau);
+          grad[2][3] = grad[2][3] + div_by<real>((real)1.0f * u0c, tau, tc.rtau);
 #pragma unroll
           for (int c = 0; c < 4; c++) umu_prev[c] = umc[c];
         }
-        pi_update<real, COUPLED>(p, b, step, tau, I, e0, pc, grad, S10, pinew);
+        pi_update<real, COUPLED>(p, b, step, tc, I, e0, pc, grad, S10, pinew);
       } else {
         real u0c = Cc[RF_U0 * G::NC];
         umu_prev[0] = u0c * 1.0f;
@@ -340,7 +342,7 @@ __global__ void __launch_bounds__(TJ * TK, MINB)
         umu_prev[2] = u0c * e0[2];
         umu_prev[3] = u0c * e0[3];
       }
-      if (DO_KT) ev_update<real, DO_IS>(p, b, step, tau, I, pin, S4, pinew);
+      if (DO_KT) ev_update<real, DO_IS>(p, b, step, tc, I, pin, S4, pinew);
       if (b.write_src) {
         if (DO_KT)
 #pragma unroll
