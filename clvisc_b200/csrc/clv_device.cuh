@@ -105,8 +105,18 @@ template <class real> __device__ __forceinline__ real div_step(real x, int step)
 // ------------------------------------------------------------------ EOS
 // Table lookup of eos_table.h:39-62: row/col from the energy density, two
 // nearest texels (the second wraps to the next row), clamp-to-edge, lerp.
+// CLV_EOS_INLINE (default 1): inline the lookup at every call site, or keep
+// one out-of-line copy per precision to shrink the kernels' code
+#ifndef CLV_EOS_INLINE
+#define CLV_EOS_INLINE 1
+#endif
+#if CLV_EOS_INLINE
+#define CLV_EOS_ATTR __forceinline__
+#else
+#define CLV_EOS_ATTR __noinline__
+#endif
 template <class real>
-__device__ __forceinline__ real eos_comp(const Params& p, real eps, int c) {
+__device__ CLV_EOS_ATTR real eos_comp(const Params& p, real eps, int c) {
   const Recips<real>& rc = recips<real>(p);
   real ed_per_row = p.eos_step * p.eos_ncol;
   int row = (int)div_by<real>(eps, ed_per_row, rc.eos_epr);

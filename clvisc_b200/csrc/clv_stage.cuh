@@ -365,6 +365,12 @@ __global__ void __launch_bounds__(128) visc_stage_kernel(Params p, ViscBuffers<r
           Q[d][c] = tau * (T0m + pim0);
         }
       }
+      // limited slopes at stencil cells 1, 2, 3 (each face uses two of them)
+      real DA[3][4];
+#pragma unroll
+      for (int d = 0; d < 3; d++)
+#pragma unroll
+        for (int c = 0; c < 4; c++) DA[d][c] = slope<real>(Q[d][c], Q[d + 1][c], Q[d + 2][c]);
       real F[2][4];
 #pragma unroll
       for (int f = 0; f < 2; f++) {
@@ -374,8 +380,8 @@ __global__ void __launch_bounds__(128) visc_stage_kernel(Params p, ViscBuffers<r
         real pt = pr_half * tau;
 #pragma unroll
         for (int c = 0; c < 4; c++) {
-          real DAl = slope<real>(Q[l - 1][c], Q[l][c], Q[l + 1][c]);
-          real DAr = slope<real>(Q[r - 1][c], Q[r][c], Q[r + 1][c]);
+          real DAl = DA[l - 1][c];
+          real DAr = DA[r - 1][c];
           real AL = Q[l][c] + 0.5f * DAl;
           real AR = Q[r][c] - 0.5f * DAr;
           real p0l = (l == 2) ? pc[c] : b.pi_st[c * ld + Jl];
@@ -424,12 +430,15 @@ __global__ void __launch_bounds__(128) visc_stage_kernel(Params p, ViscBuffers<r
         real U[5];
 #pragma unroll
         for (int d = 0; d < 5; d++) U[d] = u0[d] * ((d == 2) ? pc[m] : b.pi_st[m * ld + I + st.off[d]]);
+        real DU[3];
+#pragma unroll
+        for (int d = 0; d < 3; d++) DU[d] = slope<real>(U[d], U[d + 1], U[d + 2]);
         real Fm[2];
 #pragma unroll
         for (int f = 0; f < 2; f++) {
           const int l = 1 + f, r = 2 + f;
-          real DAl = slope<real>(U[l - 1], U[l], U[l + 1]);
-          real DAr = slope<real>(U[r - 1], U[r], U[r + 1]);
+          real DAl = DU[l - 1];
+          real DAr = DU[r - 1];
           real AL = U[l] + 0.5f * DAl;
           real AR = U[r] - 0.5f * DAr;
           real Jp = AR * vh[f];

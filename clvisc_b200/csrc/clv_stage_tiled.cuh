@@ -21,6 +21,15 @@
 
 namespace clv {
 
+#ifndef CLV_TILED_INLINE
+#define CLV_TILED_INLINE 1
+#endif
+#if CLV_TILED_INLINE
+#define CLV_TILED_ATTR __forceinline__
+#else
+#define CLV_TILED_ATTR __noinline__
+#endif
+
 // record fields (planes of the shared-memory region)
 enum { RF_E = 0, RF_VX, RF_VY, RF_VZ, RF_PR, RF_U0, RF_Q0, RF_Q1, RF_Q2, RF_Q3, RF_PI, RF_N = RF_PI + 10 };
 // slope / face-flux components: 0..3 KT (Q), 4..13 IS (u0*pi)
@@ -46,7 +55,7 @@ template <class real, int TJ, int TK> struct TileSmem {
 
 // record of one (clamped) cell of the stage input
 template <class real>
-__device__ __forceinline__ void make_record(const Params& p, const ViscBuffers<real>& b, real tau, int i, int j, int k,
+__device__ CLV_TILED_ATTR void make_record(const Params& p, const ViscBuffers<real>& b, real tau, int i, int j, int k,
                                             real* dst, int stride) {
   i = min(max(i, 0), p.nx - 1);
   j = min(max(j, 0), p.ny - 1);
@@ -79,7 +88,7 @@ __device__ __forceinline__ void make_record(const Params& p, const ViscBuffers<r
 
 // limited slopes of the 14 components at the middle of three records
 template <class real>
-__device__ __forceinline__ void slopes3(const real* L, int sl, const real* M, int sm, const real* R, int sr,
+__device__ CLV_TILED_ATTR void slopes3(const real* L, int sl, const real* M, int sm, const real* R, int sr,
                                         real* out, int so) {
 #pragma unroll
   for (int c = 0; c < 4; c++)
@@ -93,7 +102,7 @@ __device__ __forceinline__ void slopes3(const real* L, int sl, const real* M, in
 // flux through the face between records L and R along axis a, given their
 // slopes (kt1d_visc face part and kt1d_real face part)
 template <class real, bool DO_IS, bool DO_KT>
-__device__ __forceinline__ void face_flux(const Params& p, real tau, int a, const real* L, int sl, const real* sL,
+__device__ CLV_TILED_ATTR void face_flux(const Params& p, real tau, int a, const real* L, int sl, const real* sL,
                                           int ssl, const real* R, int sr, const real* sR, int ssr, real F[NCOMP]) {
   real h[4];
 #pragma unroll
