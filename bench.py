@@ -144,15 +144,16 @@ def read_traffic():
     return None
 
 
-def cpu_baseline(steps=2, warmup=0):
-    """The oracle on a 385 x 385 x SLAB_NZ slab, all host threads."""
+def cpu_baseline(steps=2, warmup=0, nx=NX, ny=NY, nz=NZ):
+    """The oracle on an nx x ny x SLAB_NZ eta slab of the event, all host threads."""
     sys.path.insert(0, os.path.join(ROOT, 'oracle'))
     import numpy as np
     import oracle as O
-    cfg = make_cfg(nz=SLAB_NZ)
-    ic = initial_condition().reshape(NX, NY, NZ, 4)
-    k0 = NZ // 2 - SLAB_NZ // 2
-    sub = np.ascontiguousarray(ic[:, :, k0:k0 + SLAB_NZ]).reshape(-1, 4)
+    slab = min(SLAB_NZ, nz)
+    cfg = make_cfg(nz=slab, nx=nx, ny=ny)
+    ic = initial_condition(nx=nx, ny=ny, nz=nz).reshape(nx, ny, nz, 4)
+    k0 = nz // 2 - slab // 2
+    sub = np.ascontiguousarray(ic[:, :, k0:k0 + slab]).reshape(-1, 4)
     o = O.OracleVisc(cfg)
     o.load_ini(sub)
     for n in range(warmup):
@@ -162,20 +163,38 @@ def cpu_baseline(steps=2, warmup=0):
         o.step(n)
     dt = time.perf_counter() - t
     cores = int(os.environ.get('OMP_NUM_THREADS', os.cpu_count() or 1))
-    cells = NX * NY * SLAB_NZ
+    cells = nx * ny * slab
     return {'value': cells * steps / dt, 'unit': UNIT, 'cores': cores, 'kind': 'port',
-            'sample': '%d steps of a %dx%dx%d eta slab of the same event (oracle, OpenMP)' % (steps, NX, NY, SLAB_NZ),
+            'sample': '%d steps of a %dx%dx%d eta slab of the same event (oracle, OpenMP)' % (steps, nx, ny, slab),
             'seconds': dt}
+
+
+def max_over_ranks(x, dist):
+    """The maximum of a per-rank float over all ranks (x itself with one rank)."""
+    if dist is None:
+        return x
+    import torch
+    dev = 'cuda' if dist.get_backend() == 'nccl' else 'cpu'
+    t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate_rate(cells, steps, ms, world):
+    """Whole-job cell-updates/s: every rank advances its own replica of
+    `cells` cells for `steps` steps; `ms` is the slowest rank's time."""
+    return world * cells * steps / (ms * 1e-3)
 
 
 def run_reference(args, rank, world):
     if rank != 0:
         return
-    cb = cpu_baseline(steps=max(1, args.steps), warmup=min(args.warmup, 1))
+    nx, ny, nz = args.grid
+    cb = cpu_baseline(steps=max(1, args.steps), warmup=min(args.warmup, 1), nx=nx, ny=ny, nz=nz)
     line = {'impl': 'reference', 'metric': METRIC, 'value': cb['value'], 'unit': UNIT, 'n_gpus': world,
             'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': 1e3 * cb['seconds'] / max(1, args.steps),
             'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic',
-            'config': {'workload': 'viscous 385x385x115 Pb+Pb b=8 fm, FP32, lattice EOS (slab sample)'},
+            'config': {'workload': 'viscous %dx%dx%d Pb+Pb b=8 fm, FP32, lattice EOS (slab sample)' % (nx, ny, nz)},
             'cpu_baseline': {k: cb[k] for k in ('value', 'unit', 'cores', 'kind', 'sample')},
             'e2e': {'value': cb['value'], 'unit': UNIT, 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}}
     print(json.dumps(line), flush=True)
@@ -212,13 +231,9 @@ def run_gpu(args, rank, world, dist):
             v.step(n)
         e1.record(stream)
         torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1)
+    ms = max_over_ranks(e0.elapsed_time(e1), dist)
     barrier()
-    if dist is not None:
-        t = torch.tensor([ms], device='cuda')
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = world * cells * args.steps / (ms * 1e-3)
+    value = aggregate_rate(cells, args.steps, ms, world)
 
     if args.no_e2e:
         if rank == 0:
@@ -238,13 +253,9 @@ def run_gpu(args, rank, world, dist):
     out = v2.ideal.ev_to_host()
     f1.record(stream)
     torch.cuda.synchronize()
-    e2e_ms = f0.elapsed_time(f1)
+    e2e_ms = max_over_ranks(f0.elapsed_time(f1), dist)
     e2e_wall = time.perf_counter() - t0
-    if dist is not None:
-        t = torch.tensor([e2e_ms], device='cuda')
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e = world * cells * args.steps / (e2e_ms * 1e-3)
+    e2e = aggregate_rate(cells, args.steps, e2e_ms, world)
     h2d = ic.nbytes / args.steps
     d2h = out.nbytes / args.steps
 
@@ -266,7 +277,7 @@ def run_gpu(args, rank, world, dist):
                          'frac': achieved / peak, 'peak_kind': peak_kind,
                          'traffic': None if traffic is None else traffic * cells / 2,
                          'alg_bytes_per_launch': ALG_BYTES_PER_CELL_UPDATE * cells / 2,
-                         'kernel': 'visc_stage_kernel<float,IS+KT> (2 launches per step)'},
+                         'kernel': 'visc_stage_tiled_kernel<float,IS,KT> (2 launches per step)'},
             'clocks': clocks.summary(),
         }
         if not args.no_cpu_baseline:
@@ -278,7 +289,7 @@ def run_gpu(args, rank, world, dist):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--gpus', type=int, default=1)
-    ap.add_argument('--steps', type=int, default=20)
+    ap.add_argument('--steps', type=int, default=50)
     ap.add_argument('--warmup', type=int, default=3)
     ap.add_argument('--impl', default='b200', choices=['b200', 'reference'])
     ap.add_argument('--no-cpu-baseline', action='store_true')
@@ -288,21 +299,21 @@ def main():
     args = ap.parse_args()
     world = int(os.environ.get('WORLD_SIZE', '1'))
     rank = int(os.environ.get('RANK', '0'))
+    if args.impl == 'reference':
+        # rank 0 alone times the CPU path; the other ranks exit without work
+        # and without joining a process group
+        run_reference(args, rank, world)
+        return
     dist = None
     if world > 1:
         import datetime
+        import torch
         import torch.distributed as tdist
-        backend = 'gloo' if args.impl == 'reference' else 'nccl'
-        if backend == 'nccl':
-            import torch
-            torch.cuda.set_device(int(os.environ.get('LOCAL_RANK', 0)))
-        tdist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+        torch.cuda.set_device(int(os.environ.get('LOCAL_RANK', 0)))
+        tdist.init_process_group('nccl', timeout=datetime.timedelta(seconds=120))
         dist = tdist
     try:
-        if args.impl == 'reference':
-            run_reference(args, rank, world)
-        else:
-            run_gpu(args, rank, world, dist)
+        run_gpu(args, rank, world, dist)
     finally:
         if dist is not None:
             dist.destroy_process_group()
