@@ -15,6 +15,7 @@ CLV_FLAG_RIEMANN_TEST = 1
 CLV_FLAG_GUBSER_VISC_TEST = 2
 CLV_FLAG_PIMN_OMEGA_COUPLING = 4
 CLV_FLAG_OMEGA_OMEGA_COUPLING = 8
+CLV_FLAG_BULK = 16
 
 CLV_OPT_STAGE_KERNEL = 1
 CLV_OPT_CHUNK = 2
@@ -43,6 +44,8 @@ class ClvParams(ctypes.Structure):
         ('eos_num_ed', ctypes.c_int), ('eos_nrow', ctypes.c_int), ('eos_ncol', ctypes.c_int),
         ('eos_table', ctypes.c_void_p),
         ('flags', ctypes.c_int),
+        ('zetaos_max', ctypes.c_float), ('zetaos_t0', ctypes.c_float), ('zetaos_width', ctypes.c_float),
+        ('zetaos_skew', ctypes.c_float),
     ]
 
 

@@ -84,6 +84,10 @@ def read_config(argv=None, info_path=None):
         'ETAOS_LEFT_SLOP': (gf('intrinsic', 'ETAOS_LEFT_SLOP'), 'eta/s slope below the kink'),
         'ETAOS_RIGHT_SLOP': (gf('intrinsic', 'ETAOS_RIGHT_SLOP'), 'eta/s slope above the kink'),
         'LAM1': (gf('intrinsic', 'LAM1'), 'lambda_1 of the pi^2 term'),
+        'ZETAOS_MAX': (gf('intrinsic', 'ZETAOS_MAX'), 'peak zeta/s of the bulk sector (0: off)'),
+        'ZETAOS_T0': (gf('intrinsic', 'ZETAOS_T0'), 'T of the zeta/s peak'),
+        'ZETAOS_WIDTH': (gf('intrinsic', 'ZETAOS_WIDTH'), 'width of the zeta/s peak'),
+        'ZETAOS_SKEW': (gf('intrinsic', 'ZETAOS_SKEW'), 'skewness of the zeta/s peak'),
         'BSZ': (gi('opencl', 'local_workgroup_size'), 'work-group size (accepted, unused)'),
     }
     parser = argparse.ArgumentParser(description='CLVisc B200 hydro configuration')
@@ -120,7 +124,7 @@ def write_config(configs, comments=''):
         'NX', 'NY', 'NZ', 'ntskip', 'nxskip', 'nyskip', 'nzskip', 'DT', 'DX', 'DY', 'DZ')}
     c['intrinsic'] = {k: str(getattr(configs, k)) for k in (
         'TAU0', 'eos_type', 'TFRZ', 'ETAOS_XMIN', 'ETAOS_YMIN', 'ETAOS_LEFT_SLOP', 'ETAOS_RIGHT_SLOP', 'LAM1',
-        'BSZ')}
+        'ZETAOS_MAX', 'ZETAOS_T0', 'ZETAOS_WIDTH', 'ZETAOS_SKEW', 'BSZ')}
     with open(os.path.join(configs.fPathOut, 'hydro.info'), 'w') as f:
         c.write(f)
         f.write('#comments: ' + comments)

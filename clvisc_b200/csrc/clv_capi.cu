@@ -63,6 +63,10 @@ int to_params(const clv_params* in, clv::Params* out) {
   p.eos_num = in->eos_num_ed; p.eos_nrow = in->eos_nrow; p.eos_ncol = in->eos_ncol;
   p.eos = in->eos_table;
   p.flags = in->flags;
+  p.ZETAOS_MAX = in->zetaos_max; p.ZETAOS_T0 = in->zetaos_t0;
+  p.ZETAOS_WIDTH = in->zetaos_width; p.ZETAOS_SKEW = in->zetaos_skew;
+  if ((in->flags & CLV_FLAG_BULK) && (!(in->zetaos_width > 0.0f) || !(in->zetaos_max >= 0.0f)))
+    return fail(CLV_ERR_INVALID, "bulk sector: zetaos_width must be > 0 and zetaos_max >= 0%s");
   // correctly rounded reciprocals in each precision (host IEEE arithmetic, no
   // contraction): the kernels divide by these constants with clv::div_by
   const float epr = in->eos_ed_step * in->eos_ncol;  // as the kernels form it
@@ -143,7 +147,9 @@ int visc_stage_t(const clv::Params& p, int step, double tau, int parts, const cl
     return fail(CLV_ERR_INVALID, "visc stage: null buffer for the pi update%s");
   if (kt && (!v.evnew || !v.pin || (!is && !v.pi2in))) return fail(CLV_ERR_INVALID, "visc stage: null buffer for update_ev%s");
   if (v.write_udiff && (!kt || !v.udiff)) return fail(CLV_ERR_INVALID, "visc stage: write_udiff needs CLV_PART_KT%s");
-  if (g_stage_kernel == 0) {
+  const bool bulk = p.flags & clv::FLAG_BULK;
+  // the tiled kernel has no bulk sector; bulk runs take the per-cell kernel
+  if (g_stage_kernel == 0 && !bulk) {
     if (is && kt) return launch_tiled<real, true, true>(p, v, step, tau, s);
     if (is) return launch_tiled<real, true, false>(p, v, step, tau, s);
     return launch_tiled<real, false, true>(p, v, step, tau, s);
@@ -152,11 +158,19 @@ int visc_stage_t(const clv::Params& p, int step, double tau, int parts, const cl
   dim3 grid(nblk(ncell(p), bs));
   const clv::TauConst<real> t = tau_const<real>(p, tau);
   const bool cpl = p.flags & (clv::FLAG_GUBSER_VISC | clv::FLAG_PIMN_OMEGA | clv::FLAG_OMEGA_OMEGA);
-  if (is && kt && cpl) clv::visc_stage_kernel<real, true, true, true><<<grid, bs, 0, s>>>(p, v, step, t);
-  else if (is && kt) clv::visc_stage_kernel<real, true, true, false><<<grid, bs, 0, s>>>(p, v, step, t);
-  else if (is && cpl) clv::visc_stage_kernel<real, true, false, true><<<grid, bs, 0, s>>>(p, v, step, t);
-  else if (is) clv::visc_stage_kernel<real, true, false, false><<<grid, bs, 0, s>>>(p, v, step, t);
-  else clv::visc_stage_kernel<real, false, true, false><<<grid, bs, 0, s>>>(p, v, step, t);
+  if (bulk) {
+    if (is && kt && cpl) clv::visc_stage_kernel<real, true, true, true, true><<<grid, bs, 0, s>>>(p, v, step, t);
+    else if (is && kt) clv::visc_stage_kernel<real, true, true, false, true><<<grid, bs, 0, s>>>(p, v, step, t);
+    else if (is && cpl) clv::visc_stage_kernel<real, true, false, true, true><<<grid, bs, 0, s>>>(p, v, step, t);
+    else if (is) clv::visc_stage_kernel<real, true, false, false, true><<<grid, bs, 0, s>>>(p, v, step, t);
+    else clv::visc_stage_kernel<real, false, true, false, true><<<grid, bs, 0, s>>>(p, v, step, t);
+  } else {
+    if (is && kt && cpl) clv::visc_stage_kernel<real, true, true, true, false><<<grid, bs, 0, s>>>(p, v, step, t);
+    else if (is && kt) clv::visc_stage_kernel<real, true, true, false, false><<<grid, bs, 0, s>>>(p, v, step, t);
+    else if (is && cpl) clv::visc_stage_kernel<real, true, false, true, false><<<grid, bs, 0, s>>>(p, v, step, t);
+    else if (is) clv::visc_stage_kernel<real, true, false, false, false><<<grid, bs, 0, s>>>(p, v, step, t);
+    else clv::visc_stage_kernel<real, false, true, false, false><<<grid, bs, 0, s>>>(p, v, step, t);
+  }
   return cuda_check("visc_stage_kernel");
 }
 
@@ -213,7 +227,7 @@ int hypersf_t(const clv::Params& p, int visc, double tau_old, double tau_new, co
 
 extern "C" {
 
-int clv_version(void) { return 0x000101; }
+int clv_version(void) { return 0x000102; }
 const char* clv_last_error(void) { return g_err.c_str(); }
 int clv_alignment(void) { return kAlign; }
 

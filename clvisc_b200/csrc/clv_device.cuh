@@ -31,6 +31,8 @@ struct Params {
   int eos_num, eos_nrow, eos_ncol;
   const float* eos;  // nrow*ncol texels of (cs2, p, T, s)
   int flags;
+  // bulk sector (FLAG_BULK): zeta/s(T) peak, position, width, skewness
+  float ZETAOS_MAX, ZETAOS_T0, ZETAOS_WIDTH, ZETAOS_SKEW;
   Recips<float> rf;   // reciprocals for float kernels
   Recips<double> rd;  // reciprocals for double kernels
 };
@@ -49,6 +51,7 @@ enum : int {
   FLAG_GUBSER_VISC = 2,
   FLAG_PIMN_OMEGA = 4,
   FLAG_OMEGA_OMEGA = 8,
+  FLAG_BULK = 16,
 };
 
 template <class real> struct Acu;
@@ -180,14 +183,17 @@ __device__ __forceinline__ real max_speed(const Params& p, real e, real vx, real
   return cmax<real>(lam, 1.0f);
 }
 
-// helper.h:128-167; returns the energy density
-template <class real> __device__ __forceinline__ real root_newton(const Params& p, real T00, real M) {
+// helper.h:128-167; returns the energy density. With BULK the pressure is
+// P(e) + bulk, the bulk viscous pressure of the cell.
+template <class real, bool BULK = false>
+__device__ __forceinline__ real root_newton(const Params& p, real T00, real M, real bulk = (real)0.0f) {
   real vl = 0.0f;
   real vh = 1.0f;
   real dpe = 1.0f / 3.0f;
   real v = 0.5f * (vl + vh);
   real ed = T00 - M * v;
   real pr = eosP<real>(p, ed);
+  if (BULK) pr = pr + bulk;
   real f = (T00 + pr) * v - M;
   real df = (T00 + pr) - M * v * dpe;
   real dvold = vh - vl;
@@ -207,6 +213,7 @@ template <class real> __device__ __forceinline__ real root_newton(const Params& 
     if (fabs(dv) < 0.00001f || i > 100) break;
     ed = T00 - M * v;
     pr = eosP<real>(p, ed);
+    if (BULK) pr = pr + bulk;
     f = (T00 + pr) * v - M;
     df = (T00 + pr) - M * v * dpe;
     if (f > 0.0f) {
@@ -216,6 +223,15 @@ template <class real> __device__ __forceinline__ real root_newton(const Params& 
     }
   }
   return T00 - M * v;
+}
+
+// Bulk sector (no counterpart in the reference): zeta/s(T) as a skewed Cauchy
+// peak, ZETAOS_MAX w^2 / (w^2 + (T - T0)^2), w = WIDTH (1 + SKEW sign(T - T0))
+// (the JETSCAPE parametrisation, Everett et al., PRC 103, 054904 (2021)).
+template <class real> __device__ __forceinline__ real zetaos(const Params& p, real T) {
+  real dT = T - p.ZETAOS_T0;
+  real w = p.ZETAOS_WIDTH * (1.0f + p.ZETAOS_SKEW * csign<real>(dT));
+  return p.ZETAOS_MAX * (w * w) / (w * w + dT * dT);
 }
 
 // helper.h:23-26

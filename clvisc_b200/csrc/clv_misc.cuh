@@ -21,6 +21,10 @@ __global__ void visc_initialize_kernel(Params p, real* pi1, uint8_t* goodcell, r
   pi1[pidx(1, 1) * ld + I] = tmp;
   pi1[pidx(2, 2) * ld + I] = tmp;
   pi1[pidx(3, 3) * ld + I] = -2.0f * tmp;
+  if (p.flags & FLAG_BULK) {  // bulk sector: Navier-Stokes Pi of Bjorken flow, theta = 1/tau
+    real zetav = zetaos<real>(p, T) * s * CLV_HBARC;
+    pi1[10 * ld + I] = -zetav / tau;
+  }
 #pragma unroll
   for (int c = 0; c < 4; c++) udiff[c * ld + I] = 0.0f;
   goodcell[I] = 1;

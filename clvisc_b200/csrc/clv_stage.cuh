@@ -20,7 +20,7 @@ namespace clv {
 
 template <class real> struct ViscBuffers {
   const real* ev_st;   // 4 planes: d_ev[step], stencil input
-  const real* pi_st;   // 10 planes: d_pi[step], stencil input
+  const real* pi_st;   // 10 planes (11 with the bulk sector: plane 10 is Pi): d_pi[step], stencil input
   const real* ev1;     // 4 planes: d_ev[1]
   const real* ev2e;    // plane 0 of d_ev[2] (read at stage 1)
   const real* pi1;     // 10 planes: d_pi[1], start point of the pi update
@@ -28,7 +28,7 @@ template <class real> struct ViscBuffers {
   const real* pi2in;   // 10 planes: new pi, read when the pi update is not fused
   real* evnew;         // 4 planes
   real* pinew;         // 10 planes
-  real* src;           // 14 planes: KT sources 0..3, IS sources 4..13
+  real* src;           // 14 planes: KT sources 0..3, IS sources 4..13 (14: bulk source)
   real* udiff;         // 4 planes
   uint8_t* goodcell;   // 1 byte per cell
   typename KeyT<real>::type* edmax_key;  // optional max of evnew energy density
@@ -60,13 +60,21 @@ __device__ __forceinline__ Stencil make_stencil(int q, int L, long long stride) 
   return s;
 }
 
+// weight of pi^{mu nu} sigma^{mu nu} in the full contraction over mu <= nu:
+// g_{mu mu} g_{nu nu}, doubled off the diagonal (bulk sector)
+template <class real> __device__ __forceinline__ real pisig_weight(int mu, int nu) {
+  real w = (mu == nu) ? (real)1.0f : (real)2.0f;
+  return ((mu == 0) != (nu == 0)) ? -w : w;
+}
+
 // update_pimn (kernel_IS.cl:501-709) for cell I: e0 and pc are the stage
 // input ev and pi at the cell, grad the velocity gradients, S10 the IS sources
 // (updated in place); writes pi_new and goodcell, returns the new pi in pinew.
-template <class real, bool COUPLED>
+// With BULK, component 10 of pc, S10 and pinew is the bulk pressure Pi.
+template <class real, bool COUPLED, bool BULK>
 __device__ __forceinline__ void pi_update(const Params& p, const ViscBuffers<real>& b, int step,
-                                          const TauConst<real>& tc, long long I, const real e0[4], const real pc[10],
-                                          const real grad[3][4], real S10[10], real pinew[10]) {
+                                          const TauConst<real>& tc, long long I, const real e0[4], const real pc[11],
+                                          const real grad[3][4], real S10[11], real pinew[11]) {
   const long long ld = p.ld;
   const real acu = Acu<real>::v;
   const real tau = tc.tau;
@@ -132,6 +140,7 @@ __device__ __forceinline__ void pi_update(const Params& p, const ViscBuffers<rea
   const real den = u_new[0] + p.DT * one_over_taupi;
   const real rden = (real)1.0f / den;
   real max_pimn_abs = 0.0f;
+  real pisig = 0.0f;  // bulk sector: pi^{mu nu} sigma_{mu nu}
 #pragma unroll
   for (int mu = 0; mu < 4; mu++)
 #pragma unroll
@@ -142,6 +151,7 @@ __device__ __forceinline__ void pi_update(const Params& p, const ViscBuffers<rea
                    2.0f / 3.0f * (gmn<real>(mu, nu) - u[mu] * u[nu]) * theta;
       const int mn = pidx(mu, nu);
       if (u[0] > 10000.0f) sigma = 0.0f;
+      if (BULK) pisig = pisig + pisig_weight<real>(mu, nu) * pc[mn] * sigma;
       real piNS = etav * sigma;
       real pi_old = b.pi1[mn * ld + I] * u_old[0];
       real src = div_by<real>(-pc[mn] * theta, (real)3.0f, rc.three) - div_by<real>(pc[mn] * u[0], tau, tc.rtau);
@@ -165,26 +175,51 @@ __device__ __forceinline__ void pi_update(const Params& p, const ViscBuffers<rea
       if (fabs(pi_old) > max_pimn_abs) max_pimn_abs = fabs(pi_old);
       pinew[mn] = pi_old;
     }
+  if (BULK) {
+    // Bulk sector (no counterpart in the reference): the 14-moment relaxation
+    // equation of Denicol, Niemi, Molnar and Rischke (PRD 85, 114047 (2012)),
+    // tau_Pi D Pi + Pi = -zeta theta - 2/3 tau_Pi Pi theta
+    //   + 8/5 (1/3 - cs2) tau_Pi pi^{mu nu} sigma_{mu nu},
+    // tau_Pi = zeta / (14.55 (1/3 - cs2)^2 (e + P)), for the density u0 Pi
+    // with the same implicit relaxation step as the shear components.
+    real cs2 = eos_comp<real>(p, ed_step, 0);
+    real local_zetaos = zetaos<real>(p, temperature);
+    real zetav = local_zetaos * sdens * CLV_HBARC;
+    real dcs = 1.0f / 3.0f - cs2;
+    real one_over_taubulk = 14.55f * dcs * dcs * temperature / (cmax<real>(acu, local_zetaos) * CLV_HBARC);
+    real bulkNS = -zetav * theta;
+    if (u[0] > 10000.0f) bulkNS = 0.0f;
+    real bc = pc[10];
+    real srcB = div_by<real>(bc * theta, (real)3.0f, rc.three) - div_by<real>(bc * u[0], tau, tc.rtau) +
+                0.8f * dcs * pisig;
+    S10[10] += srcB;
+    real b_old = b.pi1[10 * ld + I] * u_old[0];
+    pinew[10] = (b_old + div_step(S10[10] * p.DT, step) + p.DT * one_over_taubulk * bulkNS) /
+                (u_new[0] + p.DT * one_over_taubulk);
+  }
   real pre = eosP<real>(p, e2s0);
   real T00 = (e2s0 + pre) * u_new[0] * u_new[0] - pre;
   uint8_t good = 1;
+  constexpr int NPI = BULK ? 11 : 10;
   if (max_pimn_abs > T00) {
 #pragma unroll
-    for (int m = 0; m < 10; m++) pinew[m] = 0.0f;
+    for (int m = 0; m < NPI; m++) pinew[m] = 0.0f;
     good = 0;
   }
 #pragma unroll
-  for (int m = 0; m < 10; m++) b.pinew[m * ld + I] = pinew[m];
+  for (int m = 0; m < NPI; m++) b.pinew[m * ld + I] = pinew[m];
   b.goodcell[I] = good;
 }
 
 // update_ev (kernel_visc.cl:322-393) for cell I: pin = pi^{tau mu} at the
 // start of the step, S4 the KT sources; the new pi^{tau mu} comes from pinew
 // (fused pi update) or from pi_new_in. Also get_udiff and the edmax key.
-template <class real, bool FUSED_PI>
+// With BULK, pin[4] is Pi at the start of the step and the pressure of the
+// old and the new state is P(e) + Pi.
+template <class real, bool FUSED_PI, bool BULK>
 __device__ __forceinline__ void ev_update(const Params& p, const ViscBuffers<real>& b, int step,
-                                          const TauConst<real>& tc, long long I, const real pin[4], const real S4[4],
-                                          const real pinew[10]) {
+                                          const TauConst<real>& tc, long long I, const real pin[5], const real S4[4],
+                                          const real pinew[11]) {
   const long long ld = p.ld;
   const real acu = Acu<real>::v;
   const real tau = tc.tau;
@@ -193,6 +228,7 @@ __device__ __forceinline__ void ev_update(const Params& p, const ViscBuffers<rea
   for (int c = 0; c < 4; c++) e1[c] = b.ev1[c * ld + I];
   real ed = e1[0], vx = e1[1], vy = e1[2], vz = e1[3];
   real pressure = eosP<real>(p, ed);
+  if (BULK) pressure = pressure + pin[4];
   real u0 = gamma3<real>(vx, vy, vz);
   real umu[4] = {u0 * 1.0f, u0 * vx, u0 * vy, u0 * vz};
   real old_time = tau - (step - 1) * p.DT;
@@ -202,6 +238,8 @@ __device__ __forceinline__ void ev_update(const Params& p, const ViscBuffers<rea
     real g0 = c == 0 ? (real)1.0f : (real)0.0f;
     T0m[c] = ((ed + pressure) * u0 * umu[c] - pressure * g0 + pin[c]) * old_time;
   }
+  real bnew = 0.0f;
+  if (BULK) bnew = FUSED_PI ? pinew[10] : b.pi2in[10 * ld + I];
 #pragma unroll
   for (int c = 0; c < 4; c++) {
     real pim2 = FUSED_PI ? pinew[c] : b.pi2in[c * ld + I];
@@ -219,7 +257,7 @@ __device__ __forceinline__ void ev_update(const Params& p, const ViscBuffers<rea
     T03 *= SCALE_COEF * T00 / M;
     M = SCALE_COEF * T00;
   }
-  real ed_find = root_newton<real>(p, T00, M);
+  real ed_find = root_newton<real, BULK>(p, T00, M, bnew);
   if (ed_find < acu) {
     T01 = 0.0f;
     T02 = 0.0f;
@@ -227,6 +265,7 @@ __device__ __forceinline__ void ev_update(const Params& p, const ViscBuffers<rea
   }
   ed_find = cmax<real>(0.0f, ed_find);
   real pr = eosP<real>(p, ed_find);
+  if (BULK) pr = pr + bnew;
   real epv = cmax<real>(acu, T00 + pr);
   const real repv = (real)1.0f / epv;
   real en[4] = {ed_find, div_by<real>(T01, epv, repv), div_by<real>(T02, epv, repv), div_by<real>(T03, epv, repv)};
@@ -244,13 +283,14 @@ __device__ __forceinline__ void ev_update(const Params& p, const ViscBuffers<rea
 }
 
 // --------------------------------------------------------------- viscous
-template <class real, bool DO_IS, bool DO_KT, bool COUPLED>
-__global__ void __launch_bounds__(128) visc_stage_kernel(Params p, ViscBuffers<real> b, int step, TauConst<real> tc) {
+// One cell of the fused viscous stage. With BULK the pi fields carry an
+// eleventh plane, the bulk pressure Pi, and the sources an eleventh IS term.
+template <class real, bool DO_IS, bool DO_KT, bool COUPLED, bool BULK>
+__device__ __forceinline__ void visc_stage_cell(const Params& p, const ViscBuffers<real>& b, int step,
+                                                const TauConst<real>& tc, long long I) {
   const real tau = tc.tau;
   const Recips<real>& rc = recips<real>(p);
-  const long long N = (long long)p.nx * p.ny * p.nz;
-  const long long I = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (I >= N) return;
+  constexpr int NPI = BULK ? 11 : 10;
   const long long ld = p.ld;
   const int k = (int)(I % p.nz);
   const long long t = I / p.nz;
@@ -262,26 +302,29 @@ __global__ void __launch_bounds__(128) visc_stage_kernel(Params p, ViscBuffers<r
   real e0[4];
 #pragma unroll
   for (int c = 0; c < 4; c++) e0[c] = b.ev_st[c * ld + I];
-  real pc[10];
+  real pc[11];
 #pragma unroll
-  for (int m = 0; m < 10; m++) pc[m] = b.pi_st[m * ld + I];
+  for (int m = 0; m < NPI; m++) pc[m] = b.pi_st[m * ld + I];
+  if (!BULK) pc[10] = 0.0f;
   // pi at the start of the step: read before this thread's pi_new store,
   // which may alias it (in-place second stage)
-  real pin[4];
+  real pin[5];
 #pragma unroll
   for (int c = 0; c < 4; c++) pin[c] = DO_KT ? b.pin[c * ld + I] : (real)0.0f;
+  pin[4] = (BULK && DO_KT) ? b.pin[10 * ld + I] : (real)0.0f;
 
-  real S4[4], S10[10];
+  real S4[4], S10[11];
   if (step == 1) {
 #pragma unroll
     for (int c = 0; c < 4; c++) S4[c] = 0.0f;
 #pragma unroll
-    for (int m = 0; m < 10; m++) S10[m] = 0.0f;
+    for (int m = 0; m < 11; m++) S10[m] = 0.0f;
   } else {
 #pragma unroll
     for (int c = 0; c < 4; c++) S4[c] = DO_KT ? b.src[c * ld + I] : (real)0.0f;
 #pragma unroll
-    for (int m = 0; m < 10; m++) S10[m] = DO_IS ? b.src[(4 + m) * ld + I] : (real)0.0f;
+    for (int m = 0; m < NPI; m++) S10[m] = DO_IS ? b.src[(4 + m) * ld + I] : (real)0.0f;
+    if (!BULK) S10[10] = 0.0f;
   }
 
   // Christoffel terms
@@ -298,7 +341,7 @@ __global__ void __launch_bounds__(128) visc_stage_kernel(Params p, ViscBuffers<r
   if (DO_KT) {  // kernel_visc.cl:24-50
     real ed = e0[0], vx = e0[1], vy = e0[2], vz = e0[3];
     real u0 = gamma3<real>(vx, vy, vz);
-    real bulkpi = 0.0f;
+    real bulkpi = BULK ? pc[10] : (real)0.0f;  // fills the reference's placeholder, kernel_visc.cl:31-33
     real pressure = eosP<real>(p, ed) + bulkpi;
     real Tzz_tilde = (ed + pressure) * u0 * u0 * vz * vz + pressure + pc[pidx(3, 3)];
     real Ttz_tilde = (ed + pressure) * u0 * u0 * vz + pc[pidx(0, 3)];
@@ -355,6 +398,7 @@ __global__ void __launch_bounds__(128) visc_stage_kernel(Params p, ViscBuffers<r
       for (int d = 0; d < 5; d++) {
         const long long J = I + st.off[d];
         pr[d] = eosP<real>(p, E[d][0]);
+        if (BULK) pr[d] = pr[d] + ((d == 2) ? pc[10] : b.pi_st[10 * ld + J]);
         real A = (E[d][0] + pr[d]) * u0[d];
         real u4[4] = {(real)1.0f * u0[d], E[d][1] * u0[d], E[d][2] * u0[d], E[d][3] * u0[d]};
 #pragma unroll
@@ -424,9 +468,9 @@ __global__ void __launch_bounds__(128) visc_stage_kernel(Params p, ViscBuffers<r
         grad[2][2] = grad[2][2] + div_by<real>((real)0.0f * u0[2], tau, tc.rtau);
         grad[2][3] = grad[2][3] + div_by<real>((real)1.0f * u0[2], tau, tc.rtau);
       }
-      // KT flux of u0*pi^{mn}, kt1d_real (helper.h:249-285)
+      // KT flux of u0*pi^{mn}, kt1d_real (helper.h:249-285); with BULK also of u0*Pi
 #pragma unroll 2
-      for (int m = 0; m < 10; m++) {
+      for (int m = 0; m < NPI; m++) {
         real U[5];
 #pragma unroll
         for (int d = 0; d < 5; d++) U[d] = u0[d] * ((d == 2) ? pc[m] : b.pi_st[m * ld + I + st.off[d]]);
@@ -452,9 +496,9 @@ __global__ void __launch_bounds__(128) visc_stage_kernel(Params p, ViscBuffers<r
     }
   }
 
-  real pinew[10];
-  if (DO_IS) pi_update<real, COUPLED>(p, b, step, tc, I, e0, pc, grad, S10, pinew);
-  if (DO_KT) ev_update<real, DO_IS>(p, b, step, tc, I, pin, S4, pinew);
+  real pinew[11];
+  if (DO_IS) pi_update<real, COUPLED, BULK>(p, b, step, tc, I, e0, pc, grad, S10, pinew);
+  if (DO_KT) ev_update<real, DO_IS, BULK>(p, b, step, tc, I, pin, S4, pinew);
 
   if (b.write_src) {
     if (DO_KT)
@@ -462,8 +506,16 @@ __global__ void __launch_bounds__(128) visc_stage_kernel(Params p, ViscBuffers<r
       for (int c = 0; c < 4; c++) b.src[c * ld + I] = S4[c];
     if (DO_IS)
 #pragma unroll
-      for (int m = 0; m < 10; m++) b.src[(4 + m) * ld + I] = S10[m];
+      for (int m = 0; m < NPI; m++) b.src[(4 + m) * ld + I] = S10[m];
   }
+}
+
+template <class real, bool DO_IS, bool DO_KT, bool COUPLED, bool BULK>
+__global__ void __launch_bounds__(128) visc_stage_kernel(Params p, ViscBuffers<real> b, int step, TauConst<real> tc) {
+  const long long N = (long long)p.nx * p.ny * p.nz;
+  const long long I = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (I >= N) return;
+  visc_stage_cell<real, DO_IS, DO_KT, COUPLED, BULK>(p, b, step, tc, I);
 }
 
 // ----------------------------------------------------------------- ideal

@@ -245,13 +245,16 @@ __global__ void __launch_bounds__(TJ * TK, MINB)
       const long long I = ((long long)i * p.ny + jj) * p.nz + kk;
       const real* Cc = &s.C[0][cself];
       real e0[4] = {Cc[RF_E * G::NC], Cc[RF_VX * G::NC], Cc[RF_VY * G::NC], Cc[RF_VZ * G::NC]};
-      real pc[10];
+      real pc[11];  // component 10 (bulk) unused: this kernel has no bulk sector
 #pragma unroll
       for (int m = 0; m < 10; m++) pc[m] = Cc[(RF_PI + m) * G::NC];
-      real pin[4];
+      real pin[5];
 #pragma unroll
       for (int c = 0; c < 4; c++) pin[c] = DO_KT ? b.pin[c * ld + I] : (real)0.0f;
-      real S4[4], S10[10];
+      pin[4] = 0.0f;
+      pc[10] = 0.0f;
+      real S4[4], S10[11];
+      S10[10] = 0.0f;
       if (step == 1) {
 #pragma unroll
         for (int c = 0; c < 4; c++) S4[c] = 0.0f;
@@ -312,7 +315,7 @@ __global__ void __launch_bounds__(TJ * TK, MINB)
         }
       }
 
-      real pinew[10];
+      real pinew[11];
       if (DO_IS) {
         // velocity gradients, kernel_IS.cl:134-137 / 217-220 / 299-304
         real grad[3][4];
@@ -343,7 +346,7 @@ __global__ void __launch_bounds__(TJ * TK, MINB)
 #pragma unroll
           for (int c = 0; c < 4; c++) umu_prev[c] = umc[c];
         }
-        pi_update<real, COUPLED>(p, b, step, tc, I, e0, pc, grad, S10, pinew);
+        pi_update<real, COUPLED, false>(p, b, step, tc, I, e0, pc, grad, S10, pinew);
       } else {
         real u0c = Cc[RF_U0 * G::NC];
         umu_prev[0] = u0c * 1.0f;
@@ -351,7 +354,7 @@ __global__ void __launch_bounds__(TJ * TK, MINB)
         umu_prev[2] = u0c * e0[2];
         umu_prev[3] = u0c * e0[3];
       }
-      if (DO_KT) ev_update<real, DO_IS>(p, b, step, tc, I, pin, S4, pinew);
+      if (DO_KT) ev_update<real, DO_IS, false>(p, b, step, tc, I, pin, S4, pinew);
       if (b.write_src) {
         if (DO_KT)
 #pragma unroll

@@ -8,6 +8,11 @@ sequence is the reference's: pi is initialised from the still-empty state and
 an ideal stage is run on it (visc.py:101-102), so the first time step sees the
 same pi and d_ev[2] as the reference's.
 
+Bulk viscosity is an extension (the reference has none): with ZETAOS_MAX > 0
+the pi buffers carry an eleventh plane, the bulk pressure Pi, which the same
+kernels advance (14-moment relaxation, P + Pi in T^{mu nu}); bulk_to_host()
+reads it. ZETAOS_MAX = 0 (the default) leaves every result unchanged.
+
 IS_stepUpdate and visc_stepUpdate launch the two halves of a Runge-Kutta
 stage separately, as the reference does. evolve() launches one fused kernel
 per stage that does both halves in one pass over memory; it skips the
@@ -22,6 +27,7 @@ import numpy as np
 import torch
 
 from . import _lib
+from .config import float_literal
 from .ideal import CLIdeal
 
 
@@ -44,15 +50,24 @@ class CLVisc(object):
             flags |= _lib.CLV_FLAG_PIMN_OMEGA_COUPLING
         if self.cfg.omega_omega_coupling:
             flags |= _lib.CLV_FLAG_OMEGA_OMEGA_COUPLING
+        self.bulk = float(getattr(self.cfg, 'ZETAOS_MAX', 0.0)) > 0.0
+        p = self.ideal.params
+        p.zetaos_max = float_literal(getattr(self.cfg, 'ZETAOS_MAX', 0.0))
+        p.zetaos_t0 = float_literal(getattr(self.cfg, 'ZETAOS_T0', 0.18))
+        p.zetaos_width = float_literal(getattr(self.cfg, 'ZETAOS_WIDTH', 0.02))
+        p.zetaos_skew = float_literal(getattr(self.cfg, 'ZETAOS_SKEW', 0.0))
+        if self.bulk:
+            flags |= _lib.CLV_FLAG_BULK
         self.ideal.params.flags = flags
         self.params = self.ideal.params
 
         z = lambda w: torch.zeros((w, self.ld), dtype=self.dtype, device=self.device)
-        self.d_pi = [z(10), z(10), z(10)]
-        self.d_src = z(14)        # d_Src (planes 0..3) and d_IS_src (planes 4..13)
+        npi = 11 if self.bulk else 10  # plane 10: the bulk pressure
+        self.d_pi = [z(npi), z(npi), z(npi)]
+        self.d_src = z(4 + npi)   # d_Src (planes 0..3), d_IS_src (planes 4..13), bulk source (14)
         self.d_udiff = z(4)
         self.d_goodcell = torch.ones(self.ld, dtype=torch.uint8, device=self.device)
-        self.d_pi_old = z(10)
+        self.d_pi_old = z(npi)
         self.d_pi_sf = torch.zeros((self.ideal.hypersf_capacity, 10), dtype=self.dtype, device=self.device)
         self._key = torch.zeros(1, dtype=torch.int64, device=self.device)
         self.IS_initialize()
@@ -171,7 +186,14 @@ class CLVisc(object):
 
     def pi_to_host(self, slot=1):
         """d_pi[slot] as (cells, 10)."""
-        return self.ideal.field_to_host(self.d_pi[slot])
+        return self.ideal.field_to_host(self.d_pi[slot][:10])
+
+    def bulk_to_host(self, slot=1):
+        """The bulk pressure Pi of d_pi[slot] as (cells,); zeros without the
+        bulk sector."""
+        if not self.bulk:
+            return np.zeros(self.size, self.cfg.real)
+        return self.d_pi[slot][10, :self.size].cpu().numpy()
 
     def evolve(self, max_loops=1000, save_hypersf=True, save_bulk=False, plot_bulk=False, save_pi=True,
                force_run_to_maxloop=False, save_vorticity=False, jet_eloss_src=None, debug=False):
@@ -179,7 +201,8 @@ class CLVisc(object):
         if save_vorticity:
             raise NotImplementedError('vorticity output is not part of this backend')
         c = self.cfg
-        if c.ETAOS_YMIN < 1.0E-6 and c.ETAOS_LEFT_SLOP < 1.0E-6 and c.ETAOS_RIGHT_SLOP < 1.0E-6:
+        if (c.ETAOS_YMIN < 1.0E-6 and c.ETAOS_LEFT_SLOP < 1.0E-6 and c.ETAOS_RIGHT_SLOP < 1.0E-6
+                and not self.bulk):
             # visc.py:483-489: ideal evolution when eta/s vanishes
             self.ideal.evolve(max_loops, save_hypersf, save_bulk, plot_bulk, force_run_to_maxloop, jet_eloss_src)
             self.save_pimn_sf(set_to_zero=True)

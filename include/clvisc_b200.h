@@ -11,7 +11,8 @@
  *     of `ld` elements each (plane c starts at ptr + c*ld), and cell
  *     I = i*NY*NZ + j*NZ + k, the reference's order (kernel_visc.cl:145).
  *     ev has 4 planes (ed, vx, vy, veta); pi has 10 planes in the reference's
- *     packed order 00 01 02 03 11 12 13 22 23 33 (helper.h:31).
+ *     packed order 00 01 02 03 11 12 13 22 23 33 (helper.h:31), and an
+ *     eleventh, the bulk pressure Pi, when CLV_FLAG_BULK is set.
  *   - The element type is float when clv_params.precision == 4 and double
  *     when it is 8 (the reference's use_float32 flag, config.py:200).
  *   - `stream` is a cudaStream_t passed as void* (NULL = legacy stream).
@@ -39,6 +40,15 @@ extern "C" {
 #define CLV_FLAG_GUBSER_VISC_TEST 2
 #define CLV_FLAG_PIMN_OMEGA_COUPLING 4
 #define CLV_FLAG_OMEGA_OMEGA_COUPLING 8
+/* Bulk viscosity, an extension with no counterpart in the reference (its
+ * kernel_visc.cl:31-33 keeps a zero placeholder for the bulk pressure): pi
+ * fields carry an eleventh plane Pi and the stage sources a fifteenth.
+ * zeta/s(T) = zetaos_max w^2 / (w^2 + (T - zetaos_t0)^2) with
+ * w = zetaos_width (1 + zetaos_skew sign(T - zetaos_t0)); Pi relaxes by the
+ * 14-moment equation tau_Pi D Pi + Pi = -zeta theta - 2/3 tau_Pi Pi theta
+ * + 8/5 (1/3 - cs2) tau_Pi pi:sigma, tau_Pi = zeta / (14.55 (1/3 - cs2)^2 (e+P)),
+ * and P + Pi replaces P in T^{mu nu}. */
+#define CLV_FLAG_BULK 16
 
 /* parts of a viscous stage (visc.py:287 IS_stepUpdate, visc.py:232 visc_stepUpdate) */
 #define CLV_PART_IS 1
@@ -59,13 +69,14 @@ typedef struct clv_params {
   int eos_num_ed, eos_nrow, eos_ncol;
   const float *eos_table; /* device, eos_nrow*eos_ncol texels of (cs2, p, T, s) */
   int flags;              /* CLV_FLAG_* */
+  float zetaos_max, zetaos_t0, zetaos_width, zetaos_skew; /* bulk sector (CLV_FLAG_BULK) */
 } clv_params;
 
 /* Buffers of one viscous Runge-Kutta stage. `step` is 1 or 2 as in
  * visc.py:536-543; d_ev[], d_pi[] are the reference's three-slot buffers. */
 typedef struct clv_visc_buffers {
   const void *ev_st;     /* d_ev[step]: stencil input, 4 planes                */
-  const void *pi_st;     /* d_pi[step]: stencil input, 10 planes               */
+  const void *pi_st;     /* d_pi[step]: stencil input, 10 planes (11: bulk)    */
   const void *ev1;       /* d_ev[1]                                            */
   const void *ev2_ed;    /* plane 0 of d_ev[2] (read by step 1's pi update)    */
   const void *pi1;       /* d_pi[1]: start point of the pi update              */
@@ -73,7 +84,7 @@ typedef struct clv_visc_buffers {
   const void *pi_new_in; /* d_pi[3-step]: read when CLV_PART_IS is not fused   */
   void *ev_new;          /* d_ev[3-step]                                       */
   void *pi_new;          /* d_pi[3-step]                                       */
-  void *src;             /* 14 planes: d_Src (4) then d_IS_src (10)            */
+  void *src;             /* 14 planes: d_Src (4) then d_IS_src (10); 15: bulk  */
   void *udiff;           /* 4 planes                                           */
   unsigned char *goodcell; /* 1 byte per cell (the reference's d_goodcell)     */
   void *edmax_key;       /* optional: running max of ev_new energy density     */
@@ -113,7 +124,8 @@ int clv_ideal_stage(const clv_params *p, int step, double tau, const void *ev_st
 int clv_visc_stage(const clv_params *p, int step, double tau, int parts, const clv_visc_buffers *b, void *stream);
 
 /* visc_initialize (kernel_IS.cl:10-36): Navier-Stokes pi from ev, udiff = 0,
- * goodcell = 1. Components of pi1 other than 11, 22, 33 are left as they are. */
+ * goodcell = 1. Components of pi1 other than 11, 22, 33 are left as they are.
+ * With CLV_FLAG_BULK also Pi = -zeta / tau (Navier-Stokes, Bjorken flow). */
 int clv_visc_initialize(const clv_params *p, void *pi1, unsigned char *goodcell, void *udiff, const void *ev,
                         double tau, void *stream);
 

@@ -129,7 +129,8 @@ void ideal_update_ev(const Consts& c, real* evnew, const real* ev1, const real* 
 // ============================================================= kernel_visc.cl
 // kernel_visc.cl:11-53
 template <class real>
-void visc_christoffel(const Consts& c, real* SrcT, const real* ev, const real* pi, real tau, int step) {
+void visc_christoffel(const Consts& c, real* SrcT, const real* ev, const real* pi, real tau, int step,
+                      const real* bulk = nullptr) {
   Helper<real> H(c);
   (void)tau;
   const long N = (long)ncells(c);
@@ -139,7 +140,7 @@ void visc_christoffel(const Consts& c, real* SrcT, const real* ev, const real* p
     V4<real> e_v = ld4(ev, I);
     real ed = e_v.s0, vx = e_v.s1, vy = e_v.s2, vz = e_v.s3;
     real u0 = Helper<real>::gamma(vx, vy, vz);
-    real bulkpi = 0.0f;
+    real bulkpi = bulk ? bulk[I] : (real)0.0f;  // the bulk sector fills the reference's placeholder
     real pressure = H.E.P(ed) + bulkpi;
     real Tzz_tilde = (ed + pressure) * u0 * u0 * vz * vz + pressure + pi[10 * I + idx(3, 3)];
     real Ttz_tilde = (ed + pressure) * u0 * u0 * vz + pi[10 * I + idx(0, 3)];
@@ -156,12 +157,13 @@ void visc_christoffel(const Consts& c, real* SrcT, const real* ev, const real* p
 // kernel_visc.cl:68-127
 template <class real>
 V4<real> kt1d_visc(const Helper<real>& H, const V4<real> ev[5], const V4<real> pim0[5], const V4<real> pimi[5],
-                   real vip_half, real vim_half, real tau, int along) {
+                   real vip_half, real vim_half, real tau, int along, const real* bulk5 = nullptr) {
   const real TH = CLVO_THETA;
   real pr[5];
   V4<real> Q[5];
   for (int i = 0; i < 5; i++) {
     pr[i] = H.E.P(ev[i].s0);
+    if (bulk5) pr[i] = pr[i] + bulk5[i];  // bulk sector: P -> P + Pi
     Q[i] = smul<real>(tau, Helper<real>::t0m(ev[i], pr[i]) + pim0[i]);
   }
   V4<real> DA0, DA1;
@@ -205,7 +207,8 @@ V4<real> kt1d_visc(const Helper<real>& H, const V4<real> ev[5], const V4<real> p
 
 // kernel_visc.cl:131-318 (kt_src_alongx/y/z)
 template <class real>
-void visc_along(const Consts& c, int axis, real* Src, const real* ev, const real* pi, real tau) {
+void visc_along(const Consts& c, int axis, real* Src, const real* ev, const real* pi, real tau,
+                const real* bulk = nullptr) {
   Helper<real> H(c);
   const int n0 = axis == 0 ? c.NY : c.NX;
   const int n1 = axis == 2 ? c.NY : c.NZ;
@@ -221,16 +224,18 @@ void visc_along(const Consts& c, int axis, real* Src, const real* ev, const real
         else { i = a; j = b; k = t; }
         size_t IND = cell(c, i, j, k);
         V4<real> e[5], p0[5], pr_[5];
+        real b5[5];
         for (int d = -2; d <= 2; d++) {
           size_t J = nbr(c, i, j, k, axis, d);
           e[d + 2] = ld4(ev, J);
+          b5[d + 2] = bulk ? bulk[J] : (real)0.0f;
           const real* p = pi + 10 * J;
           p0[d + 2] = V4<real>{p[0], p[1], p[2], p[3]};
           pr_[d + 2] = V4<real>{p[idx(r, 0)], p[idx(r, 1)], p[idx(r, 2)], p[idx(r, 3)]};
         }
         real vip_half = 0.5f * (comp(e[2], r) + comp(e[3], r));
         real vim_half = 0.5f * (comp(e[1], r) + comp(e[2], r));
-        V4<real> f = kt1d_visc(H, e, p0, pr_, vip_half, vim_half, tau, axis);
+        V4<real> f = kt1d_visc(H, e, p0, pr_, vip_half, vim_half, tau, axis, bulk ? b5 : nullptr);
         V4<real> s = ld4(Src, IND);
         if (axis == 0) st4(Src, IND, s - vdiv<real>(f, (real)c.DX));
         else if (axis == 1) st4(Src, IND, s - vdiv<real>(f, (real)c.DY));
@@ -241,7 +246,7 @@ void visc_along(const Consts& c, int axis, real* Src, const real* ev, const real
 // kernel_visc.cl:322-393
 template <class real>
 void visc_update_ev(const Consts& c, real* evnew, const real* ev1, const real* pi1, const real* pi2, const real* Src,
-                    real tau, int step) {
+                    real tau, int step, const real* bulk1 = nullptr, const real* bulk2 = nullptr) {
   Helper<real> H(c);
   const real acu = Acu<real>::v;
   const long N = (long)ncells(c);
@@ -250,6 +255,7 @@ void visc_update_ev(const Consts& c, real* evnew, const real* ev1, const real* p
     V4<real> e_v = ld4(ev1, I);
     real ed = e_v.s0, vx = e_v.s1, vy = e_v.s2, vz = e_v.s3;
     real pressure = H.E.P(ed);
+    if (bulk1) pressure = pressure + bulk1[I];  // bulk sector
     real u0 = Helper<real>::gamma(vx, vy, vz);
     V4<real> umu = smul<real>(u0, V4<real>{1.0f, vx, vy, vz});
     V4<real> pim0 = V4<real>{pi1[10 * I + 0], pi1[10 * I + 1], pi1[10 * I + 2], pi1[10 * I + 3]};
@@ -270,7 +276,7 @@ void visc_update_ev(const Consts& c, real* evnew, const real* ev1, const real* p
       M = SCALE_COEF * T00;
     }
     real ed_find;
-    H.rootFinding_newton(&ed_find, T00, M);
+    H.rootFinding_newton(&ed_find, T00, M, nullptr, bulk2 ? bulk2 + I : nullptr);
     if (ed_find < acu) {
       T01 = 0.0f;
       T02 = 0.0f;
@@ -278,6 +284,7 @@ void visc_update_ev(const Consts& c, real* evnew, const real* ev1, const real* p
     }
     ed_find = cl_max<real>(0.0f, ed_find);
     real pr = H.E.P(ed_find);
+    if (bulk2) pr = pr + bulk2[I];
     real epv = cl_max<real>(acu, T00 + pr);
     st4(evnew, I, V4<real>{ed_find, T01 / epv, T02 / epv, T03 / epv});
   }
@@ -286,7 +293,8 @@ void visc_update_ev(const Consts& c, real* evnew, const real* ev1, const real* p
 // =============================================================== kernel_IS.cl
 // kernel_IS.cl:10-36
 template <class real>
-void visc_initialize(const Consts& c, real* pi1, real* goodcell, real* udiff, const real* ev, real tau) {
+void visc_initialize(const Consts& c, real* pi1, real* goodcell, real* udiff, const real* ev, real tau,
+                     real* bulk1 = nullptr) {
   Helper<real> H(c);
   const long N = (long)ncells(c);
 #pragma omp parallel for schedule(static)
@@ -298,6 +306,10 @@ void visc_initialize(const Consts& c, real* pi1, real* goodcell, real* udiff, co
     pi1[10 * I + idx(1, 1)] = tmp;
     pi1[10 * I + idx(2, 2)] = tmp;
     pi1[10 * I + idx(3, 3)] = -2.0f * tmp;
+    if (bulk1) {  // bulk sector: Navier-Stokes value for Bjorken flow, theta = 1/tau
+      real zetav = H.zetaos(cpTs.s2) * cpTs.s3 * CLVO_HBARC;
+      bulk1[I] = -zetav / tau;
+    }
     st4(udiff, I, V4<real>{0.0f, 0.0f, 0.0f, 0.0f});
     goodcell[I] = 1.0f;
   }
@@ -305,7 +317,8 @@ void visc_initialize(const Consts& c, real* pi1, real* goodcell, real* udiff, co
 
 // kernel_IS.cl:41-67
 template <class real>
-void visc_src_christoffel(const Consts& c, real* Src, const real* pi1, const real* ev, real tau, int step) {
+void visc_src_christoffel(const Consts& c, real* Src, const real* pi1, const real* ev, real tau, int step,
+                          real* SrcB = nullptr) {
   const long N = (long)ncells(c);
 #pragma omp parallel for schedule(static)
   for (long I = 0; I < N; I++) {
@@ -313,6 +326,7 @@ void visc_src_christoffel(const Consts& c, real* Src, const real* pi1, const rea
     const real* p = pi1 + 10 * I;
     if (step == 1)
       for (int mn = 0; mn < 10; mn++) S[mn] = 0.0f;
+    if (SrcB && step == 1) SrcB[I] = 0.0f;  // bulk sector: no Christoffel term
     V4<real> e_v = ld4(ev, I);
     real uz = e_v.s3 * Helper<real>::gamma(e_v.s1, e_v.s2, e_v.s3);
     S[0] -= 2.0f * uz * p[idx(0, 3)] / tau;
@@ -327,7 +341,8 @@ void visc_src_christoffel(const Consts& c, real* Src, const real* pi1, const rea
 
 // kernel_IS.cl:74-318 (visc_src_alongx/y/z)
 template <class real>
-void visc_src_along(const Consts& c, int axis, real* Src, real* ud, const real* pi1, const real* ev, real tau) {
+void visc_src_along(const Consts& c, int axis, real* Src, real* ud, const real* pi1, const real* ev, real tau,
+                    real* SrcB = nullptr, const real* bulk1 = nullptr) {
   Helper<real> H(c);
   const real TH = CLVO_THETA;
   const int n0 = axis == 0 ? c.NY : c.NX;
@@ -372,6 +387,12 @@ void visc_src_along(const Consts& c, int axis, real* Src, real* ud, const real* 
                                            u0[4] * pi1[10 * Jn[4] + mn], v_mh, v_ph, lam_mh, lam_ph);
           real D = axis == 0 ? (real)c.DX : (axis == 1 ? (real)c.DY : tau * c.DZ);
           Src[10 * IND + mn] = Src[10 * IND + mn] - f / D;
+        }
+        if (SrcB) {  // bulk sector: KT flux of u0 * Pi, the eleventh component
+          real f = Helper<real>::kt1d_real(u0[0] * bulk1[Jn[0]], u0[1] * bulk1[Jn[1]], u0[2] * bulk1[Jn[2]],
+                                           u0[3] * bulk1[Jn[3]], u0[4] * bulk1[Jn[4]], v_mh, v_ph, lam_mh, lam_ph);
+          real D = axis == 0 ? (real)c.DX : (axis == 1 ? (real)c.DY : tau * c.DZ);
+          SrcB[IND] = SrcB[IND] - f / D;
         }
       }
 }
@@ -435,11 +456,19 @@ real omega_omega(int lam, int mu, int nu, const real omega[6], const real u[4]) 
   return firstTerm + secondTerm;
 }
 
+// weight of pi^{mu nu} sigma^{mu nu} in the full contraction over mu <= nu:
+// g_{mu mu} g_{nu nu}, doubled off the diagonal (bulk sector)
+template <class real> inline real pisig_weight(int mu, int nu) {
+  real w = (mu == nu) ? (real)1.0f : (real)2.0f;
+  return ((mu == 0) != (nu == 0)) ? -w : w;
+}
+
 // kernel_IS.cl:501-709
 template <class real>
 void update_pimn(const Consts& c, real* pinew, real* goodcell, const real* pi1, const real* pistep, const real* ev1,
                  const real* ev2, const real* udiff, const real* udx, const real* udy, const real* udz, real* Src,
-                 real tau, int step) {
+                 real tau, int step, real* bulknew = nullptr, const real* bulk1 = nullptr,
+                 const real* bulkstep = nullptr, real* SrcB = nullptr) {
   Helper<real> H(c);
   const real acu = Acu<real>::v;
   const long N = (long)ncells(c);
@@ -498,12 +527,14 @@ void update_pimn(const Consts& c, real* pinew, real* goodcell, const real* pi1, 
     }
     real sigma;
     real max_pimn_abs = 0.0f;
+    real pisig = 0.0f;  // bulk sector: pi^{mu nu} sigma_{mu nu}, sigma as below (twice the usual shear tensor)
     for (int mu = 0; mu < 4; mu++)
       for (int nu = mu; nu < 4; nu++) {
         sigma = dot(gm<real>(mu), da[nu]) + dot(gm<real>(nu), da[mu]) - (u[mu] * DU[nu] + u[nu] * DU[mu]) -
                 2.0f / 3.0f * (gmn<real>(mu, nu) - u[mu] * u[nu]) * theta;
         int mn = idx(mu, nu);
         if (u[0] > 10000.0f) sigma = 0.0f;
+        if (bulknew) pisig = pisig + pisig_weight<real>(mu, nu) * pi2[mn] * sigma;
         real piNS = etav * sigma;
         real pi_old = pi1[10 * I + mn] * u_old.s0;
         real src = -pi2[mn] * theta / 3.0f - pi2[mn] * u[0] / tau;
@@ -531,11 +562,36 @@ void update_pimn(const Consts& c, real* pinew, real* goodcell, const real* pi1, 
         if (std::fabs(pi_old) > max_pimn_abs) max_pimn_abs = std::fabs(pi_old);
         pinew[10 * I + mn] = pi_old;
       }
+    if (bulknew) {
+      // Bulk sector (no counterpart in the reference): the 14-moment
+      // relaxation equation of Denicol, Niemi, Molnar and Rischke (PRD 85,
+      // 114047 (2012)), tau_Pi D Pi + Pi = -zeta theta - delta_PiPi Pi theta
+      // + lambda_Pipi pi^{mu nu} sigma_{mu nu}, with delta_PiPi = 2/3 tau_Pi,
+      // lambda_Pipi = 8/5 (1/3 - cs2) tau_Pi and
+      // tau_Pi = zeta / (14.55 (1/3 - cs2)^2 (e + P)), written like the shear
+      // update above for the conserved density u0 * Pi:
+      // d(u0 Pi) + div(v u0 Pi) = Pi theta / 3 - Pi u0 / tau
+      //   + 4/5 (1/3 - cs2) pisig - (Pi - Pi_NS) / tau_Pi.
+      real local_zetaos = H.zetaos(temperature);
+      real zetav = local_zetaos * cpTs.s3 * CLVO_HBARC;
+      real dcs = 1.0f / 3.0f - cpTs.s0;
+      real one_over_taubulk = 14.55f * dcs * dcs * temperature / (cl_max<real>(acu, local_zetaos) * CLVO_HBARC);
+      real bulkNS = -zetav * theta;
+      if (u[0] > 10000.0f) bulkNS = 0.0f;
+      real bc = bulkstep[I];
+      real srcB = bc * theta / 3.0f - bc * u[0] / tau + 0.8f * dcs * pisig;
+      SrcB[I] += srcB;
+      real b_old = bulk1[I] * u_old.s0;
+      b_old = (b_old + SrcB[I] * c.DT / step + c.DT * one_over_taubulk * bulkNS) /
+              (u_new.s0 + c.DT * one_over_taubulk);
+      bulknew[I] = b_old;
+    }
     real pre = H.E.P(e_v2.s0);
     real T00 = (e_v2.s0 + pre) * u_new.s0 * u_new.s0 - pre;
     goodcell[I] = 1.0f;
     if (max_pimn_abs > T00) {
       for (int mn = 0; mn < 10; mn++) pinew[10 * I + mn] = 0.0f;
+      if (bulknew) bulknew[I] = 0.0f;
       goodcell[I] = 0.0f;
     }
   }
@@ -831,31 +887,36 @@ extern "C" {
   void clvo_ideal_update_ev_##sfx(const Consts* c, real* evnew, const real* ev1, const real* Src, real tau, int step) { \
     clvo::ideal_update_ev<real>(*c, evnew, ev1, Src, tau, step);                                                        \
   }                                                                                                                     \
-  void clvo_visc_christoffel_##sfx(const Consts* c, real* Src, const real* ev, const real* pi, real tau, int step) {  \
-    clvo::visc_christoffel<real>(*c, Src, ev, pi, tau, step);                                                           \
+  void clvo_visc_christoffel_##sfx(const Consts* c, real* Src, const real* ev, const real* pi, real tau, int step,   \
+                                   const real* bulk) {                                                                 \
+    clvo::visc_christoffel<real>(*c, Src, ev, pi, tau, step, bulk);                                                     \
   }                                                                                                                     \
-  void clvo_visc_along_##sfx(const Consts* c, int axis, real* Src, const real* ev, const real* pi, real tau) {        \
-    clvo::visc_along<real>(*c, axis, Src, ev, pi, tau);                                                                 \
+  void clvo_visc_along_##sfx(const Consts* c, int axis, real* Src, const real* ev, const real* pi, real tau,         \
+                             const real* bulk) {                                                                       \
+    clvo::visc_along<real>(*c, axis, Src, ev, pi, tau, bulk);                                                           \
   }                                                                                                                     \
   void clvo_visc_update_ev_##sfx(const Consts* c, real* evnew, const real* ev1, const real* pi1, const real* pi2,     \
-                                 const real* Src, real tau, int step) {                                                \
-    clvo::visc_update_ev<real>(*c, evnew, ev1, pi1, pi2, Src, tau, step);                                               \
+                                 const real* Src, real tau, int step, const real* bulk1, const real* bulk2) {          \
+    clvo::visc_update_ev<real>(*c, evnew, ev1, pi1, pi2, Src, tau, step, bulk1, bulk2);                                 \
   }                                                                                                                     \
-  void clvo_visc_initialize_##sfx(const Consts* c, real* pi1, real* goodcell, real* udiff, const real* ev, real tau) { \
-    clvo::visc_initialize<real>(*c, pi1, goodcell, udiff, ev, tau);                                                     \
+  void clvo_visc_initialize_##sfx(const Consts* c, real* pi1, real* goodcell, real* udiff, const real* ev, real tau,  \
+                                  real* bulk1) {                                                                       \
+    clvo::visc_initialize<real>(*c, pi1, goodcell, udiff, ev, tau, bulk1);                                              \
   }                                                                                                                     \
   void clvo_visc_src_christoffel_##sfx(const Consts* c, real* Src, const real* pi1, const real* ev, real tau,        \
-                                       int step) {                                                                     \
-    clvo::visc_src_christoffel<real>(*c, Src, pi1, ev, tau, step);                                                      \
+                                       int step, real* SrcB) {                                                         \
+    clvo::visc_src_christoffel<real>(*c, Src, pi1, ev, tau, step, SrcB);                                                \
   }                                                                                                                     \
   void clvo_visc_src_along_##sfx(const Consts* c, int axis, real* Src, real* ud, const real* pi1, const real* ev,     \
-                                 real tau) {                                                                           \
-    clvo::visc_src_along<real>(*c, axis, Src, ud, pi1, ev, tau);                                                        \
+                                 real tau, real* SrcB, const real* bulk1) {                                            \
+    clvo::visc_src_along<real>(*c, axis, Src, ud, pi1, ev, tau, SrcB, bulk1);                                           \
   }                                                                                                                     \
   void clvo_update_pimn_##sfx(const Consts* c, real* pinew, real* goodcell, const real* pi1, const real* pistep,       \
                               const real* ev1, const real* ev2, const real* udiff, const real* udx, const real* udy,   \
-                              const real* udz, real* Src, real tau, int step) {                                        \
-    clvo::update_pimn<real>(*c, pinew, goodcell, pi1, pistep, ev1, ev2, udiff, udx, udy, udz, Src, tau, step);          \
+                              const real* udz, real* Src, real tau, int step, real* bulknew, const real* bulk1,        \
+                              const real* bulkstep, real* SrcB) {                                                      \
+    clvo::update_pimn<real>(*c, pinew, goodcell, pi1, pistep, ev1, ev2, udiff, udx, udy, udz, Src, tau, step, bulknew, \
+                            bulk1, bulkstep, SrcB);                                                                    \
   }                                                                                                                     \
   void clvo_get_udiff_##sfx(const Consts* c, real* udiff, const real* ev0, const real* ev1) {                          \
     clvo::get_udiff<real>(*c, udiff, ev0, ev1);                                                                         \
@@ -882,6 +943,7 @@ extern "C" {
   real clvo_root_newton_##sfx(const Consts* c, real T00, real M, int* iters) {                                          \
     real e; clvo::Helper<real>(*c).rootFinding_newton(&e, T00, M, iters); return e;                                     \
   }                                                                                                                     \
+  real clvo_zetaos_##sfx(const Consts* c, real T) { return clvo::Helper<real>(*c).zetaos(T); }                          \
   void clvo_test_hypersf_##sfx(const Consts* c, real* out4) {                                                           \
     clvo::Hypersf<real> H(*c);                                                                                          \
     real ed[16]; for (int q = 0; q < 8; q++) { ed[q] = 3.0f; ed[8 + q] = 2.0f; }                                        \
@@ -894,5 +956,5 @@ extern "C" {
 DEF(float, f32)
 DEF(double, f64)
 
-int clvo_abi_version(void) { return 1; }
+int clvo_abi_version(void) { return 2; }
 }

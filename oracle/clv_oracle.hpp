@@ -36,6 +36,10 @@ struct Consts {
   int gubser_visc_test;    // -D GUBSER_VISC_TEST
   int pimn_omega_coupling; // -D PIMUNU_OMEGA_COUPLING
   int omega_omega_coupling;// -D OMEGA_OMEGA_COUPLING
+  // Bulk viscosity. The reference has none (kernel_visc.cl:31-33 keeps a
+  // zero placeholder); these fields select the bulk sector specified below.
+  int bulk;
+  float ZETAOS_MAX, ZETAOS_T0, ZETAOS_WIDTH, ZETAOS_SKEW;
 };
 
 // real_type.h:9,16
@@ -178,6 +182,16 @@ template <class real> struct Helper {
     return (temperature < c.ETAOS_XMIN) ? (c.ETAOS_LEFT_SLOP * (temperature - c.ETAOS_XMIN) + c.ETAOS_YMIN)
                                         : (c.ETAOS_RIGHT_SLOP * (temperature - c.ETAOS_XMIN) + c.ETAOS_YMIN);
   }
+  // Bulk sector (no counterpart in the reference). zeta/s(T) is a skewed
+  // Cauchy peak, (zeta/s)_max w^2 / (w^2 + (T - T0)^2) with
+  // w = width * (1 + skew * sign(T - T0)), the parametrisation of the
+  // JETSCAPE Bayesian analysis (Everett et al., PRC 103, 054904 (2021));
+  // it needs only +, -, *, /, so both sides evaluate it to the same bits.
+  real zetaos(real temperature) const {
+    real dT = temperature - c.ZETAOS_T0;
+    real w = c.ZETAOS_WIDTH * (1.0f + c.ZETAOS_SKEW * cl_sign<real>(dT));
+    return c.ZETAOS_MAX * (w * w) / (w * w + dT * dT);
+  }
   static real gamma(real vx, real vy, real vz) {  // helper.h:46-48
     return 1.0f / std::sqrt(cl_max<real>(1.0f - vx * vx - vy * vy - vz * vz, acu));
   }
@@ -220,13 +234,15 @@ template <class real> struct Helper {
     *EdFind = E1;
   }
   // helper.h:128-167
-  void rootFinding_newton(real* ed_find, real T00, real M, int* iters = nullptr) const {
+  // With bulk != nullptr the pressure is P(e) + Pi (the bulk sector).
+  void rootFinding_newton(real* ed_find, real T00, real M, int* iters = nullptr, const real* bulk = nullptr) const {
     real vl = 0.0f;
     real vh = 1.0f;
     real dpe = 1.0f / 3.0f;
     real v = 0.5f * (vl + vh);
     real ed = T00 - M * v;
     real pr = E.P(ed);
+    if (bulk) pr = pr + *bulk;
     real f = (T00 + pr) * v - M;
     real df = (T00 + pr) - M * v * dpe;
     real dvold = vh - vl;
@@ -246,6 +262,7 @@ template <class real> struct Helper {
       if (std::fabs(dv) < 0.00001f || i > 100) break;
       ed = T00 - M * v;
       pr = E.P(ed);
+      if (bulk) pr = pr + *bulk;
       f = (T00 + pr) * v - M;
       df = (T00 + pr) - M * v * dpe;
       if (f > 0.0f) {

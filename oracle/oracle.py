@@ -33,6 +33,9 @@ class Consts(ctypes.Structure):
         ('eos_table', ctypes.c_void_p),
         ('riemann_test', ctypes.c_int), ('gubser_visc_test', ctypes.c_int),
         ('pimn_omega_coupling', ctypes.c_int), ('omega_omega_coupling', ctypes.c_int),
+        ('bulk', ctypes.c_int),
+        ('ZETAOS_MAX', ctypes.c_float), ('ZETAOS_T0', ctypes.c_float), ('ZETAOS_WIDTH', ctypes.c_float),
+        ('ZETAOS_SKEW', ctypes.c_float),
     ]
 
 
@@ -55,7 +58,7 @@ def load():
         _lib.clvo_hypersf_f32.restype = ctypes.c_long
         _lib.clvo_hypersf_f64.restype = ctypes.c_long
         for sfx, rt in (('f32', ctypes.c_float), ('f64', ctypes.c_double)):
-            for fn in ('P', 'T', 'S', 'CS2', 'root_fixed', 'root_newton'):
+            for fn in ('P', 'T', 'S', 'CS2', 'root_fixed', 'root_newton', 'zetaos'):
                 getattr(_lib, 'clvo_%s_%s' % (fn, sfx)).restype = rt
     return _lib
 
@@ -91,29 +94,38 @@ class Kernels(object):
         self.f('ideal_update_ev')(ctypes.byref(self.c), _p(evnew), _p(ev1), _p(Src), self.r(tau), int(step))
 
     # kernel_visc.cl
-    def visc_christoffel(self, Src, ev, pi, tau, step):
-        self.f('visc_christoffel')(ctypes.byref(self.c), _p(Src), _p(ev), _p(pi), self.r(tau), int(step))
+    # the bulk arguments are None (NULL) without the bulk sector
+    def visc_christoffel(self, Src, ev, pi, tau, step, bulk=None):
+        self.f('visc_christoffel')(ctypes.byref(self.c), _p(Src), _p(ev), _p(pi), self.r(tau), int(step), _p(bulk))
 
-    def visc_along(self, axis, Src, ev, pi, tau):
-        self.f('visc_along')(ctypes.byref(self.c), int(axis), _p(Src), _p(ev), _p(pi), self.r(tau))
+    def visc_along(self, axis, Src, ev, pi, tau, bulk=None):
+        self.f('visc_along')(ctypes.byref(self.c), int(axis), _p(Src), _p(ev), _p(pi), self.r(tau), _p(bulk))
 
-    def visc_update_ev(self, evnew, ev1, pi1, pi2, Src, tau, step):
+    def visc_update_ev(self, evnew, ev1, pi1, pi2, Src, tau, step, bulk1=None, bulk2=None):
         self.f('visc_update_ev')(ctypes.byref(self.c), _p(evnew), _p(ev1), _p(pi1), _p(pi2), _p(Src), self.r(tau),
-                                 int(step))
+                                 int(step), _p(bulk1), _p(bulk2))
 
     # kernel_IS.cl
-    def visc_initialize(self, pi1, goodcell, udiff, ev, tau):
-        self.f('visc_initialize')(ctypes.byref(self.c), _p(pi1), _p(goodcell), _p(udiff), _p(ev), self.r(tau))
+    def visc_initialize(self, pi1, goodcell, udiff, ev, tau, bulk1=None):
+        self.f('visc_initialize')(ctypes.byref(self.c), _p(pi1), _p(goodcell), _p(udiff), _p(ev), self.r(tau),
+                                  _p(bulk1))
 
-    def visc_src_christoffel(self, Src, pi1, ev, tau, step):
-        self.f('visc_src_christoffel')(ctypes.byref(self.c), _p(Src), _p(pi1), _p(ev), self.r(tau), int(step))
+    def visc_src_christoffel(self, Src, pi1, ev, tau, step, SrcB=None):
+        self.f('visc_src_christoffel')(ctypes.byref(self.c), _p(Src), _p(pi1), _p(ev), self.r(tau), int(step),
+                                       _p(SrcB))
 
-    def visc_src_along(self, axis, Src, ud, pi1, ev, tau):
-        self.f('visc_src_along')(ctypes.byref(self.c), int(axis), _p(Src), _p(ud), _p(pi1), _p(ev), self.r(tau))
+    def visc_src_along(self, axis, Src, ud, pi1, ev, tau, SrcB=None, bulk1=None):
+        self.f('visc_src_along')(ctypes.byref(self.c), int(axis), _p(Src), _p(ud), _p(pi1), _p(ev), self.r(tau),
+                                 _p(SrcB), _p(bulk1))
 
-    def update_pimn(self, pinew, goodcell, pi1, pistep, ev1, ev2, udiff, udx, udy, udz, Src, tau, step):
+    def update_pimn(self, pinew, goodcell, pi1, pistep, ev1, ev2, udiff, udx, udy, udz, Src, tau, step,
+                    bulknew=None, bulk1=None, bulkstep=None, SrcB=None):
         self.f('update_pimn')(ctypes.byref(self.c), _p(pinew), _p(goodcell), _p(pi1), _p(pistep), _p(ev1), _p(ev2),
-                              _p(udiff), _p(udx), _p(udy), _p(udz), _p(Src), self.r(tau), int(step))
+                              _p(udiff), _p(udx), _p(udy), _p(udz), _p(Src), self.r(tau), int(step),
+                              _p(bulknew), _p(bulk1), _p(bulkstep), _p(SrcB))
+
+    def zetaos(self, T):
+        return self.f('zetaos')(ctypes.byref(self.c), self.r(T))
 
     def get_udiff(self, udiff, ev0, ev1):
         self.f('get_udiff')(ctypes.byref(self.c), _p(udiff), _p(ev0), _p(ev1))
@@ -149,6 +161,11 @@ def make_consts(cfg, meta, table, efrz, eos_kind=0):
     c.gubser_visc_test = int(bool(getattr(cfg, 'gubser_visc_test', False)))
     c.pimn_omega_coupling = int(bool(getattr(cfg, 'pimn_omega_coupling', False)))
     c.omega_omega_coupling = int(bool(getattr(cfg, 'omega_omega_coupling', False)))
+    c.ZETAOS_MAX = fl(getattr(cfg, 'ZETAOS_MAX', 0.0))
+    c.ZETAOS_T0 = fl(getattr(cfg, 'ZETAOS_T0', 0.18))
+    c.ZETAOS_WIDTH = fl(getattr(cfg, 'ZETAOS_WIDTH', 0.02))
+    c.ZETAOS_SKEW = fl(getattr(cfg, 'ZETAOS_SKEW', 0.0))
+    c.bulk = int(float(getattr(cfg, 'ZETAOS_MAX', 0.0)) > 0.0)
     return c
 
 
@@ -261,11 +278,18 @@ class OracleVisc(object):
         self.d_goodcell = np.ones(self.size, real)
         self.d_pi_old = z(10)
         self.pisf = []
+        # bulk sector (no counterpart in the reference): Pi per cell in three
+        # slots like d_pi, and its IS source
+        self.bulk = bool(self.ideal.consts.bulk)
+        zb = lambda: np.zeros(self.size, real) if self.bulk else None
+        self.d_bulk = [zb(), zb(), zb()]
+        self.d_bulk_src = zb()
         self.IS_initialize()
         self.ideal_predict_for_first_step()
 
     def IS_initialize(self):  # visc.py:143-149
-        self.k.visc_initialize(self.d_pi[1], self.d_goodcell, self.d_udiff, self.ideal.d_ev[1], self.ideal.tau)
+        self.k.visc_initialize(self.d_pi[1], self.d_goodcell, self.d_udiff, self.ideal.d_ev[1], self.ideal.tau,
+                               self.d_bulk[1])
 
     def ideal_predict_for_first_step(self):  # visc.py:468-470
         self.ideal.stepUpdate(1)
@@ -274,21 +298,22 @@ class OracleVisc(object):
         self.ideal.load_ini(dat)
 
     def visc_stepUpdate(self, step):  # visc.py:232-283
-        k, ev, pi = self.k, self.ideal.d_ev, self.d_pi
+        k, ev, pi, bp = self.k, self.ideal.d_ev, self.d_pi, self.d_bulk
         tau = self.ideal.tau
-        k.visc_christoffel(self.ideal.d_Src, ev[step], pi[step], tau, step)
+        k.visc_christoffel(self.ideal.d_Src, ev[step], pi[step], tau, step, bp[step])
         for axis in range(3):
-            k.visc_along(axis, self.ideal.d_Src, ev[step], pi[step], tau)
-        k.visc_update_ev(ev[3 - step], ev[1], pi[0], pi[3 - step], self.ideal.d_Src, tau, step)
+            k.visc_along(axis, self.ideal.d_Src, ev[step], pi[step], tau, bp[step])
+        k.visc_update_ev(ev[3 - step], ev[1], pi[0], pi[3 - step], self.ideal.d_Src, tau, step, bp[0], bp[3 - step])
 
     def IS_stepUpdate(self, step):  # visc.py:287-314
-        k, ev, pi = self.k, self.ideal.d_ev, self.d_pi
+        k, ev, pi, bp = self.k, self.ideal.d_ev, self.d_pi, self.d_bulk
         tau = self.ideal.tau
-        k.visc_src_christoffel(self.d_IS_src, pi[step], ev[step], tau, step)
+        k.visc_src_christoffel(self.d_IS_src, pi[step], ev[step], tau, step, self.d_bulk_src)
         for axis, ud in enumerate((self.d_udx, self.d_udy, self.d_udz)):
-            k.visc_src_along(axis, self.d_IS_src, ud, pi[step], ev[step], tau)
+            k.visc_src_along(axis, self.d_IS_src, ud, pi[step], ev[step], tau, self.d_bulk_src, bp[step])
         k.update_pimn(pi[3 - step], self.d_goodcell, pi[1], pi[step], ev[1], ev[2], self.d_udiff, self.d_udx,
-                      self.d_udy, self.d_udz, self.d_IS_src, tau, step)
+                      self.d_udy, self.d_udz, self.d_IS_src, tau, step, bp[3 - step], bp[1], bp[step],
+                      self.d_bulk_src)
 
     def update_udiff(self, ev0, ev1):
         self.k.get_udiff(self.d_udiff, ev0, ev1)
@@ -299,6 +324,8 @@ class OracleVisc(object):
     def step(self, loop):  # visc.py:527-544
         ev = self.ideal.d_ev
         self.d_pi[0][...] = self.d_pi[1]
+        if self.bulk:
+            self.d_bulk[0][...] = self.d_bulk[1]
         ev[0][...] = ev[1]
         self.IS_stepUpdate(1)
         self.visc_stepUpdate(1)
@@ -330,7 +357,8 @@ class OracleVisc(object):
 
     def evolve(self, max_loops=1000, save_hypersf=True, force_run_to_maxloop=False):  # visc.py:473-560
         c = self.cfg
-        if c.ETAOS_YMIN < 1.0E-6 and c.ETAOS_LEFT_SLOP < 1.0E-6 and c.ETAOS_RIGHT_SLOP < 1.0E-6:
+        if (c.ETAOS_YMIN < 1.0E-6 and c.ETAOS_LEFT_SLOP < 1.0E-6 and c.ETAOS_RIGHT_SLOP < 1.0E-6
+                and not self.bulk):
             self.ideal.evolve(max_loops, save_hypersf, force_run_to_maxloop)
             return
         loop = 0
