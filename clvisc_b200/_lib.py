@@ -86,6 +86,10 @@ _SIGS = {
                                     _VP, _VP, ctypes.c_longlong, _VP, _VP], ctypes.c_int),
     'clv_aos_to_soa': ([_P, _VP, _VP, ctypes.c_longlong, ctypes.c_int, _VP], ctypes.c_int),
     'clv_soa_to_aos': ([_P, _VP, _VP, ctypes.c_longlong, ctypes.c_int, _VP], ctypes.c_int),
+    # batched events (clv_batch is passed as a pointer to its ctypes mirror in batch.py)
+    'clv_batch_stage': ([_P, ctypes.c_int, _VP, ctypes.c_int, ctypes.c_int, _VP], ctypes.c_int),
+    'clv_batch_advance': ([_P, _VP, ctypes.c_int, _VP], ctypes.c_int),
+    'clv_batch_occupancy': ([_P, ctypes.c_int, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
 }
 
 

@@ -2,7 +2,9 @@
 
 The library is compiled without fused multiply-add contraction and with IEEE
 division and square root, so each kernel's arithmetic matches a plain
-evaluation of the reference OpenCL source in the same precision.
+evaluation of the reference OpenCL source in the same precision. The
+translation units compile in parallel into objects under _build/ and are then
+linked into one shared library.
 
     python -m clvisc_b200.build          # build if sources changed
     python -m clvisc_b200.build --force  # rebuild
@@ -10,20 +12,22 @@ evaluation of the reference OpenCL source in the same precision.
 import os
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, 'libclvisc_b200.so')
-SOURCES = ['csrc/clv_capi.cu', 'csrc/clv_noalloc.cu']
+OBJDIR = os.path.join(HERE, '_build')
+SOURCES = ['csrc/clv_capi.cu', 'csrc/clv_noalloc.cu', 'csrc/clv_batch.cu']
 DEPS = ['csrc/clv_device.cuh', 'csrc/clv_stage.cuh', 'csrc/clv_stage_tiled.cuh', 'csrc/clv_misc.cuh',
-        'csrc/clv_hypersf.cuh',
+        'csrc/clv_hypersf.cuh', 'csrc/clv_batch.cuh',
         '../include/clvisc_b200.h']
 
 NVCC_FLAGS = [
     '-gencode', 'arch=compute_100a,code=sm_100a',
     '-O3', '-lineinfo', '-std=c++17',
     '--fmad=false', '-prec-div=true', '-prec-sqrt=true', '-ftz=false',
-    '-Xcompiler', '-fPIC', '-shared',
+    '-Xcompiler', '-fPIC',
 ]
 
 
@@ -44,10 +48,29 @@ def stale():
 def build(force=False, verbose=False, extra=()):
     if not force and not stale():
         return LIB
-    cmd = [nvcc()] + NVCC_FLAGS + list(extra) + ['-o', LIB] + [os.path.join(HERE, s) for s in SOURCES]
+    os.makedirs(OBJDIR, exist_ok=True)
+    objs = [os.path.join(OBJDIR, os.path.basename(s).replace('.cu', '.o')) for s in SOURCES]
+
+    def compile_one(src_obj):
+        src, obj = src_obj
+        cmd = [nvcc()] + NVCC_FLAGS + list(extra) + ['-c', '-o', obj, os.path.join(HERE, src)]
+        if verbose:
+            print(' '.join(cmd), flush=True)
+        r = subprocess.run(cmd, cwd=HERE, capture_output=True, text=True)
+        return cmd, r
+
+    with ThreadPoolExecutor(max_workers=len(SOURCES)) as ex:
+        results = list(ex.map(compile_one, zip(SOURCES, objs)))
+    for cmd, r in results:
+        if verbose or r.returncode:
+            sys.stdout.write(r.stdout)
+            sys.stderr.write(r.stderr)
+        if r.returncode:
+            raise subprocess.CalledProcessError(r.returncode, cmd)
+    link = [nvcc(), '-gencode', 'arch=compute_100a,code=sm_100a', '-shared', '-o', LIB] + objs
     if verbose:
-        print(' '.join(cmd))
-    subprocess.check_call(cmd, cwd=HERE)
+        print(' '.join(link), flush=True)
+    subprocess.check_call(link, cwd=HERE)
     return LIB
 
 

@@ -225,6 +225,16 @@ int hypersf_t(const clv::Params& p, int visc, double tau_old, double tau_new, co
 
 }  // namespace
 
+// shared with the library's other translation units
+namespace clv_host {
+int params_from_abi(const clv_params* in, clv::Params* out) { return to_params(in, out); }
+int set_error(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+int check_cuda(const char* where) { return cuda_check(where); }
+}  // namespace clv_host
+
 extern "C" {
 
 int clv_version(void) { return 0x000102; }

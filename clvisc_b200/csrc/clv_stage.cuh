@@ -73,9 +73,8 @@ template <class real> __device__ __forceinline__ real pisig_weight(int mu, int n
 // With BULK, component 10 of pc, S10 and pinew is the bulk pressure Pi.
 template <class real, bool COUPLED, bool BULK>
 __device__ __forceinline__ void pi_update(const Params& p, const ViscBuffers<real>& b, int step,
-                                          const TauConst<real>& tc, long long I, const real e0[4], const real pc[11],
-                                          const real grad[3][4], real S10[11], real pinew[11]) {
-  const long long ld = p.ld;
+                                          const TauConst<real>& tc, long long I, long long ld, const real e0[4],
+                                          const real pc[11], const real grad[3][4], real S10[11], real pinew[11]) {
   const real acu = Acu<real>::v;
   const real tau = tc.tau;
   const Recips<real>& rc = recips<real>(p);
@@ -218,9 +217,8 @@ __device__ __forceinline__ void pi_update(const Params& p, const ViscBuffers<rea
 // old and the new state is P(e) + Pi.
 template <class real, bool FUSED_PI, bool BULK>
 __device__ __forceinline__ void ev_update(const Params& p, const ViscBuffers<real>& b, int step,
-                                          const TauConst<real>& tc, long long I, const real pin[5], const real S4[4],
-                                          const real pinew[11]) {
-  const long long ld = p.ld;
+                                          const TauConst<real>& tc, long long I, long long ld, const real pin[5],
+                                          const real S4[4], const real pinew[11]) {
   const real acu = Acu<real>::v;
   const real tau = tc.tau;
   real e1[4];
@@ -283,19 +281,26 @@ __device__ __forceinline__ void ev_update(const Params& p, const ViscBuffers<rea
 }
 
 // --------------------------------------------------------------- viscous
+// Grid of one event: sizes and plane stride (the single-event kernels take
+// them from Params, the batch kernel from its event table).
+struct GridDims {
+  int nx, ny, nz;
+  long long ld;
+};
+
 // One cell of the fused viscous stage. With BULK the pi fields carry an
 // eleventh plane, the bulk pressure Pi, and the sources an eleventh IS term.
 template <class real, bool DO_IS, bool DO_KT, bool COUPLED, bool BULK>
-__device__ __forceinline__ void visc_stage_cell(const Params& p, const ViscBuffers<real>& b, int step,
-                                                const TauConst<real>& tc, long long I) {
+__device__ __forceinline__ void visc_stage_cell(const Params& p, const GridDims gd, const ViscBuffers<real>& b,
+                                                int step, const TauConst<real>& tc, long long I) {
   const real tau = tc.tau;
   const Recips<real>& rc = recips<real>(p);
   constexpr int NPI = BULK ? 11 : 10;
-  const long long ld = p.ld;
-  const int k = (int)(I % p.nz);
-  const long long t = I / p.nz;
-  const int j = (int)(t % p.ny);
-  const int i = (int)(t / p.ny);
+  const long long ld = gd.ld;
+  const int k = (int)(I % gd.nz);
+  const long long t = I / gd.nz;
+  const int j = (int)(t % gd.ny);
+  const int i = (int)(t / gd.ny);
   const real acu = Acu<real>::v;
 
   // centre cell of the stage input
@@ -365,8 +370,8 @@ __device__ __forceinline__ void visc_stage_cell(const Params& p, const ViscBuffe
 #pragma unroll 1
   for (int a = 0; a < 3; a++) {
     const int q = a == 0 ? i : (a == 1 ? j : k);
-    const int L = a == 0 ? p.nx : (a == 1 ? p.ny : p.nz);
-    const long long stride = a == 0 ? (long long)p.ny * p.nz : (a == 1 ? (long long)p.nz : 1ll);
+    const int L = a == 0 ? gd.nx : (a == 1 ? gd.ny : gd.nz);
+    const long long stride = a == 0 ? (long long)gd.ny * gd.nz : (a == 1 ? (long long)gd.nz : 1ll);
     const Stencil st = make_stencil(q, L, stride);
     const real D = a == 0 ? (real)p.DX : (a == 1 ? (real)p.DY : tc.dzt);
     const real rD = a == 0 ? rc.DX : (a == 1 ? rc.DY : tc.rdzt);
@@ -497,8 +502,8 @@ __device__ __forceinline__ void visc_stage_cell(const Params& p, const ViscBuffe
   }
 
   real pinew[11];
-  if (DO_IS) pi_update<real, COUPLED, BULK>(p, b, step, tc, I, e0, pc, grad, S10, pinew);
-  if (DO_KT) ev_update<real, DO_IS, BULK>(p, b, step, tc, I, pin, S4, pinew);
+  if (DO_IS) pi_update<real, COUPLED, BULK>(p, b, step, tc, I, ld, e0, pc, grad, S10, pinew);
+  if (DO_KT) ev_update<real, DO_IS, BULK>(p, b, step, tc, I, ld, pin, S4, pinew);
 
   if (b.write_src) {
     if (DO_KT)
@@ -515,7 +520,7 @@ __global__ void __launch_bounds__(128) visc_stage_kernel(Params p, ViscBuffers<r
   const long long N = (long long)p.nx * p.ny * p.nz;
   const long long I = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (I >= N) return;
-  visc_stage_cell<real, DO_IS, DO_KT, COUPLED, BULK>(p, b, step, tc, I);
+  visc_stage_cell<real, DO_IS, DO_KT, COUPLED, BULK>(p, GridDims{p.nx, p.ny, p.nz, p.ld}, b, step, tc, I);
 }
 
 // ----------------------------------------------------------------- ideal

@@ -346,7 +346,7 @@ __global__ void __launch_bounds__(TJ * TK, MINB)
 #pragma unroll
           for (int c = 0; c < 4; c++) umu_prev[c] = umc[c];
         }
-        pi_update<real, COUPLED, false>(p, b, step, tc, I, e0, pc, grad, S10, pinew);
+        pi_update<real, COUPLED, false>(p, b, step, tc, I, ld, e0, pc, grad, S10, pinew);
       } else {
         real u0c = Cc[RF_U0 * G::NC];
         umu_prev[0] = u0c * 1.0f;
@@ -354,7 +354,7 @@ __global__ void __launch_bounds__(TJ * TK, MINB)
         umu_prev[2] = u0c * e0[2];
         umu_prev[3] = u0c * e0[3];
       }
-      if (DO_KT) ev_update<real, DO_IS, false>(p, b, step, tc, I, pin, S4, pinew);
+      if (DO_KT) ev_update<real, DO_IS, false>(p, b, step, tc, I, ld, pin, S4, pinew);
       if (b.write_src) {
         if (DO_KT)
 #pragma unroll

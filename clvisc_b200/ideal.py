@@ -27,6 +27,65 @@ def plane_stride(n):
     return ((n + 63) // 64) * 64
 
 
+def make_params(c, meta, eos_table, efrz, nx, ny, nz, ld):
+    """clv_params of a run: the grid, and the constants the reference passes
+    to its kernels as -D float literals (ideal.py:146-171, eos.py:194-201)."""
+    p = _lib.ClvParams()
+    p.nx, p.ny, p.nz = nx, ny, nz
+    p.ld = ld
+    p.precision = 4 if c.use_float32 else 8
+    for key in ('dt', 'dx', 'dy', 'dz', 'tau0'):
+        setattr(p, key, float_literal(getattr(c, key.upper())))
+    p.etaos_xmin = float_literal(c.ETAOS_XMIN)
+    p.etaos_ymin = float_literal(c.ETAOS_YMIN)
+    p.etaos_left_slop = float_literal(c.ETAOS_LEFT_SLOP)
+    p.etaos_right_slop = float_literal(c.ETAOS_RIGHT_SLOP)
+    p.lam1 = float_literal(c.LAM1)
+    p.efrz = float_literal(efrz)
+    p.nxskip, p.nyskip, p.nzskip = c.nxskip, c.nyskip, c.nzskip
+    p.eos_ed_start = float_literal(meta['ed_start'])
+    p.eos_ed_step = float_literal(meta['ed_step'])
+    p.eos_num_ed = int(meta['num_of_ed'])
+    p.eos_nrow, p.eos_ncol = int(meta['nrow']), int(meta['ncol'])
+    p.eos_table = eos_table.data_ptr()
+    flags = 0
+    if getattr(c, 'riemann_test', False):
+        flags |= _lib.CLV_FLAG_RIEMANN_TEST
+    p.flags = flags
+    return p
+
+
+def add_visc_params(c, p):
+    """The viscous run's flags (visc.py:111-121) and bulk-sector constants on
+    top of make_params(); returns whether the bulk sector is on."""
+    flags = p.flags
+    if getattr(c, 'gubser_visc_test', False):
+        flags |= _lib.CLV_FLAG_GUBSER_VISC_TEST
+    if getattr(c, 'pimn_omega_coupling', False):
+        flags |= _lib.CLV_FLAG_PIMN_OMEGA_COUPLING
+    if getattr(c, 'omega_omega_coupling', False):
+        flags |= _lib.CLV_FLAG_OMEGA_OMEGA_COUPLING
+    bulk = float(getattr(c, 'ZETAOS_MAX', 0.0)) > 0.0
+    p.zetaos_max = float_literal(getattr(c, 'ZETAOS_MAX', 0.0))
+    p.zetaos_t0 = float_literal(getattr(c, 'ZETAOS_T0', 0.18))
+    p.zetaos_width = float_literal(getattr(c, 'ZETAOS_WIDTH', 0.02))
+    p.zetaos_skew = float_literal(getattr(c, 'ZETAOS_SKEW', 0.0))
+    if bulk:
+        flags |= _lib.CLV_FLAG_BULK
+    p.flags = flags
+    return bulk
+
+
+def load_eos(cfg, handcrafted_eos, device):
+    """(Eos object, device float32 table, table metadata, freeze-out energy density)."""
+    eos = Eos(cfg.eos_type) if handcrafted_eos is None else handcrafted_eos
+    if handcrafted_eos is None:
+        table, meta = eos.create_table(*TABLE_SHAPE[cfg.eos_type])
+    else:
+        table, meta = eos.create_table()
+    return eos, torch.from_numpy(table.reshape(-1)).to(device), meta, eos.f_ed(cfg.TFRZ)
+
+
 class CLIdeal(object):
     """Ideal hydro (pyvisc/ideal.py:28)."""
 
@@ -44,14 +103,7 @@ class CLIdeal(object):
         self.ld = plane_stride(self.size)
         self.tau = self.cfg.real(self.cfg.TAU0)
 
-        self.eos = Eos(self.cfg.eos_type) if handcrafted_eos is None else handcrafted_eos
-        if handcrafted_eos is None:
-            nrow, ncol = TABLE_SHAPE[self.cfg.eos_type]
-            table, meta = self.eos.create_table(nrow, ncol)
-        else:
-            table, meta = self.eos.create_table()
-        self.eos_table = torch.from_numpy(table.reshape(-1)).to(self.device)
-        self.efrz = self.eos.f_ed(self.cfg.TFRZ)
+        self.eos, self.eos_table, meta, self.efrz = load_eos(self.cfg, handcrafted_eos, self.device)
         self.params = self._make_params(meta)
 
         z = lambda w: torch.zeros((w, self.ld), dtype=self.dtype, device=self.device)
@@ -73,30 +125,7 @@ class CLIdeal(object):
 
     # ------------------------------------------------------------ helpers
     def _make_params(self, meta):
-        c = self.cfg
-        p = _lib.ClvParams()
-        p.nx, p.ny, p.nz = c.NX, c.NY, c.NZ
-        p.ld = self.ld
-        p.precision = 4 if c.use_float32 else 8
-        for key in ('dt', 'dx', 'dy', 'dz', 'tau0'):
-            setattr(p, key, float_literal(getattr(c, key.upper())))
-        p.etaos_xmin = float_literal(c.ETAOS_XMIN)
-        p.etaos_ymin = float_literal(c.ETAOS_YMIN)
-        p.etaos_left_slop = float_literal(c.ETAOS_LEFT_SLOP)
-        p.etaos_right_slop = float_literal(c.ETAOS_RIGHT_SLOP)
-        p.lam1 = float_literal(c.LAM1)
-        p.efrz = float_literal(self.efrz)
-        p.nxskip, p.nyskip, p.nzskip = c.nxskip, c.nyskip, c.nzskip
-        p.eos_ed_start = float_literal(meta['ed_start'])
-        p.eos_ed_step = float_literal(meta['ed_step'])
-        p.eos_num_ed = int(meta['num_of_ed'])
-        p.eos_nrow, p.eos_ncol = int(meta['nrow']), int(meta['ncol'])
-        p.eos_table = self.eos_table.data_ptr()
-        flags = 0
-        if getattr(c, 'riemann_test', False):
-            flags |= _lib.CLV_FLAG_RIEMANN_TEST
-        p.flags = flags
-        return p
+        return make_params(self.cfg, meta, self.eos_table, self.efrz, self.cfg.NX, self.cfg.NY, self.cfg.NZ, self.ld)
 
     @property
     def stream(self):

@@ -27,8 +27,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from .config import float_literal
-from .ideal import CLIdeal
+from .ideal import CLIdeal, add_visc_params
 
 
 class CLVisc(object):
@@ -43,22 +42,7 @@ class CLVisc(object):
         self.ld = self.ideal.ld
         self.device = self.ideal.device
         self.dtype = self.ideal.dtype
-        flags = self.ideal.params.flags
-        if self.cfg.gubser_visc_test:
-            flags |= _lib.CLV_FLAG_GUBSER_VISC_TEST
-        if self.cfg.pimn_omega_coupling:
-            flags |= _lib.CLV_FLAG_PIMN_OMEGA_COUPLING
-        if self.cfg.omega_omega_coupling:
-            flags |= _lib.CLV_FLAG_OMEGA_OMEGA_COUPLING
-        self.bulk = float(getattr(self.cfg, 'ZETAOS_MAX', 0.0)) > 0.0
-        p = self.ideal.params
-        p.zetaos_max = float_literal(getattr(self.cfg, 'ZETAOS_MAX', 0.0))
-        p.zetaos_t0 = float_literal(getattr(self.cfg, 'ZETAOS_T0', 0.18))
-        p.zetaos_width = float_literal(getattr(self.cfg, 'ZETAOS_WIDTH', 0.02))
-        p.zetaos_skew = float_literal(getattr(self.cfg, 'ZETAOS_SKEW', 0.0))
-        if self.bulk:
-            flags |= _lib.CLV_FLAG_BULK
-        self.ideal.params.flags = flags
+        self.bulk = add_visc_params(self.cfg, self.ideal.params)
         self.params = self.ideal.params
 
         z = lambda w: torch.zeros((w, self.ld), dtype=self.dtype, device=self.device)

@@ -173,6 +173,68 @@ int clv_hypersf_append_noalloc(const clv_params *p, int visc, double tau_old, do
                                const void *ev_new, const void *pi_old, const void *pi_new, void *sf, void *txyz,
                                void *pisf, long long capacity, long long *total, void *stream);
 
+/* ------------------------------------------------------------------------
+ * Batched events: many independent events on grids of different sizes
+ * advanced together. No counterpart in the reference, which runs one event
+ * per process (its event-by-event scripts loop over CLVisc objects).
+ *
+ * Event e's fields live in arenas shared by all events: its w-plane field
+ * starts at element off * (w planes of ld_e elements) of the arena -- ev
+ * slots and udiff at off_ev (4 planes), pi slots at off_pi (10 planes, 11
+ * with CLV_FLAG_BULK), the sources at off_src (14, or 15), goodcell at byte
+ * off_cell. The clv_params of a batch carry the shared constants; its nx, ny,
+ * nz, ld describe no event (set them to the largest event). Each event evolves
+ * bit for bit as CLVisc.evolve would evolve it alone (visc.py:473-560):
+ * both Runge-Kutta stages fused, the maximum energy density recorded with tau
+ * at every multiple of ntskip steps, the event stopping when that maximum is
+ * below efrz. Gubser, coupling and Riemann test flags are not batched. */
+typedef struct clv_batch_event {
+  int nx, ny, nz, reserved;
+  long long ld, off_ev, off_pi, off_src, off_cell;
+} clv_batch_event;
+
+/* device control block of a batch */
+typedef struct clv_batch_ctl {
+  int loop;                /* steps taken                     */
+  int n_active;            /* events still running            */
+  long long active_cells;  /* their cells                     */
+  int done;                /* 1 when no event is left         */
+  int hist_len;            /* stop tests recorded in history  */
+} clv_batch_ctl;
+
+typedef struct clv_batch {
+  const clv_batch_event *events; /* device, n_events entries (at most 1024)          */
+  int n_events;
+  void *ev[3], *pi[3];           /* arenas of d_ev[0..2], d_pi[0..2]                   */
+  void *src, *udiff;             /* arenas of the stage sources and udiff              */
+  unsigned char *goodcell;       /* arena of goodcell                                  */
+  void *keys;                    /* n_events max-energy-density keys (precision bytes) */
+  clv_batch_ctl *ctl;            /* device control block                               */
+  int *active;                   /* n_events: running events, compacted                */
+  long long *prefix;             /* n_events + 1: cell prefix over active              */
+  int *loops;                    /* n_events: steps at which each stopped (-1: running) */
+  double *history;               /* hist_cap x n_events x (tau, max ed)                */
+  int hist_cap;
+  double tau0, dt, efrz;         /* the host's double TAU0, DT, freeze-out energy density */
+  int ntskip;                    /* stop-test cadence                                  */
+  int max_loops;                 /* stop every event after this many steps (-1: never) */
+} clv_batch;
+
+/* One fused Runge-Kutta stage (step 1 or 2) of every running event: one
+ * persistent launch of grid_blocks blocks of block_size (64, 128 or 256)
+ * threads; grid_blocks <= 0 sizes the grid to fill the GPU once. Reads tau and
+ * the running list from the device, so it can be captured in a CUDA graph. */
+int clv_batch_stage(const clv_params *p, int step, const clv_batch *b, int block_size, int grid_blocks,
+                    void *stream);
+/* After a step (first = 0) or once before the first step (first = 1, with
+ * keys holding each event's initial maximum energy density): count the step,
+ * apply the stop test at multiples of ntskip, record the history, rebuild the
+ * running list. ctl must start as {0, 0, 0, 0, 0}, loops as -1, keys as 0
+ * except for the first call. */
+int clv_batch_advance(const clv_params *p, const clv_batch *b, int first, void *stream);
+/* Resident blocks per SM of the batch stage kernel at block_size threads. */
+int clv_batch_occupancy(const clv_params *p, int block_size, int *blocks_per_sm);
+
 /* Host-boundary layout transposes: (n, w) row-major <-> w planes of ld. */
 int clv_aos_to_soa(const clv_params *p, const void *aos, void *soa, long long n, int w, void *stream);
 int clv_soa_to_aos(const clv_params *p, const void *soa, void *aos, long long n, int w, void *stream);

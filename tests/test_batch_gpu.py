@@ -1,0 +1,104 @@
+"""Batched events on the GPU: every event of a CLViscBatch must evolve bit for
+bit as a CLVisc object running that event alone (construction, load_ini and
+evolve to freeze-out, visc.py:473-560), whatever the other events in the batch,
+with or without the CUDA graph, before and after autotuning."""
+import numpy as np
+import pytest
+
+from parity_util import assert_same, make_cfg, seeded_ic
+
+pytestmark = pytest.mark.gpu
+
+GRIDS = [(21, 19, 1), (33, 29, 1), (17, 15, 5), (27, 31, 1), (9, 9, 1)]
+BULK = dict(ZETAOS_MAX=0.08, ZETAOS_T0=0.18, ZETAOS_WIDTH=0.03)
+
+
+def _cfg(grid, use_float32, bulk, **kw):
+    extra = dict(BULK) if bulk else {}
+    extra.update(kw)
+    return make_cfg(*grid, use_float32=use_float32, dx=0.6, dz=0.6, dt=0.04, ntskip=4, etaos=0.16, **extra)
+
+
+def _ics(use_float32, bulk):
+    out = []
+    for e, g in enumerate(GRIDS):
+        out.append(seeded_ic(_cfg(g, use_float32, bulk), seed=100 + e, b=2.0 * e, edmax=6.0 + e))
+    return out
+
+
+def _single(grid, ic, use_float32, bulk):
+    from clvisc_b200.visc import CLVisc
+    v = CLVisc(_cfg(grid, use_float32, bulk))
+    v.load_ini(ic)
+    v.evolve(save_hypersf=False)
+    return v
+
+
+def _batch(use_float32, bulk, ics, **kw):
+    from clvisc_b200.batch import CLViscBatch
+    b = CLViscBatch(_cfg(GRIDS[0], use_float32, bulk), GRIDS, **kw)
+    for e, ic in enumerate(ics):
+        b.load_ini(e, ic)
+    return b
+
+
+@pytest.mark.parametrize('use_float32', [True, False])
+@pytest.mark.parametrize('bulk', [False, True])
+def test_batch_events_match_single_runs(cuda_lib, use_float32, bulk):
+    ics = _ics(use_float32, bulk)
+    b = _batch(use_float32, bulk, ics)
+    b.evolve()
+    loops = b.loops()
+    assert (loops > 0).all()
+    assert len(set(loops.tolist())) > 1  # events stop at different steps
+    for e, (g, ic) in enumerate(zip(GRIDS, ics)):
+        v = _single(g, ic, use_float32, bulk)
+        tag = 'event %d %s' % (e, g)
+        h = np.array(v.ideal.history, np.float64)
+        assert_same(tag + ' history', b.history(e).astype(np.float64), h)
+        assert loops[e] == (len(h) - 1) * 4
+        assert_same(tag + ' ev[1]', b.ev_to_host(e), v.ideal.field_to_host(v.ideal.d_ev[1]))
+        assert_same(tag + ' pi[1]', b.pi_to_host(e), v.pi_to_host(1))
+        assert_same(tag + ' Pi[1]', b.bulk_to_host(e), v.bulk_to_host(1))
+        assert_same(tag + ' ev[2]', b.ev_to_host(e, slot=2), v.ideal.field_to_host(v.ideal.d_ev[2]))
+
+
+@pytest.mark.parametrize('use_float32', [True, False])
+def test_batch_graph_equals_eager_and_autotune_restores(cuda_lib, use_float32):
+    ics = _ics(use_float32, True)
+    runs = []
+    for mode in ('eager', 'graph', 'tuned'):
+        b = _batch(use_float32, True, ics)
+        if mode == 'tuned':
+            res = b.autotune(steps=3)
+            assert len(res) >= 3 and (b.block_size, b.grid_blocks) in res
+        steps = b.evolve(use_graph=(mode != 'eager'))
+        runs.append((steps, b.loops(), [b.ev_to_host(e) for e in range(len(GRIDS))],
+                     [b.bulk_to_host(e) for e in range(len(GRIDS))]))
+    for steps, loops, evs, bulks in runs[1:]:
+        assert steps == runs[0][0]
+        np.testing.assert_array_equal(loops, runs[0][1])
+        for e in range(len(GRIDS)):
+            assert_same('ev event %d' % e, evs[e], runs[0][2][e])
+            assert_same('Pi event %d' % e, bulks[e], runs[0][3][e])
+
+
+def test_batch_max_loops(cuda_lib):
+    """max_loops stops every event after that many steps, as
+    CLVisc.evolve(max_loops, force_run_to_maxloop=True) does for one event
+    that has not frozen out by then."""
+    from clvisc_b200.batch import CLViscBatch
+    from clvisc_b200.visc import CLVisc
+    ics = _ics(True, False)
+    b = CLViscBatch(_cfg(GRIDS[0], True, False), GRIDS, max_loops=10)
+    for e, ic in enumerate(ics):
+        b.load_ini(e, ic)
+    assert b.evolve() == 10
+    assert (b.loops() == 10).all()
+    for e in (0, 2):
+        v = CLVisc(_cfg(GRIDS[e], True, False))
+        v.load_ini(ics[e])
+        v.evolve(max_loops=10, save_hypersf=False, force_run_to_maxloop=True)
+        assert_same('ev event %d' % e, b.ev_to_host(e), v.ideal.field_to_host(v.ideal.d_ev[1]))
+        assert_same('history event %d' % e, b.history(e).astype(np.float64),
+                    np.array(v.ideal.history, np.float64))
