@@ -200,6 +200,104 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+# The batched workload: 64 seeded (2+1)D Pb+Pb events, NX = NY odd in
+# [121, 301], b uniform in [0, 12] fm (both drawn from default_rng(seed)),
+# seeds 1000..1063, dx = 0.16 fm, dtau = 0.02 fm, eta/s = 0.16, zeta/s a
+# skewed-Cauchy peak of 0.05 at T = 0.18 GeV (width 0.02 GeV), lattice EOS,
+# FP32, every event run to freeze-out (T < 137 MeV).
+BATCH_EVENTS = 64
+
+
+def batch_event_spec(e):
+    import numpy as np
+    rng = np.random.default_rng(1000 + e)
+    n = 2 * int(rng.integers(60, 151)) + 1
+    return n, float(rng.uniform(0.0, 12.0)), 1000 + e
+
+
+def batch_cfg(n=121):
+    from clvisc_b200.config import read_config, set_real
+    cfg = read_config([])
+    cfg.NX = cfg.NY = n
+    cfg.NZ = 1
+    cfg.DX = cfg.DY = 0.16
+    cfg.DZ = 0.15
+    cfg.DT = 0.02
+    cfg.TAU0 = 0.6
+    cfg.eos_type = 'lattice_pce165'
+    cfg.use_float32 = True
+    cfg.ETAOS_XMIN, cfg.ETAOS_YMIN, cfg.ETAOS_LEFT_SLOP, cfg.ETAOS_RIGHT_SLOP = 0.18, 0.16, 0.0, 0.0
+    cfg.ZETAOS_MAX, cfg.ZETAOS_T0, cfg.ZETAOS_WIDTH, cfg.ZETAOS_SKEW = 0.05, 0.18, 0.02, 0.0
+    cfg.TFRZ = 0.137
+    cfg.ntskip = 20
+    cfg.fPathOut = '/tmp/clv_bench_batch'
+    return set_real(cfg)
+
+
+def run_batch(n_events=BATCH_EVENTS, one_at_a_time=True):
+    """events/h of the batched runner against CLVisc one event at a time."""
+    import numpy as np
+    import torch
+    from clvisc_b200.batch import CLViscBatch
+    from clvisc_b200.initial import glauber_event
+    from clvisc_b200.visc import CLVisc
+    specs = [batch_event_spec(e) for e in range(n_events)]
+    t = time.perf_counter()
+    ics = [glauber_event(n, n, 1, 0.16, 0.16, 0.15, b=bb, seed=sd, edmax=50.0) for n, bb, sd in specs]
+    ic_s = time.perf_counter() - t
+    grids = [(n, n, 1) for n, _, _ in specs]
+    cfg = batch_cfg()
+    out = {'metric': 'events/h (%d seeded (2+1)D events, 121^2..301^2, to freeze-out)' % n_events,
+           'unit': 'events/h', 'events': n_events, 'cells': int(sum(n * n for n, _, _ in specs)),
+           'ic_host_s': ic_s}
+    # autotuned launch shape (timed separately), then the timed batch from host arrays
+    bt = CLViscBatch(cfg, grids)
+    for e, ic in enumerate(ics):
+        bt.load_ini(e, ic)
+    t = time.perf_counter()
+    tuning = bt.autotune(steps=3)
+    out['autotune_s'] = time.perf_counter() - t
+    out['launch'] = {'block': bt.block_size, 'grid': bt.grid_blocks,
+                     'candidates_ms_per_step': {'%dx%d' % k: round(v, 4) for k, v in sorted(tuning.items())}}
+    shape = (bt.block_size, bt.grid_blocks)
+    del bt
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    bt = CLViscBatch(cfg, grids, block_size=shape[0], grid_blocks=shape[1])
+    for e, ic in enumerate(ics):
+        bt.load_ini(e, ic)
+    t_solve = time.perf_counter()
+    steps = bt.evolve()
+    torch.cuda.synchronize()
+    t_solved = time.perf_counter()
+    finals = [bt.ev_to_host(e) for e in range(n_events)]
+    t_end = time.perf_counter()
+    loops = bt.loops()
+    out.update({'value': n_events / (t_solved - t_solve) * 3600.0, 'solve_s': t_solved - t_solve,
+                'e2e': {'value': n_events / (t_end - t) * 3600.0, 'unit': 'events/h', 'seconds': t_end - t,
+                        'h2d_bytes': int(sum(ic.nbytes for ic in ics)),
+                        'd2h_bytes': int(sum(f.nbytes for f in finals))},
+                'batch_steps': int(steps), 'event_steps': [int(x) for x in loops],
+                'cell_updates_per_s': float(sum(n * n * int(l) for (n, _, _), l in zip(specs, loops)) /
+                                            (t_solved - t_solve))})
+    if one_at_a_time:
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        same = True
+        for e, ic in enumerate(ics):
+            v = CLVisc(batch_cfg(specs[e][0]))
+            v.load_ini(ic)
+            v.evolve(save_hypersf=False)
+            f = v.ideal.ev_to_host()
+            same = same and bool(np.array_equal(f, finals[e]))
+        t1 = time.perf_counter() - t
+        out['one_at_a_time'] = {'value': n_events / t1 * 3600.0, 'unit': 'events/h', 'seconds': t1,
+                                'api': 'CLVisc(cfg); load_ini; evolve(save_hypersf=False); ev_to_host per event',
+                                'bitwise_equal_to_batch': same}
+        out['speedup_e2e'] = out['e2e']['value'] / out['one_at_a_time']['value']
+    return out
+
+
 def run_gpu(args, rank, world, dist):
     import numpy as np
     import torch
@@ -283,6 +381,8 @@ def run_gpu(args, rank, world, dist):
         if not args.no_cpu_baseline:
             cb = cpu_baseline(steps=2)
             line['cpu_baseline'] = {k: cb[k] for k in ('value', 'unit', 'cores', 'kind', 'sample')}
+        if args.batch_events > 0 and world == 1:
+            line['batch'] = run_batch(args.batch_events, one_at_a_time=not args.no_one_at_a_time)
         print(json.dumps(line), flush=True)
 
 
@@ -294,11 +394,20 @@ def main():
     ap.add_argument('--impl', default='b200', choices=['b200', 'reference'])
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--no-e2e', action='store_true', help='device-timed steps only (profiling runs)')
+    ap.add_argument('--batch-events', type=int, default=BATCH_EVENTS,
+                    help='events of the batched workload reported under "batch" (0: skip)')
+    ap.add_argument('--no-one-at-a-time', action='store_true', help='skip the one-event-at-a-time comparison')
+    ap.add_argument('--batch-only', action='store_true', help='print only the batched workload line')
     ap.add_argument('--grid', type=lambda s: tuple(int(x) for x in s.split(',')), default=(NX, NY, NZ),
                     help='nx,ny,nz (default: the 385,385,115 workload)')
     args = ap.parse_args()
     world = int(os.environ.get('WORLD_SIZE', '1'))
     rank = int(os.environ.get('RANK', '0'))
+    if args.batch_only:
+        import torch
+        torch.cuda.set_device(int(os.environ.get('LOCAL_RANK', 0)))
+        print(json.dumps(run_batch(args.batch_events, one_at_a_time=not args.no_one_at_a_time)), flush=True)
+        return
     if args.impl == 'reference':
         # rank 0 alone times the CPU path; the other ranks exit without work
         # and without joining a process group
