@@ -257,13 +257,13 @@ def run_batch(n_events=BATCH_EVENTS, one_at_a_time=True):
     t = time.perf_counter()
     tuning = bt.autotune(steps=3)
     out['autotune_s'] = time.perf_counter() - t
-    out['launch'] = {'block': bt.block_size, 'grid': bt.grid_blocks,
-                     'candidates_ms_per_step': {'%dx%d' % k: round(v, 4) for k, v in sorted(tuning.items())}}
-    shape = (bt.block_size, bt.grid_blocks)
+    out['launch'] = {'block': bt.block_size, 'grid': bt.grid_blocks, 'max_registers': bt.max_registers,
+                     'candidates_ms_per_step': {'%dx%d/r%d' % k: round(v, 4) for k, v in sorted(tuning.items())}}
+    shape = (bt.block_size, bt.grid_blocks, bt.max_registers)
     del bt
     torch.cuda.synchronize()
     t = time.perf_counter()
-    bt = CLViscBatch(cfg, grids, block_size=shape[0], grid_blocks=shape[1])
+    bt = CLViscBatch(cfg, grids, block_size=shape[0], grid_blocks=shape[1], max_registers=shape[2])
     for e, ic in enumerate(ics):
         bt.load_ini(e, ic)
     t_solve = time.perf_counter()
@@ -283,17 +283,20 @@ def run_batch(n_events=BATCH_EVENTS, one_at_a_time=True):
     if one_at_a_time:
         torch.cuda.synchronize()
         t = time.perf_counter()
-        same = True
+        differ = 0
+        singles = []
         for e, ic in enumerate(ics):
             v = CLVisc(batch_cfg(specs[e][0]))
             v.load_ini(ic)
             v.evolve(save_hypersf=False)
-            f = v.ideal.ev_to_host()
-            same = same and bool(np.array_equal(f, finals[e]))
+            singles.append(v.ideal.ev_to_host())
         t1 = time.perf_counter() - t
+        for f, g in zip(singles, finals):  # bit patterns, so that NaN equals NaN
+            differ += int(np.count_nonzero(f.view(np.uint32) != g.view(np.uint32)))
+        out['nan_values'] = int(sum(np.count_nonzero(np.isnan(g)) for g in finals))
         out['one_at_a_time'] = {'value': n_events / t1 * 3600.0, 'unit': 'events/h', 'seconds': t1,
                                 'api': 'CLVisc(cfg); load_ini; evolve(save_hypersf=False); ev_to_host per event',
-                                'bitwise_equal_to_batch': same}
+                                'bitwise_equal_to_batch': differ == 0, 'values_differing': differ}
         out['speedup_e2e'] = out['e2e']['value'] / out['one_at_a_time']['value']
     return out
 

@@ -45,7 +45,7 @@ class ClvParams(ctypes.Structure):
         ('eos_table', ctypes.c_void_p),
         ('flags', ctypes.c_int),
         ('zetaos_max', ctypes.c_float), ('zetaos_t0', ctypes.c_float), ('zetaos_width', ctypes.c_float),
-        ('zetaos_skew', ctypes.c_float),
+        ('zetaos_skew', ctypes.c_float), ('zetaos_tmin', ctypes.c_float),
     ]
 
 
@@ -87,9 +87,9 @@ _SIGS = {
     'clv_aos_to_soa': ([_P, _VP, _VP, ctypes.c_longlong, ctypes.c_int, _VP], ctypes.c_int),
     'clv_soa_to_aos': ([_P, _VP, _VP, ctypes.c_longlong, ctypes.c_int, _VP], ctypes.c_int),
     # batched events (clv_batch is passed as a pointer to its ctypes mirror in batch.py)
-    'clv_batch_stage': ([_P, ctypes.c_int, _VP, ctypes.c_int, ctypes.c_int, _VP], ctypes.c_int),
+    'clv_batch_stage': ([_P, ctypes.c_int, _VP, ctypes.c_int, ctypes.c_int, ctypes.c_int, _VP], ctypes.c_int),
     'clv_batch_advance': ([_P, _VP, ctypes.c_int, _VP], ctypes.c_int),
-    'clv_batch_occupancy': ([_P, ctypes.c_int, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
+    'clv_batch_occupancy': ([_P, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
 }
 
 

@@ -74,7 +74,7 @@ class CLViscBatch(object):
     """Batched viscous hydro: events of one configuration on their own grids."""
 
     def __init__(self, configs, grids, handcrafted_eos=None, gpu_id=0, max_loops=-1, block_size=None,
-                 grid_blocks=None):
+                 grid_blocks=None, max_registers=0):
         self.cfg = set_real(configs)
         if not torch.cuda.is_available():
             raise RuntimeError('CLViscBatch needs a CUDA device; there is no CPU path')
@@ -128,6 +128,7 @@ class CLViscBatch(object):
         self.d_history = torch.zeros(1, dtype=torch.float64, device=dev)
         self.block_size = block_size
         self.grid_blocks = grid_blocks
+        self.max_registers = int(max_registers)
         self.tuning = None
         self._graph = None
         self._h_ctl = torch.zeros(ctypes.sizeof(_Ctl), dtype=torch.uint8).pin_memory()
@@ -209,16 +210,18 @@ class CLViscBatch(object):
         b.max_loops = self.max_loops
         return b
 
-    def _launch_step(self, b, bs, grid):
+    def _launch_step(self, b, bs, grid, regs):
         for step in (1, 2):
             _lib.check(self.lib.clv_batch_stage(ctypes.byref(self.params), step, ctypes.byref(b), int(bs), int(grid),
-                                                self.stream), 'clv_batch_stage')
+                                                int(regs), self.stream), 'clv_batch_stage')
         _lib.check(self.lib.clv_batch_advance(ctypes.byref(self.params), ctypes.byref(b), 0, self.stream),
                    'clv_batch_advance')
 
-    def occupancy(self, bs):
+    def occupancy(self, bs, regs=0):
+        """Resident stage-kernel blocks per SM at bs threads (regs: 0, or 128
+        for the register-capped FP32 variant)."""
         n = ctypes.c_int()
-        _lib.check(self.lib.clv_batch_occupancy(ctypes.byref(self.params), int(bs), ctypes.byref(n)),
+        _lib.check(self.lib.clv_batch_occupancy(ctypes.byref(self.params), int(bs), int(regs), ctypes.byref(n)),
                    'clv_batch_occupancy')
         return n.value
 
@@ -227,8 +230,8 @@ class CLViscBatch(object):
             self.block_size = 128
         if self.grid_blocks is None:
             sms = torch.cuda.get_device_properties(self.device).multi_processor_count
-            self.grid_blocks = sms * max(1, self.occupancy(self.block_size))
-        return self.block_size, self.grid_blocks
+            self.grid_blocks = sms * max(1, self.occupancy(self.block_size, self.max_registers))
+        return self.block_size, self.grid_blocks, self.max_registers
 
     # ------------------------------------------------------------- evolve
     def _start(self, hist_cap):
@@ -263,20 +266,20 @@ class CLViscBatch(object):
         if hist_cap is None:
             hist_cap = (self.max_loops // c.ntskip + 2) if self.max_loops >= 0 else 4096
         b = self._start(hist_cap)
-        bs, grid = self._launch_shape()
+        bs, grid, regs = self._launch_shape()
         k = int(steps_per_check or c.ntskip)
         if use_graph:
-            key = (bs, grid, k, self.hist_cap, self.d_history.data_ptr())
+            key = (bs, grid, regs, k, self.hist_cap, self.d_history.data_ptr())
             if self._graph is None or self._graph_key != key:
                 self._graph = None
-                self.occupancy(bs)  # loads the stage kernel before the capture
+                self.occupancy(bs, regs)  # loads the stage kernel before the capture
                 s = torch.cuda.Stream(self.device)
                 s.wait_stream(torch.cuda.current_stream(self.device))
                 g = torch.cuda.CUDAGraph()
                 with torch.cuda.stream(s):
                     with torch.cuda.graph(g, stream=s):
                         for _ in range(k):
-                            self._launch_step(b, bs, grid)
+                            self._launch_step(b, bs, grid, regs)
                 torch.cuda.current_stream(self.device).wait_stream(s)
                 self._graph, self._graph_key = g, key
             while not self._ctl().done:
@@ -284,7 +287,7 @@ class CLViscBatch(object):
         else:
             while not self._ctl().done:
                 for _ in range(k):
-                    self._launch_step(b, bs, grid)
+                    self._launch_step(b, bs, grid, regs)
         return self._ctl().loop
 
     # ------------------------------------------------------------ results
@@ -334,31 +337,36 @@ class CLViscBatch(object):
                 getattr(self, n).copy_(v)
 
     def autotune(self, steps=4, block_sizes=(64, 128, 256)):
-        """Choose the stage kernel's block size and persistent grid by timing
-        `steps` steps of this batch for each candidate (state restored after
-        each); call after load_ini. Returns {(block, grid): ms per step}."""
+        """Choose the stage kernel's block size, grid and register cap by
+        timing `steps` steps of this batch for each candidate (state restored
+        after each); call after load_ini. Candidates: every block size, each
+        with persistent grids of 1..occupancy blocks per SM and the one-cell-
+        per-thread grid, with and (FP32) without the 128-register cap.
+        Returns {(block, grid, max_registers): ms per step}."""
         sms = torch.cuda.get_device_properties(self.device).multi_processor_count
         hist = self.hist_cap
         b = self._start(max(hist, steps // self.cfg.ntskip + 2))
         snap = self._snapshot()
         results = {}
         total = sum(self.sizes)
-        for bs in block_sizes:
-            occ = max(1, self.occupancy(bs))
-            grids = sorted({sms * k for k in range(1, occ + 1)} | {(total + bs - 1) // bs})
-            for grid in grids:
-                self._launch_step(b, bs, grid)  # warm-up
-                torch.cuda.synchronize(self.device)
-                t0 = torch.cuda.Event(enable_timing=True)
-                t1 = torch.cuda.Event(enable_timing=True)
-                t0.record()
-                for _ in range(steps):
-                    self._launch_step(b, bs, grid)
-                t1.record()
-                torch.cuda.synchronize(self.device)
-                results[(bs, grid)] = t0.elapsed_time(t1) / steps
-                self._restore(snap)
-        self.block_size, self.grid_blocks = min(results, key=results.get)
+        caps = (0, 128) if self.cfg.use_float32 else (0,)
+        for regs in caps:
+            for bs in block_sizes:
+                occ = max(1, self.occupancy(bs, regs))
+                grids = sorted({sms * k for k in range(1, occ + 1)} | {(total + bs - 1) // bs})
+                for grid in grids:
+                    self._launch_step(b, bs, grid, regs)  # warm-up
+                    torch.cuda.synchronize(self.device)
+                    t0 = torch.cuda.Event(enable_timing=True)
+                    t1 = torch.cuda.Event(enable_timing=True)
+                    t0.record()
+                    for _ in range(steps):
+                        self._launch_step(b, bs, grid, regs)
+                    t1.record()
+                    torch.cuda.synchronize(self.device)
+                    results[(bs, grid, regs)] = t0.elapsed_time(t1) / steps
+                    self._restore(snap)
+        self.block_size, self.grid_blocks, self.max_registers = min(results, key=results.get)
         self.tuning = results
         self._graph = None
         return results

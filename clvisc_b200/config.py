@@ -88,6 +88,7 @@ def read_config(argv=None, info_path=None):
         'ZETAOS_T0': (gf('intrinsic', 'ZETAOS_T0'), 'T of the zeta/s peak'),
         'ZETAOS_WIDTH': (gf('intrinsic', 'ZETAOS_WIDTH'), 'width of the zeta/s peak'),
         'ZETAOS_SKEW': (gf('intrinsic', 'ZETAOS_SKEW'), 'skewness of the zeta/s peak'),
+        'ZETAOS_TMIN': (gf('intrinsic', 'ZETAOS_TMIN'), 'no bulk pressure below this temperature'),
         'BSZ': (gi('opencl', 'local_workgroup_size'), 'work-group size (accepted, unused)'),
     }
     parser = argparse.ArgumentParser(description='CLVisc B200 hydro configuration')
@@ -124,7 +125,7 @@ def write_config(configs, comments=''):
         'NX', 'NY', 'NZ', 'ntskip', 'nxskip', 'nyskip', 'nzskip', 'DT', 'DX', 'DY', 'DZ')}
     c['intrinsic'] = {k: str(getattr(configs, k)) for k in (
         'TAU0', 'eos_type', 'TFRZ', 'ETAOS_XMIN', 'ETAOS_YMIN', 'ETAOS_LEFT_SLOP', 'ETAOS_RIGHT_SLOP', 'LAM1',
-        'ZETAOS_MAX', 'ZETAOS_T0', 'ZETAOS_WIDTH', 'ZETAOS_SKEW', 'BSZ')}
+        'ZETAOS_MAX', 'ZETAOS_T0', 'ZETAOS_WIDTH', 'ZETAOS_SKEW', 'ZETAOS_TMIN', 'BSZ')}
     with open(os.path.join(configs.fPathOut, 'hydro.info'), 'w') as f:
         c.write(f)
         f.write('#comments: ' + comments)

@@ -57,9 +57,9 @@ int make_args(const clv_params* pp, const clv_batch* b, clv::Params* p, clv::Bat
   return CLV_OK;
 }
 
-template <class real, bool BULK, int BS>
+template <class real, bool BULK, int BS, int MINB>
 int launch_stage(const clv::Params& p, const clv::BatchArgs<real>& a, int step, int grid, cudaStream_t s) {
-  auto kern = clv::batch_stage_kernel<real, BULK, BS>;
+  auto kern = clv::batch_stage_kernel<real, BULK, BS, MINB>;
   if (grid <= 0) {
     int dev = 0, sms = 0, per_sm = 0;
     cudaGetDevice(&dev);
@@ -71,16 +71,28 @@ int launch_stage(const clv::Params& p, const clv::BatchArgs<real>& a, int step, 
   return clv_host::check_cuda("batch_stage_kernel");
 }
 
+// the 128-register cap is offered in FP32 only (FP64 spills heavily under it)
+template <class real> constexpr int capped_minb(int bs) { return sizeof(real) == 4 ? 512 / bs : 1; }
+
 template <class real, bool BULK>
-int stage_bs(const clv::Params& p, const clv::BatchArgs<real>& a, int step, int bs, int grid, cudaStream_t s) {
-  if (bs == 64) return launch_stage<real, BULK, 64>(p, a, step, grid, s);
-  if (bs == 128) return launch_stage<real, BULK, 128>(p, a, step, grid, s);
-  if (bs == 256) return launch_stage<real, BULK, 256>(p, a, step, grid, s);
+int stage_bs(const clv::Params& p, const clv::BatchArgs<real>& a, int step, int bs, int grid, bool cap,
+             cudaStream_t s) {
+  if (cap && sizeof(real) == 8) return clv_host::set_error(CLV_ERR_INVALID, "batch: max_registers is FP32 only");
+  if (bs == 64)
+    return cap ? launch_stage<real, BULK, 64, capped_minb<real>(64)>(p, a, step, grid, s)
+               : launch_stage<real, BULK, 64, 1>(p, a, step, grid, s);
+  if (bs == 128)
+    return cap ? launch_stage<real, BULK, 128, capped_minb<real>(128)>(p, a, step, grid, s)
+               : launch_stage<real, BULK, 128, 1>(p, a, step, grid, s);
+  if (bs == 256)
+    return cap ? launch_stage<real, BULK, 256, capped_minb<real>(256)>(p, a, step, grid, s)
+               : launch_stage<real, BULK, 256, 1>(p, a, step, grid, s);
   return clv_host::set_error(CLV_ERR_INVALID, "batch: block_size must be 64, 128 or 256");
 }
 
 template <class real>
-int batch_stage_t(const clv_params* pp, int step, const clv_batch* b, int bs, int grid, cudaStream_t s) {
+int batch_stage_t(const clv_params* pp, int step, const clv_batch* b, int bs, int grid, int max_regs,
+                  cudaStream_t s) {
   clv::Params p;
   clv::BatchArgs<real> a;
   int rc = make_args<real>(pp, b, &p, &a);
@@ -88,8 +100,10 @@ int batch_stage_t(const clv_params* pp, int step, const clv_batch* b, int bs, in
   if (step != 1 && step != 2) return clv_host::set_error(CLV_ERR_INVALID, "batch: step must be 1 or 2");
   if (p.flags & (clv::FLAG_GUBSER_VISC | clv::FLAG_PIMN_OMEGA | clv::FLAG_OMEGA_OMEGA | clv::FLAG_RIEMANN))
     return clv_host::set_error(CLV_ERR_INVALID, "batch: test flags (Gubser, couplings, Riemann) are not batched");
-  if (p.flags & clv::FLAG_BULK) return stage_bs<real, true>(p, a, step, bs, grid, s);
-  return stage_bs<real, false>(p, a, step, bs, grid, s);
+  if (max_regs != 0 && max_regs != 128) return clv_host::set_error(CLV_ERR_INVALID, "batch: max_registers must be 0 or 128");
+  const bool cap = max_regs == 128;
+  if (p.flags & clv::FLAG_BULK) return stage_bs<real, true>(p, a, step, bs, grid, cap, s);
+  return stage_bs<real, false>(p, a, step, bs, grid, cap, s);
 }
 
 template <class real> int batch_advance_t(const clv_params* pp, const clv_batch* b, int first, cudaStream_t s) {
@@ -106,10 +120,10 @@ template <class real> int batch_advance_t(const clv_params* pp, const clv_batch*
 extern "C" {
 
 int clv_batch_stage(const clv_params* p, int step, const clv_batch* b, int block_size, int grid_blocks,
-                    void* stream) {
+                    int max_registers, void* stream) {
   if (!p) return clv_host::set_error(CLV_ERR_INVALID, "batch: null clv_params");
-  if (p->precision == 4) return batch_stage_t<float>(p, step, b, block_size, grid_blocks, S(stream));
-  return batch_stage_t<double>(p, step, b, block_size, grid_blocks, S(stream));
+  if (p->precision == 4) return batch_stage_t<float>(p, step, b, block_size, grid_blocks, max_registers, S(stream));
+  return batch_stage_t<double>(p, step, b, block_size, grid_blocks, max_registers, S(stream));
 }
 
 int clv_batch_advance(const clv_params* p, const clv_batch* b, int first, void* stream) {
@@ -118,23 +132,35 @@ int clv_batch_advance(const clv_params* p, const clv_batch* b, int first, void* 
   return batch_advance_t<double>(p, b, first, S(stream));
 }
 
-int clv_batch_occupancy(const clv_params* p, int block_size, int* blocks_per_sm) {
+int clv_batch_occupancy(const clv_params* p, int block_size, int max_registers, int* blocks_per_sm) {
   if (!p || !blocks_per_sm || (p->precision != 4 && p->precision != 8))
     return clv_host::set_error(CLV_ERR_INVALID, "batch_occupancy: bad argument");
-  const bool bulk = p->flags & CLV_FLAG_BULK;
-  cudaError_t e = cudaErrorInvalidValue;
-  int n = 0;
-#define CLV_OCC(real, B, BS) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, clv::batch_stage_kernel<real, B, BS>, BS, 0)
   if (block_size != 64 && block_size != 128 && block_size != 256)
     return clv_host::set_error(CLV_ERR_INVALID, "batch_occupancy: block_size must be 64, 128 or 256");
+  if (max_registers != 0 && (max_registers != 128 || p->precision != 4))
+    return clv_host::set_error(CLV_ERR_INVALID, "batch_occupancy: max_registers must be 0 (or 128 in FP32)");
+  const bool bulk = p->flags & CLV_FLAG_BULK;
+  const bool cap = max_registers == 128;
+  int n = 0;
+  cudaError_t e = cudaSuccess;
+  const void* f = nullptr;
+#define CLV_K(real, B, BS, M) f = reinterpret_cast<const void*>(clv::batch_stage_kernel<real, B, BS, M>)
+#define CLV_PICK(real, B)                                                  \
+  do {                                                                     \
+    if (block_size == 64) { if (cap) CLV_K(real, B, 64, capped_minb<real>(64)); else CLV_K(real, B, 64, 1); }     \
+    else if (block_size == 128) { if (cap) CLV_K(real, B, 128, capped_minb<real>(128)); else CLV_K(real, B, 128, 1); } \
+    else { if (cap) CLV_K(real, B, 256, capped_minb<real>(256)); else CLV_K(real, B, 256, 1); } \
+  } while (0)
   if (p->precision == 4) {
-    if (bulk) { if (block_size == 64) CLV_OCC(float, true, 64); else if (block_size == 128) CLV_OCC(float, true, 128); else CLV_OCC(float, true, 256); }
-    else { if (block_size == 64) CLV_OCC(float, false, 64); else if (block_size == 128) CLV_OCC(float, false, 128); else CLV_OCC(float, false, 256); }
+    if (bulk) CLV_PICK(float, true);
+    else CLV_PICK(float, false);
   } else {
-    if (bulk) { if (block_size == 64) CLV_OCC(double, true, 64); else if (block_size == 128) CLV_OCC(double, true, 128); else CLV_OCC(double, true, 256); }
-    else { if (block_size == 64) CLV_OCC(double, false, 64); else if (block_size == 128) CLV_OCC(double, false, 128); else CLV_OCC(double, false, 256); }
+    if (bulk) CLV_PICK(double, true);
+    else CLV_PICK(double, false);
   }
-#undef CLV_OCC
+#undef CLV_PICK
+#undef CLV_K
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, f, block_size, 0);
   if (e != cudaSuccess) return clv_host::set_error(CLV_ERR_CUDA, std::string("batch_occupancy: ") + cudaGetErrorString(e));
   *blocks_per_sm = n;
   return CLV_OK;

@@ -66,8 +66,11 @@ template <class real> __device__ __forceinline__ real batch_tau(double tau0, dou
   return (real)(tau0 + (double)n * dt);
 }
 
-template <class real, bool BULK, int BS>
-__global__ void __launch_bounds__(BS) batch_stage_kernel(Params p, BatchArgs<real> a, int step) {
+// MINB > 1 caps the registers so that MINB blocks stay resident per SM
+// (MINB = 512 / BS: at most 128 registers a thread, as the single-event
+// per-cell kernel); MINB = 1 leaves the count to the compiler.
+template <class real, bool BULK, int BS, int MINB>
+__global__ void __launch_bounds__(BS, MINB) batch_stage_kernel(Params p, BatchArgs<real> a, int step) {
   __shared__ long long s_prefix[BATCH_MAX_EVENTS + 1];
   __shared__ int s_active[BATCH_MAX_EVENTS];
   const BatchCtl ctl = *a.ctl;

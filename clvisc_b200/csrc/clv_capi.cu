@@ -18,7 +18,8 @@ using clv_host::g_err;
 
 namespace {
 
-int g_stage_kernel = 0;  // CLV_OPT_STAGE_KERNEL: 0 tiled, 1 per-cell
+int g_stage_kernel = 0;  // CLV_OPT_STAGE_KERNEL: 0 automatic, 1 per-cell, 2 tiled where it applies
+constexpr int kTiledMinNz = 24;  // fewer cells along eta: per-cell kernel
 int g_chunk = 32;        // CLV_OPT_CHUNK: x planes per tiled CTA
 int g_minb = 2;          // CLV_OPT_TILED_BLOCKS: resident tiled CTAs per SM (FP32)
 
@@ -64,7 +65,7 @@ int to_params(const clv_params* in, clv::Params* out) {
   p.eos = in->eos_table;
   p.flags = in->flags;
   p.ZETAOS_MAX = in->zetaos_max; p.ZETAOS_T0 = in->zetaos_t0;
-  p.ZETAOS_WIDTH = in->zetaos_width; p.ZETAOS_SKEW = in->zetaos_skew;
+  p.ZETAOS_WIDTH = in->zetaos_width; p.ZETAOS_SKEW = in->zetaos_skew; p.ZETAOS_TMIN = in->zetaos_tmin;
   if ((in->flags & CLV_FLAG_BULK) && (!(in->zetaos_width > 0.0f) || !(in->zetaos_max >= 0.0f)))
     return fail(CLV_ERR_INVALID, "bulk sector: zetaos_width must be > 0 and zetaos_max >= 0%s");
   // correctly rounded reciprocals in each precision (host IEEE arithmetic, no
@@ -148,8 +149,10 @@ int visc_stage_t(const clv::Params& p, int step, double tau, int parts, const cl
   if (kt && (!v.evnew || !v.pin || (!is && !v.pi2in))) return fail(CLV_ERR_INVALID, "visc stage: null buffer for update_ev%s");
   if (v.write_udiff && (!kt || !v.udiff)) return fail(CLV_ERR_INVALID, "visc stage: write_udiff needs CLV_PART_KT%s");
   const bool bulk = p.flags & clv::FLAG_BULK;
-  // the tiled kernel has no bulk sector; bulk runs take the per-cell kernel
-  if (g_stage_kernel == 0 && !bulk) {
+  // The tiled kernel has no bulk sector, and its 8 x 32 (y, eta) tile leaves
+  // most threads idle on grids with few cells along eta ((2+1)D runs have
+  // one): those runs take the per-cell kernel, which gives the same bits.
+  if (!bulk && (g_stage_kernel == 2 || (g_stage_kernel == 0 && p.nz >= kTiledMinNz))) {
     if (is && kt) return launch_tiled<real, true, true>(p, v, step, tau, s);
     if (is) return launch_tiled<real, true, false>(p, v, step, tau, s);
     return launch_tiled<real, false, true>(p, v, step, tau, s);
@@ -237,12 +240,12 @@ int check_cuda(const char* where) { return cuda_check(where); }
 
 extern "C" {
 
-int clv_version(void) { return 0x000102; }
+int clv_version(void) { return 0x000103; }
 const char* clv_last_error(void) { return g_err.c_str(); }
 int clv_alignment(void) { return kAlign; }
 
 int clv_set_option(int option, int value) {
-  if (option == CLV_OPT_STAGE_KERNEL && (value == 0 || value == 1)) {
+  if (option == CLV_OPT_STAGE_KERNEL && value >= 0 && value <= 2) {
     g_stage_kernel = value;
     return CLV_OK;
   }

@@ -33,6 +33,7 @@ struct Params {
   int flags;
   // bulk sector (FLAG_BULK): zeta/s(T) peak, position, width, skewness
   float ZETAOS_MAX, ZETAOS_T0, ZETAOS_WIDTH, ZETAOS_SKEW;
+  float ZETAOS_TMIN;  // Pi = 0 in cells colder than this
   Recips<float> rf;   // reciprocals for float kernels
   Recips<double> rd;  // reciprocals for double kernels
 };

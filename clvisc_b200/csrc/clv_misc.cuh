@@ -21,9 +21,14 @@ __global__ void visc_initialize_kernel(Params p, real* pi1, uint8_t* goodcell, r
   pi1[pidx(1, 1) * ld + I] = tmp;
   pi1[pidx(2, 2) * ld + I] = tmp;
   pi1[pidx(3, 3) * ld + I] = -2.0f * tmp;
-  if (p.flags & FLAG_BULK) {  // bulk sector: Navier-Stokes Pi of Bjorken flow, theta = 1/tau
+  if (p.flags & FLAG_BULK) {  // bulk sector: Navier-Stokes Pi of Bjorken flow, theta = 1/tau, regulated
     real zetav = zetaos<real>(p, T) * s * CLV_HBARC;
-    pi1[10 * ld + I] = -zetav / tau;
+    real b0 = -zetav / tau;
+    real pb = eos_comp<real>(p, e, 1);
+    if (b0 < -pb) b0 = -pb;
+    else if (b0 > pb) b0 = pb;
+    if (T < p.ZETAOS_TMIN) b0 = 0.0f;
+    pi1[10 * ld + I] = b0;
   }
 #pragma unroll
   for (int c = 0; c < 4; c++) udiff[c * ld + I] = 0.0f;

@@ -60,13 +60,6 @@ __device__ __forceinline__ Stencil make_stencil(int q, int L, long long stride) 
   return s;
 }
 
-// weight of pi^{mu nu} sigma^{mu nu} in the full contraction over mu <= nu:
-// g_{mu mu} g_{nu nu}, doubled off the diagonal (bulk sector)
-template <class real> __device__ __forceinline__ real pisig_weight(int mu, int nu) {
-  real w = (mu == nu) ? (real)1.0f : (real)2.0f;
-  return ((mu == 0) != (nu == 0)) ? -w : w;
-}
-
 // update_pimn (kernel_IS.cl:501-709) for cell I: e0 and pc are the stage
 // input ev and pi at the cell, grad the velocity gradients, S10 the IS sources
 // (updated in place); writes pi_new and goodcell, returns the new pi in pinew.
@@ -139,7 +132,6 @@ __device__ __forceinline__ void pi_update(const Params& p, const ViscBuffers<rea
   const real den = u_new[0] + p.DT * one_over_taupi;
   const real rden = (real)1.0f / den;
   real max_pimn_abs = 0.0f;
-  real pisig = 0.0f;  // bulk sector: pi^{mu nu} sigma_{mu nu}
 #pragma unroll
   for (int mu = 0; mu < 4; mu++)
 #pragma unroll
@@ -150,7 +142,6 @@ __device__ __forceinline__ void pi_update(const Params& p, const ViscBuffers<rea
                    2.0f / 3.0f * (gmn<real>(mu, nu) - u[mu] * u[nu]) * theta;
       const int mn = pidx(mu, nu);
       if (u[0] > 10000.0f) sigma = 0.0f;
-      if (BULK) pisig = pisig + pisig_weight<real>(mu, nu) * pc[mn] * sigma;
       real piNS = etav * sigma;
       real pi_old = b.pi1[mn * ld + I] * u_old[0];
       real src = div_by<real>(-pc[mn] * theta, (real)3.0f, rc.three) - div_by<real>(pc[mn] * u[0], tau, tc.rtau);
@@ -175,12 +166,14 @@ __device__ __forceinline__ void pi_update(const Params& p, const ViscBuffers<rea
       pinew[mn] = pi_old;
     }
   if (BULK) {
-    // Bulk sector (no counterpart in the reference): the 14-moment relaxation
-    // equation of Denicol, Niemi, Molnar and Rischke (PRD 85, 114047 (2012)),
-    // tau_Pi D Pi + Pi = -zeta theta - 2/3 tau_Pi Pi theta
-    //   + 8/5 (1/3 - cs2) tau_Pi pi^{mu nu} sigma_{mu nu},
-    // tau_Pi = zeta / (14.55 (1/3 - cs2)^2 (e + P)), for the density u0 Pi
-    // with the same implicit relaxation step as the shear components.
+    // Bulk sector (no counterpart in the reference): the relaxation equation
+    // tau_Pi D Pi + Pi = -zeta theta - 2/3 tau_Pi Pi theta with the 14-moment
+    // tau_Pi = zeta / (14.55 (1/3 - cs2)^2 (e + P)) of Denicol, Niemi, Molnar
+    // and Rischke (PRD 85, 114047 (2012)), for the density u0 Pi with the same
+    // implicit relaxation step as the shear components. No shear-bulk
+    // coupling; |Pi| <= P and Pi = 0 below ZETAOS_TMIN, which keep dilute
+    // cells at the edge of a fireball (|pi| >> e, far below freeze-out) from
+    // running away.
     real cs2 = eos_comp<real>(p, ed_step, 0);
     real local_zetaos = zetaos<real>(p, temperature);
     real zetav = local_zetaos * sdens * CLV_HBARC;
@@ -189,12 +182,16 @@ __device__ __forceinline__ void pi_update(const Params& p, const ViscBuffers<rea
     real bulkNS = -zetav * theta;
     if (u[0] > 10000.0f) bulkNS = 0.0f;
     real bc = pc[10];
-    real srcB = div_by<real>(bc * theta, (real)3.0f, rc.three) - div_by<real>(bc * u[0], tau, tc.rtau) +
-                0.8f * dcs * pisig;
+    real srcB = div_by<real>(bc * theta, (real)3.0f, rc.three) - div_by<real>(bc * u[0], tau, tc.rtau);
     S10[10] += srcB;
     real b_old = b.pi1[10 * ld + I] * u_old[0];
-    pinew[10] = (b_old + div_step(S10[10] * p.DT, step) + p.DT * one_over_taubulk * bulkNS) /
-                (u_new[0] + p.DT * one_over_taubulk);
+    b_old = (b_old + div_step(S10[10] * p.DT, step) + p.DT * one_over_taubulk * bulkNS) /
+            (u_new[0] + p.DT * one_over_taubulk);
+    const real pb = eosP<real>(p, e2s0);
+    if (b_old < -pb) b_old = -pb;
+    else if (b_old > pb) b_old = pb;
+    if (temperature < p.ZETAOS_TMIN) b_old = 0.0f;
+    pinew[10] = b_old;
   }
   real pre = eosP<real>(p, e2s0);
   real T00 = (e2s0 + pre) * u_new[0] * u_new[0] - pre;
@@ -371,6 +368,26 @@ __device__ __forceinline__ void visc_stage_cell(const Params& p, const GridDims 
   for (int a = 0; a < 3; a++) {
     const int q = a == 0 ? i : (a == 1 ? j : k);
     const int L = a == 0 ? gd.nx : (a == 1 ? gd.ny : gd.nz);
+    if (L == 1) {
+      // One cell along this axis (a (2+1)D event along eta): the five stencil
+      // cells are this cell, so both face fluxes are the same value and their
+      // difference is +0, which leaves every source unchanged, and the limited
+      // velocity difference is +0. Only the Christoffel part of the eta
+      // gradient remains. For a finite state this gives the bits of the full
+      // evaluation; a non-finite state already turns the x or y terms to NaN.
+      if (DO_IS) {
+#pragma unroll
+        for (int c = 0; c < 4; c++) grad[a][c] = 0.0f;
+        if (a == 2) {
+          const real u0c = gamma3<real>(e0[1], e0[2], e0[3]);
+          grad[2][0] = grad[2][0] + div_by<real>(e0[3] * u0c, tau, tc.rtau);
+          grad[2][1] = grad[2][1] + div_by<real>((real)0.0f * u0c, tau, tc.rtau);
+          grad[2][2] = grad[2][2] + div_by<real>((real)0.0f * u0c, tau, tc.rtau);
+          grad[2][3] = grad[2][3] + div_by<real>((real)1.0f * u0c, tau, tc.rtau);
+        }
+      }
+      continue;
+    }
     const long long stride = a == 0 ? (long long)gd.ny * gd.nz : (a == 1 ? (long long)gd.nz : 1ll);
     const Stencil st = make_stencil(q, L, stride);
     const real D = a == 0 ? (real)p.DX : (a == 1 ? (real)p.DY : tc.dzt);
@@ -564,6 +581,9 @@ __global__ void __launch_bounds__(128) ideal_stage_kernel(Params p, IdealBuffers
   for (int a = 0; a < 3; a++) {
     const int q = a == 0 ? i : (a == 1 ? j : k);
     const int L = a == 0 ? p.nx : (a == 1 ? p.ny : p.nz);
+    // one cell along this axis: both face fluxes are equal, their difference
+    // is +0 and leaves the sources unchanged (finite states; see visc_stage_cell)
+    if (L == 1) continue;
     const long long stride = a == 0 ? (long long)p.ny * p.nz : (a == 1 ? (long long)p.nz : 1ll);
     const Stencil st = make_stencil(q, L, stride);
     real E[5][4], pr[5], T[5][4];

@@ -70,6 +70,7 @@ def add_visc_params(c, p):
     p.zetaos_t0 = float_literal(getattr(c, 'ZETAOS_T0', 0.18))
     p.zetaos_width = float_literal(getattr(c, 'ZETAOS_WIDTH', 0.02))
     p.zetaos_skew = float_literal(getattr(c, 'ZETAOS_SKEW', 0.0))
+    p.zetaos_tmin = float_literal(getattr(c, 'ZETAOS_TMIN', 0.1))
     if bulk:
         flags |= _lib.CLV_FLAG_BULK
     p.flags = flags

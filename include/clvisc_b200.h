@@ -44,10 +44,10 @@ extern "C" {
  * kernel_visc.cl:31-33 keeps a zero placeholder for the bulk pressure): pi
  * fields carry an eleventh plane Pi and the stage sources a fifteenth.
  * zeta/s(T) = zetaos_max w^2 / (w^2 + (T - zetaos_t0)^2) with
- * w = zetaos_width (1 + zetaos_skew sign(T - zetaos_t0)); Pi relaxes by the
- * 14-moment equation tau_Pi D Pi + Pi = -zeta theta - 2/3 tau_Pi Pi theta
- * + 8/5 (1/3 - cs2) tau_Pi pi:sigma, tau_Pi = zeta / (14.55 (1/3 - cs2)^2 (e+P)),
- * and P + Pi replaces P in T^{mu nu}. */
+ * w = zetaos_width (1 + zetaos_skew sign(T - zetaos_t0)); Pi relaxes by
+ * tau_Pi D Pi + Pi = -zeta theta - 2/3 tau_Pi Pi theta with the 14-moment
+ * tau_Pi = zeta / (14.55 (1/3 - cs2)^2 (e+P)), is held within |Pi| <= P and
+ * at zero in cells colder than zetaos_tmin, and P + Pi replaces P in T^{mu nu}. */
 #define CLV_FLAG_BULK 16
 
 /* parts of a viscous stage (visc.py:287 IS_stepUpdate, visc.py:232 visc_stepUpdate) */
@@ -70,6 +70,7 @@ typedef struct clv_params {
   const float *eos_table; /* device, eos_nrow*eos_ncol texels of (cs2, p, T, s) */
   int flags;              /* CLV_FLAG_* */
   float zetaos_max, zetaos_t0, zetaos_width, zetaos_skew; /* bulk sector (CLV_FLAG_BULK) */
+  float zetaos_tmin;      /* bulk sector: Pi = 0 in cells colder than this */
 } clv_params;
 
 /* Buffers of one viscous Runge-Kutta stage. `step` is 1 or 2 as in
@@ -93,7 +94,9 @@ typedef struct clv_visc_buffers {
 } clv_visc_buffers;
 
 /* Tuning options (process-wide): the viscous-stage kernel variant
- * (0 = tiled, the default; 1 = one thread per cell without shared memory),
+ * (0 = automatic, the default: the tiled kernel on grids with at least 24
+ * cells along eta and no bulk sector, else one thread per cell; 1 = one
+ * thread per cell without shared memory; 2 = tiled wherever it applies),
  * the number of x planes a tiled thread block marches through, and the
  * number of tiled blocks kept resident per SM in FP32 (1 or 2; FP64 uses 1).
  * Every variant computes the same values bit for bit. */
@@ -222,10 +225,12 @@ typedef struct clv_batch {
 
 /* One fused Runge-Kutta stage (step 1 or 2) of every running event: one
  * persistent launch of grid_blocks blocks of block_size (64, 128 or 256)
- * threads; grid_blocks <= 0 sizes the grid to fill the GPU once. Reads tau and
+ * threads; grid_blocks <= 0 sizes the grid to fill the GPU once.
+ * max_registers: 0 lets the compiler choose; 128 (FP32 only) caps the
+ * registers a thread so that 512 threads stay resident per SM. Reads tau and
  * the running list from the device, so it can be captured in a CUDA graph. */
 int clv_batch_stage(const clv_params *p, int step, const clv_batch *b, int block_size, int grid_blocks,
-                    void *stream);
+                    int max_registers, void *stream);
 /* After a step (first = 0) or once before the first step (first = 1, with
  * keys holding each event's initial maximum energy density): count the step,
  * apply the stop test at multiples of ntskip, record the history, rebuild the
@@ -233,7 +238,7 @@ int clv_batch_stage(const clv_params *p, int step, const clv_batch *b, int block
  * except for the first call. */
 int clv_batch_advance(const clv_params *p, const clv_batch *b, int first, void *stream);
 /* Resident blocks per SM of the batch stage kernel at block_size threads. */
-int clv_batch_occupancy(const clv_params *p, int block_size, int *blocks_per_sm);
+int clv_batch_occupancy(const clv_params *p, int block_size, int max_registers, int *blocks_per_sm);
 
 /* Host-boundary layout transposes: (n, w) row-major <-> w planes of ld. */
 int clv_aos_to_soa(const clv_params *p, const void *aos, void *soa, long long n, int w, void *stream);

@@ -306,9 +306,14 @@ void visc_initialize(const Consts& c, real* pi1, real* goodcell, real* udiff, co
     pi1[10 * I + idx(1, 1)] = tmp;
     pi1[10 * I + idx(2, 2)] = tmp;
     pi1[10 * I + idx(3, 3)] = -2.0f * tmp;
-    if (bulk1) {  // bulk sector: Navier-Stokes value for Bjorken flow, theta = 1/tau
+    if (bulk1) {  // bulk sector: Navier-Stokes value for Bjorken flow, theta = 1/tau, regulated
       real zetav = H.zetaos(cpTs.s2) * cpTs.s3 * CLVO_HBARC;
-      bulk1[I] = -zetav / tau;
+      real b0 = -zetav / tau;
+      real pb = cpTs.s1;
+      if (b0 < -pb) b0 = -pb;
+      else if (b0 > pb) b0 = pb;
+      if (cpTs.s2 < c.ZETAOS_TMIN) b0 = 0.0f;
+      bulk1[I] = b0;
     }
     st4(udiff, I, V4<real>{0.0f, 0.0f, 0.0f, 0.0f});
     goodcell[I] = 1.0f;
@@ -456,13 +461,6 @@ real omega_omega(int lam, int mu, int nu, const real omega[6], const real u[4]) 
   return firstTerm + secondTerm;
 }
 
-// weight of pi^{mu nu} sigma^{mu nu} in the full contraction over mu <= nu:
-// g_{mu mu} g_{nu nu}, doubled off the diagonal (bulk sector)
-template <class real> inline real pisig_weight(int mu, int nu) {
-  real w = (mu == nu) ? (real)1.0f : (real)2.0f;
-  return ((mu == 0) != (nu == 0)) ? -w : w;
-}
-
 // kernel_IS.cl:501-709
 template <class real>
 void update_pimn(const Consts& c, real* pinew, real* goodcell, const real* pi1, const real* pistep, const real* ev1,
@@ -527,14 +525,12 @@ void update_pimn(const Consts& c, real* pinew, real* goodcell, const real* pi1, 
     }
     real sigma;
     real max_pimn_abs = 0.0f;
-    real pisig = 0.0f;  // bulk sector: pi^{mu nu} sigma_{mu nu}, sigma as below (twice the usual shear tensor)
     for (int mu = 0; mu < 4; mu++)
       for (int nu = mu; nu < 4; nu++) {
         sigma = dot(gm<real>(mu), da[nu]) + dot(gm<real>(nu), da[mu]) - (u[mu] * DU[nu] + u[nu] * DU[mu]) -
                 2.0f / 3.0f * (gmn<real>(mu, nu) - u[mu] * u[nu]) * theta;
         int mn = idx(mu, nu);
         if (u[0] > 10000.0f) sigma = 0.0f;
-        if (bulknew) pisig = pisig + pisig_weight<real>(mu, nu) * pi2[mn] * sigma;
         real piNS = etav * sigma;
         real pi_old = pi1[10 * I + mn] * u_old.s0;
         real src = -pi2[mn] * theta / 3.0f - pi2[mn] * u[0] / tau;
@@ -563,15 +559,17 @@ void update_pimn(const Consts& c, real* pinew, real* goodcell, const real* pi1, 
         pinew[10 * I + mn] = pi_old;
       }
     if (bulknew) {
-      // Bulk sector (no counterpart in the reference): the 14-moment
-      // relaxation equation of Denicol, Niemi, Molnar and Rischke (PRD 85,
-      // 114047 (2012)), tau_Pi D Pi + Pi = -zeta theta - delta_PiPi Pi theta
-      // + lambda_Pipi pi^{mu nu} sigma_{mu nu}, with delta_PiPi = 2/3 tau_Pi,
-      // lambda_Pipi = 8/5 (1/3 - cs2) tau_Pi and
+      // Bulk sector (no counterpart in the reference): the relaxation
+      // equation tau_Pi D Pi + Pi = -zeta theta - delta_PiPi Pi theta with the
+      // 14-moment coefficients of Denicol, Niemi, Molnar and Rischke (PRD 85,
+      // 114047 (2012)), delta_PiPi = 2/3 tau_Pi and
       // tau_Pi = zeta / (14.55 (1/3 - cs2)^2 (e + P)), written like the shear
       // update above for the conserved density u0 * Pi:
-      // d(u0 Pi) + div(v u0 Pi) = Pi theta / 3 - Pi u0 / tau
-      //   + 4/5 (1/3 - cs2) pisig - (Pi - Pi_NS) / tau_Pi.
+      // d(u0 Pi) + div(v u0 Pi) = Pi theta / 3 - Pi u0 / tau - (Pi - Pi_NS) / tau_Pi.
+      // The shear-bulk coupling lambda_Pipi pi^{mu nu} sigma_{mu nu} is left
+      // out: in dilute cells at the edge of a fireball, where |pi| >> e, it
+      // drove Pi past -P and the step became unstable (so did the regulated
+      // equation without the cut at ZETAOS_TMIN below).
       real local_zetaos = H.zetaos(temperature);
       real zetav = local_zetaos * cpTs.s3 * CLVO_HBARC;
       real dcs = 1.0f / 3.0f - cpTs.s0;
@@ -579,11 +577,20 @@ void update_pimn(const Consts& c, real* pinew, real* goodcell, const real* pi1, 
       real bulkNS = -zetav * theta;
       if (u[0] > 10000.0f) bulkNS = 0.0f;
       real bc = bulkstep[I];
-      real srcB = bc * theta / 3.0f - bc * u[0] / tau + 0.8f * dcs * pisig;
+      real srcB = bc * theta / 3.0f - bc * u[0] / tau;
       SrcB[I] += srcB;
       real b_old = bulk1[I] * u_old.s0;
       b_old = (b_old + SrcB[I] * c.DT / step + c.DT * one_over_taubulk * bulkNS) /
               (u_new.s0 + c.DT * one_over_taubulk);
+      // regulators: |Pi| <= P, so that the effective pressure P + Pi stays
+      // >= 0, and Pi = 0 in cells colder than ZETAOS_TMIN. In dilute cells at
+      // the edge of a fireball (|pi| >> e, T far below freeze-out) the
+      // relaxation equation otherwise drives Pi past -P, the T^{tau mu} ->
+      // (e, v) root find has no physical solution and the step runs away.
+      real pb = H.E.P(e_v2.s0);
+      if (b_old < -pb) b_old = -pb;
+      else if (b_old > pb) b_old = pb;
+      if (temperature < c.ZETAOS_TMIN) b_old = 0.0f;
       bulknew[I] = b_old;
     }
     real pre = H.E.P(e_v2.s0);

@@ -40,6 +40,7 @@ struct Consts {
   // zero placeholder); these fields select the bulk sector specified below.
   int bulk;
   float ZETAOS_MAX, ZETAOS_T0, ZETAOS_WIDTH, ZETAOS_SKEW;
+  float ZETAOS_TMIN;  // Pi = 0 in cells colder than this
 };
 
 // real_type.h:9,16

@@ -35,7 +35,7 @@ class Consts(ctypes.Structure):
         ('pimn_omega_coupling', ctypes.c_int), ('omega_omega_coupling', ctypes.c_int),
         ('bulk', ctypes.c_int),
         ('ZETAOS_MAX', ctypes.c_float), ('ZETAOS_T0', ctypes.c_float), ('ZETAOS_WIDTH', ctypes.c_float),
-        ('ZETAOS_SKEW', ctypes.c_float),
+        ('ZETAOS_SKEW', ctypes.c_float), ('ZETAOS_TMIN', ctypes.c_float),
     ]
 
 
@@ -165,6 +165,7 @@ def make_consts(cfg, meta, table, efrz, eos_kind=0):
     c.ZETAOS_T0 = fl(getattr(cfg, 'ZETAOS_T0', 0.18))
     c.ZETAOS_WIDTH = fl(getattr(cfg, 'ZETAOS_WIDTH', 0.02))
     c.ZETAOS_SKEW = fl(getattr(cfg, 'ZETAOS_SKEW', 0.0))
+    c.ZETAOS_TMIN = fl(getattr(cfg, 'ZETAOS_TMIN', 0.1))
     c.bulk = int(float(getattr(cfg, 'ZETAOS_MAX', 0.0)) > 0.0)
     return c
 

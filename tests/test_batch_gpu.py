@@ -71,7 +71,7 @@ def test_batch_graph_equals_eager_and_autotune_restores(cuda_lib, use_float32):
         b = _batch(use_float32, True, ics)
         if mode == 'tuned':
             res = b.autotune(steps=3)
-            assert len(res) >= 3 and (b.block_size, b.grid_blocks) in res
+            assert len(res) >= 3 and (b.block_size, b.grid_blocks, b.max_registers) in res
         steps = b.evolve(use_graph=(mode != 'eager'))
         runs.append((steps, b.loops(), [b.ev_to_host(e) for e in range(len(GRIDS))],
                      [b.bulk_to_host(e) for e in range(len(GRIDS))]))

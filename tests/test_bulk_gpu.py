@@ -111,3 +111,27 @@ def test_bulk_evolve_hypersf_parity(cuda_lib, oracle_mod, use_float32, tmp_path)
     assert n == len(sf_o) and n > 0
     assert_same('hypersf', v.ideal.d_hypersf[:n].cpu().numpy(), sf_o)
     assert_same('pisf', v.d_pi_sf[:n].cpu().numpy(), pi_o)
+
+
+def test_bulk_edge_stability_to_freezeout(cuda_lib):
+    """A peripheral (2+1)D event of the batched workload (229^2 cells of
+    0.16 fm, b = 10.5 fm, eta/s = 0.16, zeta/s peak 0.05) evolved to freeze-out
+    with the bulk sector: without the regulators (|Pi| <= P, Pi = 0 below
+    ZETAOS_TMIN) dilute cells at the edge of the fireball ran away near step
+    260. The state must stay finite and the maximum energy density must fall."""
+    import os
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    import bench
+    from clvisc_b200.initial import glauber_event
+    from clvisc_b200.visc import CLVisc
+    n, b, seed = bench.batch_event_spec(33)
+    cfg = bench.batch_cfg(n)
+    v = CLVisc(cfg)
+    v.load_ini(glauber_event(n, n, 1, 0.16, 0.16, 0.15, b=b, seed=seed, edmax=50.0))
+    v.evolve(save_hypersf=False)
+    ev = v.ideal.ev_to_host()
+    assert np.isfinite(ev).all() and np.isfinite(v.bulk_to_host()).all()
+    h = np.array(v.ideal.history, np.float64)
+    assert len(h) > 5 and (np.diff(h[:, 1]) < 0).all()
+    assert h[-1, 1] < v.ideal.efrz

@@ -132,3 +132,47 @@ def test_bulk_off_is_bitwise_unchanged(oracle_mod, use_float32):
         runs.append((v.ideal.d_ev[1].copy(), v.d_pi[1].copy()))
     np.testing.assert_array_equal(runs[0][0], runs[1][0])
     np.testing.assert_array_equal(runs[0][1], runs[1][1])
+
+
+def test_bulk_held_at_zero_below_tmin(oracle_mod):
+    """Cells colder than ZETAOS_TMIN carry no bulk pressure: with the cut above
+    every temperature of the run, Pi stays 0 and e(tau) is bit for bit the
+    run without the bulk sector (P + 0 = P)."""
+    def run(zmax, tmin):
+        cfg = make_cfg(1, 1, 1, use_float32=True, dt=0.02, etaos=0.08, ZETAOS_MAX=zmax, ZETAOS_TMIN=tmin)
+        v = oracle_mod.OracleVisc(cfg)
+        ini = np.zeros((1, 4))
+        ini[0, 0] = 4.0
+        v.load_ini(ini)
+        v.IS_initialize()
+        v.ideal.stepUpdate(1)
+        for n in range(60):
+            v.step(n)
+            if zmax > 0:
+                assert v.d_bulk[1][0] == 0.0
+        return v.ideal.d_ev[1].copy(), v.d_pi[1].copy()
+    e_cut, pi_cut = run(0.2, 5.0)
+    e_off, pi_off = run(0.0, 5.0)
+    np.testing.assert_array_equal(e_cut, e_off)
+    np.testing.assert_array_equal(pi_cut, pi_off)
+
+
+def test_bulk_bounded_by_pressure(oracle_mod):
+    """A large zeta/s drives the Navier-Stokes value -zeta theta below -P; the
+    bulk pressure is held at -P of the energy density the update reads (the
+    Runge-Kutta predictor in d_ev[2]), so P + Pi stays >= 0 there."""
+    cfg = make_cfg(1, 1, 1, use_float32=False, dt=0.02, etaos=0.0, ZETAOS_MAX=20.0, ZETAOS_T0=0.18,
+                   ZETAOS_WIDTH=0.02)
+    v = oracle_mod.OracleVisc(cfg)
+    ini = np.zeros((1, 4))
+    ini[0, 0] = 4.0
+    v.load_ini(ini)
+    v.IS_initialize()
+    v.ideal.stepUpdate(1)
+    at_bound = 0
+    for n in range(70):
+        v.step(n)
+        pb = v.k.P(v.ideal.d_ev[2][0, 0])
+        assert -pb <= v.d_bulk[1][0] <= pb
+        at_bound += v.d_bulk[1][0] == -pb
+    assert at_bound > 50

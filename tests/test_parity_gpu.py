@@ -93,11 +93,13 @@ def test_visc_parts_parity(cuda_lib, oracle_mod, use_float32, grid, stage_varian
         _compare_visc(v, o, 'parts n=%d' % n)
 
 
-@pytest.fixture(params=['tiled', 'tiled-1blk', 'tiled-chunk5', 'per-cell'])
+@pytest.fixture(params=['auto', 'tiled', 'tiled-1blk', 'tiled-chunk5', 'per-cell'])
 def stage_variant(request, cuda_lib):
     """Every viscous-stage kernel variant; restores the default afterwards."""
     from clvisc_b200 import _lib
-    opts = {'tiled': [], 'tiled-1blk': [(_lib.CLV_OPT_TILED_BLOCKS, 1)], 'tiled-chunk5': [(_lib.CLV_OPT_CHUNK, 5)],
+    tiled = (_lib.CLV_OPT_STAGE_KERNEL, 2)  # tiled on every grid, short eta axes included
+    opts = {'auto': [], 'tiled': [tiled], 'tiled-1blk': [tiled, (_lib.CLV_OPT_TILED_BLOCKS, 1)],
+            'tiled-chunk5': [tiled, (_lib.CLV_OPT_CHUNK, 5)],
             'per-cell': [(_lib.CLV_OPT_STAGE_KERNEL, 1)]}[request.param]
     for o, v in opts:
         _lib.set_option(o, v)
