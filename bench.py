@@ -280,6 +280,21 @@ def run_batch(n_events=BATCH_EVENTS, one_at_a_time=True):
                 'batch_steps': int(steps), 'event_steps': [int(x) for x in loops],
                 'cell_updates_per_s': float(sum(n * n * int(l) for (n, _, _), l in zip(specs, loops)) /
                                             (t_solved - t_solve))})
+    # end to end from the seeds: participants sampled on the host, the energy
+    # density summed on the device (clv_hotspot_ini), evolve, results to host
+    del bt
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    bt = CLViscBatch(cfg, grids, block_size=shape[0], grid_blocks=shape[1], max_registers=shape[2])
+    for e, (n, bb, sd) in enumerate(specs):
+        bt.load_hotspot_event(e, b=bb, seed=sd, edmax=50.0)
+    bt.evolve()
+    finals2 = [bt.ev_to_host(e) for e in range(n_events)]
+    t2 = time.perf_counter() - t
+    out['e2e_from_seeds'] = {'value': n_events / t2 * 3600.0, 'unit': 'events/h', 'seconds': t2,
+                             'initial_condition': 'participants on the host, energy density on the device',
+                             'nan_values': int(sum(np.count_nonzero(np.isnan(g)) for g in finals2))}
+    del bt
     if one_at_a_time:
         torch.cuda.synchronize()
         t = time.perf_counter()

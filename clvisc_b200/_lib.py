@@ -49,6 +49,11 @@ class ClvParams(ctypes.Structure):
     ]
 
 
+class ClvGlauber(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_float) for n in ('num_of_nucleons', 'sqrts', 'ro0', 'r', 'eta', 'si0',
+                                                'impact_parameter', 'edmax', 'hwn', 'eta_flat', 'eta_gw')]
+
+
 class ClvViscBuffers(ctypes.Structure):
     _fields_ = [
         ('ev_st', ctypes.c_void_p), ('pi_st', ctypes.c_void_p),
@@ -90,6 +95,13 @@ _SIGS = {
     'clv_batch_stage': ([_P, ctypes.c_int, _VP, ctypes.c_int, ctypes.c_int, ctypes.c_int, _VP], ctypes.c_int),
     'clv_batch_advance': ([_P, _VP, ctypes.c_int, _VP], ctypes.c_int),
     'clv_batch_occupancy': ([_P, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
+    # initial conditions (clv_glauber is passed as a pointer to ClvGlauber)
+    'clv_glauber_ini': ([_P, _VP, _VP, _VP], ctypes.c_int),
+    'clv_glauber_nbinary': ([_P, _VP, _VP, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                             ctypes.c_int, ctypes.c_int, _VP], ctypes.c_int),
+    'clv_hotspot_scratch_bytes': ([_P, ctypes.c_int], ctypes.c_size_t),
+    'clv_hotspot_ini': ([_P, _VP, _VP, ctypes.c_int] + [ctypes.c_double] * 7 + [_VP, ctypes.c_size_t, _VP],
+                        ctypes.c_int),
 }
 
 

@@ -186,6 +186,15 @@ class CLViscBatch(object):
         if not isinstance(dat, torch.Tensor):
             torch.cuda.current_stream(self.device).synchronize()
 
+    def load_hotspot_event(self, e, b=8.0, seed=5, edmax=50.0):
+        """Event e's d_ev[1] = initial.glauber_event(nx, ny, nz, DX, DY, DZ, b,
+        seed, edmax), summed on the device from host-sampled participants."""
+        from .initial import hotspot_ini, hotspot_table
+        c = self.cfg
+        keep = hotspot_ini(self.lib, self.event_params[e], self._view(self.d_ev[1], e, 'ev'), hotspot_table(b, seed),
+                           c.DX, c.DY, c.DZ, edmax=edmax, stream=self.stream)
+        self._keep = keep  # released by the next call, after the stream has used it
+
     def _batch(self):
         b = _Batch()
         b.events = self.d_events.data_ptr()

@@ -149,6 +149,39 @@ class CLIdeal(object):
         self._call('clv_aos_to_soa', _lib.ptr(dev), _lib.ptr(self.d_ev[1]), self.size, 4, self.stream)
         torch.cuda.current_stream(self.device).synchronize()
 
+    def optical_glauber_ini(self, system='Au+Au', cent_min=None, cent_max=None, save_binary_collisions=False):
+        """d_ev[1] from the optical Glauber model on the device
+        (visc.py:151-172, kernel_glauber.cl:86-102); with a centrality class the
+        impact parameter is its weighted mean (glauber.py:14-57) and is written
+        into the configuration, as in the reference."""
+        from .glauber import glauber_consts, weight_mean_b
+        if cent_min is not None and cent_max is not None:
+            self.cfg.ImpactParameter = weight_mean_b(cent_min, cent_max, system)
+        g = glauber_consts(self.cfg)
+        self._call('clv_glauber_ini', ctypes.byref(g), _lib.ptr(self.d_ev[1]), self.stream)
+        if save_binary_collisions:
+            self.save_nbinary()
+
+    def save_nbinary(self, dx=0.3, dy=0.3, xlow=-9.75, ylow=-9.75, nx=66, ny=66):
+        """Binary collisions on a (66, 66) grid into fPathOut/nbin.dat (glauber.py:94-103)."""
+        from .glauber import glauber_consts
+        g = glauber_consts(self.cfg)
+        out = torch.empty(nx * ny, dtype=self.dtype, device=self.device)
+        self._call('clv_glauber_nbinary', ctypes.byref(g), _lib.ptr(out), float(self.cfg.real(xlow)),
+                   float(self.cfg.real(ylow)), float(self.cfg.real(dx)), float(self.cfg.real(dy)), nx, ny, self.stream)
+        np.savetxt(os.path.join(self.cfg.fPathOut, 'nbin.dat'), out.cpu().numpy().reshape(nx, ny))
+
+    def load_hotspot_event(self, b=8.0, seed=5, edmax=50.0):
+        """d_ev[1] = initial.glauber_event(NX, NY, NZ, DX, DY, DZ, b, seed,
+        edmax), with the participants sampled on the host and the energy density
+        summed on the device."""
+        from .initial import hotspot_ini, hotspot_table
+        c = self.cfg
+        keep = hotspot_ini(self.lib, self.params, self.d_ev[1], hotspot_table(b, seed), c.DX, c.DY, c.DZ,
+                           edmax=edmax, stream=self.stream)
+        torch.cuda.current_stream(self.device).synchronize()
+        del keep
+
     def load_ini_device(self, dev_aos):
         """load_ini from a device tensor of shape (NX*NY*NZ, 4)."""
         dev_aos = dev_aos.to(self.device, self.dtype).contiguous()

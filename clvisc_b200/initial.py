@@ -42,10 +42,24 @@ def participants(rng, b, A=208, R=6.62, a=0.546, sigma_nn=6.4):
     return np.concatenate([na[hit.any(1)], nb[hit.any(0)]])
 
 
-def transverse_profile(rng, nx, ny, dx, dy, b, width=0.5, gamma_k=1.6, **kw):
-    """Sum of weighted Gaussian hotspots on the (nx, ny) grid (unnormalised)."""
+def hotspots(rng, b, gamma_k=1.6, **kw):
+    """Participant positions (n, 2) and their Gamma(k, 1/k) weights (n,)."""
     parts = participants(rng, b, **kw)
     w = rng.gamma(gamma_k, 1.0 / gamma_k, len(parts))
+    return parts, w
+
+
+def hotspot_table(b=8.0, seed=5):
+    """(n, 3) float64 array of participant (x, y, weight) of the seeded event
+    glauber_event(..., b, seed) builds, for the device generator
+    (clv_hotspot_ini)."""
+    parts, w = hotspots(np.random.default_rng(seed), b)
+    return np.ascontiguousarray(np.column_stack([parts, w]), dtype=np.float64)
+
+
+def transverse_profile(rng, nx, ny, dx, dy, b, width=0.5, gamma_k=1.6, **kw):
+    """Sum of weighted Gaussian hotspots on the (nx, ny) grid (unnormalised)."""
+    parts, w = hotspots(rng, b, gamma_k, **kw)
     x = (np.arange(nx) - nx // 2) * dx
     y = (np.arange(ny) - ny // 2) * dy
     ed = np.zeros((nx, ny))
@@ -85,3 +99,25 @@ def gaussian_2d(nx, ny, dx, dy, e0=30.0, sx=2.0, sy=2.5, dtype=np.float64):
     out = np.zeros((nx * ny, 4), dtype)
     out[:, 0] = ed.reshape(-1)
     return out
+
+
+def hotspot_ini(lib, params, ev, table, dx, dy, dz, width=0.5, plateau=2.0, sigma=1.5, edmax=50.0, stream=None):
+    """glauber_event's energy density computed on the device into the SoA
+    planes `ev` (a torch tensor of 4 planes described by `params`), from the
+    host-sampled participant table of hotspot_table()."""
+    import ctypes
+    import torch
+    from . import _lib
+    dev = ev.device
+    parts = torch.from_numpy(np.ascontiguousarray(table, dtype=np.float64)).to(dev)
+    n = int(parts.shape[0])
+    nbytes = int(lib.clv_hotspot_scratch_bytes(ctypes.byref(params), n))
+    scratch = torch.empty(nbytes + 256, dtype=torch.uint8, device=dev)
+    base = (scratch.data_ptr() + 255) // 256 * 256
+    if stream is None:
+        stream = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+    _lib.check(lib.clv_hotspot_ini(ctypes.byref(params), ctypes.c_void_p(ev.data_ptr()),
+                                   ctypes.c_void_p(parts.data_ptr()), n, float(dx), float(dy), float(dz), float(width),
+                                   float(plateau), float(sigma), float(edmax), ctypes.c_void_p(base), nbytes, stream),
+               'clv_hotspot_ini')
+    return scratch, parts  # keep alive until the stream has run

@@ -76,6 +76,14 @@ class CLVisc(object):
     def load_ini(self, dat):
         self.ideal.load_ini(dat)
 
+    def optical_glauber_ini(self, system='Au+Au', cent_min=None, cent_max=None, save_binary_collisions=False):
+        """visc.py:151-172: the optical Glauber initial condition into d_ev[1]."""
+        self.ideal.optical_glauber_ini(system, cent_min, cent_max, save_binary_collisions)
+
+    def load_hotspot_event(self, b=8.0, seed=5, edmax=50.0):
+        """The seeded Pb+Pb event of initial.glauber_event, generated on the device."""
+        self.ideal.load_hotspot_event(b, seed, edmax)
+
     def _buffers(self, step, parts, fused=False, edmax=False):
         e, pi = self.ideal.d_ev, self.d_pi
         b = _lib.ClvViscBuffers()

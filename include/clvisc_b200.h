@@ -240,6 +240,38 @@ int clv_batch_advance(const clv_params *p, const clv_batch *b, int first, void *
 /* Resident blocks per SM of the batch stage kernel at block_size threads. */
 int clv_batch_occupancy(const clv_params *p, int block_size, int max_registers, int *blocks_per_sm);
 
+/* ------------------------------------------------------------------------
+ * Initial conditions on the device. */
+
+/* The optical Glauber model's constants: the float values of the
+ * -D KEY=%ff literals glauber.py:79-90 emits from the configuration. */
+typedef struct clv_glauber {
+  float num_of_nucleons, sqrts, ro0, r, eta, si0, impact_parameter, edmax, hwn, eta_flat, eta_gw;
+} clv_glauber;
+
+/* glauber_ini (kernel_glauber.cl:86-102, called by CLVisc.optical_glauber_ini,
+ * visc.py:151-172): ev (4 planes) = (Edmax-scaled two-component energy density
+ * of Woods-Saxon thickness functions times the eta plateau profile, 0, 0, 0). */
+int clv_glauber_ini(const clv_params *p, const clv_glauber *g, void *ev, void *stream);
+/* num_of_binary_collisions (kernel_glauber.cl:104-121, glauber.py:94-103):
+ * out[i*ny + j] = Si0 Ta Tb at (xlow + i dx, ylow + j dy); out has p's precision. */
+int clv_glauber_nbinary(const clv_params *p, const clv_glauber *g, void *out, double xlow, double ylow, double dx,
+                        double dy, int nx, int ny, void *stream);
+
+/* Seeded Monte Carlo Glauber (hotspot) profile, no counterpart in the
+ * reference: parts holds n_parts (x, y, weight) triples in double (device),
+ * sampled on the host. ev (4 planes) = (e, 0, 0, 0) with
+ * e(i, j, k) = sum_p w_p exp(-((x_i - x_p)^2 + (y_j - y_p)^2) / (2 width^2)) h(eta_k)
+ * scaled to a maximum of edmax, x_i = (i - nx/2) dx, eta_k = (k - nz/2) dz,
+ * h = 1 for |eta| <= plateau, exp(-(|eta| - plateau)^2 / (2 sigma_eta^2))
+ * beyond; evaluated in double in participant order (the host construction's
+ * arithmetic). scratch: clv_hotspot_scratch_bytes(p, n_parts) bytes, 256-byte
+ * aligned. */
+size_t clv_hotspot_scratch_bytes(const clv_params *p, int n_parts);
+int clv_hotspot_ini(const clv_params *p, void *ev, const double *parts, int n_parts, double dx, double dy, double dz,
+                    double width, double plateau, double sigma_eta, double edmax, void *scratch,
+                    size_t scratch_bytes, void *stream);
+
 /* Host-boundary layout transposes: (n, w) row-major <-> w planes of ld. */
 int clv_aos_to_soa(const clv_params *p, const void *aos, void *soa, long long n, int w, void *stream);
 int clv_soa_to_aos(const clv_params *p, const void *soa, void *aos, long long n, int w, void *stream);

@@ -878,6 +878,86 @@ template <class real> struct Hypersf {
   }
 };
 
+// ============================================================ kernel_glauber.cl
+// The -D literals of glauber.py:79-90, as floats.
+struct GlauberC {
+  float NumOfNucleons, SQRTS, Ro0, R, Eta, Si0, ImpactParameter, Edmax, Hwn, Eta_flat, Eta_gw;
+};
+// kernel_glauber.cl:10-32
+template <class real> real thickness(const GlauberC& g, real x, real y) {
+  real r, th, f, z, cut, a[10], b[10];
+  const real zk[5] = {-0.9061798f, -0.5386492f, 0.0f, 0.5386493f, 0.9061798f};
+  const real Ak[5] = {0.2369269f, 0.4786287f, 0.5688889f, 0.4786287f, 0.2369269f};
+  th = 0.0f;
+  cut = 5.0f * g.R;
+  for (int j = 0; j != 10; ++j) {
+    a[j] = j * cut / 10.0f;
+    b[j] = (j + 1) * cut / 10.0f;
+    for (int i = 0; i != 5; ++i) {
+      z = (a[j] + b[j]) / 2.0f + (b[j] - a[j]) / 2.0f * zk[i];
+      r = std::sqrt(x * x + y * y + z * z);
+      f = g.Ro0 / (1.0f + std::exp((r - g.R) / g.Eta));
+      th = th + Ak[i] * f * (b[j] - a[j]) / 2.0f;
+    }
+  }
+  return 2.0f * th;
+}
+// kernel_glauber.cl:75-83
+template <class real> real Nw(const GlauberC& g, real Ta, real Tb) {
+  return Ta * (1.0f - std::pow(1.0f - g.Si0 * Tb / g.NumOfNucleons, (real)g.NumOfNucleons)) +
+         Tb * (1.0f - std::pow(1.0f - g.Si0 * Ta / g.NumOfNucleons, (real)g.NumOfNucleons));
+}
+template <class real> real Nb(const GlauberC& g, real Ta, real Tb) { return g.Si0 * Ta * Tb; }
+// kernel_glauber.cl:50-52
+template <class real> real ed_transverse(const GlauberC& g, real Ta, real Tb) {
+  return (g.Hwn * Nw<real>(g, Ta, Tb) + (1.0f - g.Hwn) * Nb<real>(g, Ta, Tb));
+}
+// kernel_glauber.cl:35-47
+template <class real> real weight_along_eta(const GlauberC& g, real z, real etas0_) {
+  real heta;
+  if (std::fabs(z - etas0_) > g.Eta_flat)
+    heta = std::exp(-std::pow(std::fabs(z - etas0_) - g.Eta_flat, (real)2.0f) / (2.0f * g.Eta_gw * g.Eta_gw));
+  else
+    heta = 1.0f;
+  return heta;
+}
+// kernel_glauber.cl:86-102 (etas0() returns 0)
+template <class real> void glauber_ini(const Consts& c, const GlauberC& g, real* ev1) {
+#pragma omp parallel for collapse(2) schedule(static)
+  for (int i = 0; i < c.NX; i++)
+    for (int j = 0; j < c.NY; j++) {
+      real x = (i - c.NX / 2) * (real)c.DX;
+      real y = (j - c.NY / 2) * (real)c.DY;
+      real Tcent = thickness<real>(g, 0.0f, 0.0f);
+      real ed_central = ed_transverse<real>(g, Tcent, Tcent);
+      real kFactor = g.Edmax / ed_central;
+      real b = g.ImpactParameter;
+      real Ta = thickness<real>(g, x - 0.5f * b, y);
+      real Tb = thickness<real>(g, x + 0.5f * b, y);
+      real edxy = kFactor * ed_transverse<real>(g, Ta, Tb);
+      real etas0_ = 0.0f;
+      for (int k = 0; k < c.NZ; k++) {
+        real etas = (k - c.NZ / 2) * (real)c.DZ;
+        real heta = weight_along_eta<real>(g, etas, etas0_);
+        st4(ev1, ((size_t)i * c.NY + j) * c.NZ + k, V4<real>{edxy * heta, 0.0f, 0.0f, 0.0f});
+      }
+    }
+}
+// kernel_glauber.cl:104-121
+template <class real> void glauber_nbinary(const GlauberC& g, real* out, real xlow, real ylow, real dx, real dy,
+                                           int nx, int ny) {
+#pragma omp parallel for collapse(2) schedule(static)
+  for (int i = 0; i < nx; i++)
+    for (int j = 0; j < ny; j++) {
+      real x = xlow + i * dx;
+      real y = ylow + j * dy;
+      real b = g.ImpactParameter;
+      real Ta = thickness<real>(g, x - 0.5f * b, y);
+      real Tb = thickness<real>(g, x + 0.5f * b, y);
+      out[(size_t)i * ny + j] = Nb<real>(g, Ta, Tb);
+    }
+}
+
 }  // namespace clvo
 
 // ================================================================= C ABI
@@ -962,6 +1042,18 @@ extern "C" {
 
 DEF(float, f32)
 DEF(double, f64)
+
+#define DEFG(real, sfx)                                                                                  \
+  void clvo_glauber_ini_##sfx(const Consts* c, const clvo::GlauberC* g, real* ev1) {                     \
+    clvo::glauber_ini<real>(*c, *g, ev1);                                                                \
+  }                                                                                                      \
+  void clvo_glauber_nbinary_##sfx(const clvo::GlauberC* g, real* out, real xlow, real ylow, real dx, real dy, \
+                                  int nx, int ny) {                                                     \
+    clvo::glauber_nbinary<real>(*g, out, xlow, ylow, dx, dy, nx, ny);                                   \
+  }                                                                                                      \
+  real clvo_thickness_##sfx(const clvo::GlauberC* g, real x, real y) { return clvo::thickness<real>(*g, x, y); }
+DEFG(float, f32)
+DEFG(double, f64)
 
 int clvo_abi_version(void) { return 2; }
 }

@@ -39,6 +39,56 @@ class Consts(ctypes.Structure):
     ]
 
 
+class GlauberC(ctypes.Structure):  # the -D literals of glauber.py:79-90
+    _fields_ = [(n, ctypes.c_float) for n in ('NumOfNucleons', 'SQRTS', 'Ro0', 'R', 'Eta', 'Si0', 'ImpactParameter',
+                                                'Edmax', 'Hwn', 'Eta_flat', 'Eta_gw')]
+
+
+def glauber_consts(cfg):
+    """Constants as glauber.py emits them: '-D KEY=%ff' of each entry."""
+    from clvisc_b200.config import float_literal as fl
+    g = GlauberC()
+    for field, key in (('NumOfNucleons', 'NumOfNucleons'), ('SQRTS', 'SQRTS'), ('Ro0', 'NucleonDensity'),
+                       ('R', 'Ra'), ('Eta', 'Eta'), ('Si0', 'Si0'), ('ImpactParameter', 'ImpactParameter'),
+                       ('Edmax', 'Edmax'), ('Hwn', 'Hwn'), ('Eta_flat', 'Eta_flat'), ('Eta_gw', 'Eta_gw')):
+        setattr(g, field, fl('%f' % float(getattr(cfg, key))))
+    return g
+
+
+def glauber_ini(cfg, consts=None):
+    """kernel_glauber.cl glauber_ini on the CPU: (cells, 4) array."""
+    lib = load()
+    from clvisc_b200.config import set_real
+    set_real(cfg)
+    real = cfg.real
+    if consts is None:
+        consts = make_consts(cfg, {'ed_start': 0, 'ed_step': 1, 'num_of_ed': 1, 'nrow': 1, 'ncol': 1}, None, 0.0)
+    ev = np.zeros((cfg.NX * cfg.NY * cfg.NZ, 4), real)
+    g = glauber_consts(cfg)
+    f = lib.clvo_glauber_ini_f32 if real == np.float32 else lib.clvo_glauber_ini_f64
+    f(ctypes.byref(consts), ctypes.byref(g), _p(ev))
+    return ev
+
+
+def glauber_nbinary(cfg, xlow=-9.75, ylow=-9.75, dx=0.3, dy=0.3, nx=66, ny=66):
+    lib = load()
+    real = np.float32 if cfg.use_float32 else np.float64
+    R = ctypes.c_float if real == np.float32 else ctypes.c_double
+    out = np.zeros(nx * ny, real)
+    f = lib.clvo_glauber_nbinary_f32 if real == np.float32 else lib.clvo_glauber_nbinary_f64
+    f(ctypes.byref(glauber_consts(cfg)), _p(out), R(real(xlow)), R(real(ylow)), R(real(dx)), R(real(dy)),
+      ctypes.c_int(nx), ctypes.c_int(ny))
+    return out
+
+
+def thickness(cfg, x, y, use_float32=False):
+    lib = load()
+    f = lib.clvo_thickness_f32 if use_float32 else lib.clvo_thickness_f64
+    R = ctypes.c_float if use_float32 else ctypes.c_double
+    f.restype = R
+    return f(ctypes.byref(glauber_consts(cfg)), R(x), R(y))
+
+
 _lib = None
 
 

@@ -12,6 +12,10 @@ What it records (all into golden.npz / golden.json):
     (Eos.eos_func_from_interp1d, eos.py:78-100) applied to the regenerated
     s95p-PCE165 (e, p, s, T) grid, sampled at the same kind of indices, and its
     f_ed(0.137);
+  * weight_mean_b: the reference's pyvisc/glauber.py weight_mean_b() for the
+    centrality classes its own __main__ lists (glauber.py:106-123), Au+Au and
+    Pb+Pb (glauber.py is imported with its pyopencl import stubbed: the
+    function itself is numpy/scipy);
   * kat: the known-answer vectors the reference's tests hold for this path
     (pyvisc/tests/test_kernel_helper.py:29-54, test_reduction.py:15-53,
     test_hypersf.py:26-59, test_bjorken.py:31-62).
@@ -33,6 +37,18 @@ sys.path.insert(0, ROOT)
 def load_ref_eos(refroot):
     path = os.path.join(refroot, 'pyvisc', 'eos', 'eos.py')
     spec = importlib.util.spec_from_file_location('ref_eos', path)
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def load_ref_glauber(refroot):
+    import types
+    for name in ('pyopencl', 'pyopencl.array'):
+        sys.modules.setdefault(name, types.ModuleType(name))
+    sys.modules['pyopencl'].array = sys.modules['pyopencl.array']
+    path = os.path.join(refroot, 'pyvisc', 'glauber.py')
+    spec = importlib.util.spec_from_file_location('ref_glauber', path)
     mod = importlib.util.module_from_spec(spec)
     spec.loader.exec_module(mod)
     return mod
@@ -87,6 +103,12 @@ def main(refroot):
                           'decimals': 3, 'law': 'ed/ed0 = (tau/tau0)^(-4/3)'},
     }
     meta['kat'] = kat
+    g = load_ref_glauber(refroot)
+    classes = list(zip([0, 5, 0, 10, 20, 10, 30, 50, 0], [5, 10, 10, 15, 30, 30, 50, 80, 80]))
+    meta['weight_mean_b'] = {'source': 'pyvisc/glauber.py:14-57, classes of glauber.py:106-123',
+                             'classes': classes,
+                             'Au+Au': [float(g.weight_mean_b(a, b, 'Au+Au')) for a, b in classes],
+                             'Pb+Pb': [float(g.weight_mean_b(a, b, 'Pb+Pb')) for a, b in classes]}
     with open(os.path.join(HERE, 'golden.json'), 'w') as f:
         json.dump(meta, f, indent=1, sort_keys=True)
     print('wrote golden.npz, golden.json')
