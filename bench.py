@@ -280,6 +280,7 @@ def run_batch(n_events=BATCH_EVENTS, one_at_a_time=True):
                 'batch_steps': int(steps), 'event_steps': [int(x) for x in loops],
                 'cell_updates_per_s': float(sum(n * n * int(l) for (n, _, _), l in zip(specs, loops)) /
                                             (t_solved - t_solve))})
+    out['nan_values'] = int(sum(np.count_nonzero(np.isnan(g)) for g in finals))
     # end to end from the seeds: participants sampled on the host, the energy
     # density summed on the device (clv_hotspot_ini), evolve, results to host
     del bt
@@ -308,7 +309,6 @@ def run_batch(n_events=BATCH_EVENTS, one_at_a_time=True):
         t1 = time.perf_counter() - t
         for f, g in zip(singles, finals):  # bit patterns, so that NaN equals NaN
             differ += int(np.count_nonzero(f.view(np.uint32) != g.view(np.uint32)))
-        out['nan_values'] = int(sum(np.count_nonzero(np.isnan(g)) for g in finals))
         out['one_at_a_time'] = {'value': n_events / t1 * 3600.0, 'unit': 'events/h', 'seconds': t1,
                                 'api': 'CLVisc(cfg); load_ini; evolve(save_hypersf=False); ev_to_host per event',
                                 'bitwise_equal_to_batch': differ == 0, 'values_differing': differ}
