@@ -100,6 +100,13 @@ _SIGS = {
     'clv_glauber_nbinary': ([_P, _VP, _VP, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                              ctypes.c_int, ctypes.c_int, _VP], ctypes.c_int),
     'clv_hotspot_scratch_bytes': ([_P, ctypes.c_int], ctypes.c_size_t),
+    # bulk-evolution diagnostics
+    'clv_bulk_slices_size': ([_P], ctypes.c_longlong),
+    'clv_bulk_slices': ([_P, _VP, _VP, _VP, _VP], ctypes.c_int),
+    'clv_bulk_sums': ([_P, _VP, _VP, _VP, _VP], ctypes.c_int),
+    'clv_bulk_lab_scratch_bytes': ([], ctypes.c_size_t),
+    'clv_bulk_lab_totals': ([_P, _VP, ctypes.c_double, ctypes.c_double, _VP, _VP, ctypes.c_size_t, _VP],
+                            ctypes.c_int),
     'clv_hotspot_ini': ([_P, _VP, _VP, ctypes.c_int] + [ctypes.c_double] * 7 + [_VP, ctypes.c_size_t, _VP],
                         ctypes.c_int),
 }

@@ -106,6 +106,8 @@ class CLIdeal(object):
 
         self.eos, self.eos_table, meta, self.efrz = load_eos(self.cfg, handcrafted_eos, self.device)
         self.params = self._make_params(meta)
+        from .bulkinfo import BulkInfo
+        self.bulkinfo = BulkInfo(self.cfg, self.lib, self.params, self.eos, self.device)
 
         z = lambda w: torch.zeros((w, self.ld), dtype=self.dtype, device=self.device)
         self.h_ev1 = np.zeros((self.size, 4), self.cfg.real)
@@ -246,7 +248,8 @@ class CLIdeal(object):
         return self.d_hypersf[:n].cpu().numpy(), self.d_sf_txyz[:n].cpu().numpy()
 
     def save(self, save_hypersf=True, save_bulk=False, viscous_on=False):
-        """Write hypersf.dat and sf_txyz.dat (ideal.py:295-315)."""
+        """Write hypersf.dat and sf_txyz.dat, and the bulk diagnostics
+        (ideal.py:295-315)."""
         self.num_of_sf = self.read_num_of_sf()
         if save_hypersf:
             hypersf, sf_txyz = self.hypersf_to_host()
@@ -254,6 +257,8 @@ class CLIdeal(object):
                        header='Tfrz=%.6e ; other rows: dS0, dS1, dS2, dS3, vx, vy, veta, etas' % self.cfg.TFRZ)
             np.savetxt(os.path.join(self.cfg.fPathOut, 'sf_txyz.dat'), sf_txyz, fmt='%.6e',
                        header='(t, x, y, z) the time-space coordinates of hypersf elements')
+        if save_bulk:
+            self.bulkinfo.save(viscous_on=viscous_on)
 
     def update_time(self, loop):
         """tau = TAU0 + (loop+1)*DT in the run precision (ideal.py:317-320)."""
@@ -270,7 +275,9 @@ class CLIdeal(object):
                 is_finished = self.get_hypersf(n, self.cfg.ntskip)
             if is_finished and not to_maxloop:
                 break
+            if (save_bulk or plot_bulk) and n % self.cfg.ntskip == 0:
+                self.bulkinfo.get(self.tau, self.d_ev[1], self.edmax)
             self.stepUpdate(step=1)
             self.update_time(loop=n)
             self.stepUpdate(step=2, jet_eloss_src=jet_eloss_src)
-        self.save(save_hypersf=save_hypersf, save_bulk=False)
+        self.save(save_hypersf=save_hypersf, save_bulk=save_bulk)

@@ -210,6 +210,8 @@ class CLVisc(object):
             is_finished = self.ideal.edmax < self.ideal.efrz
             if save_hypersf:
                 self.get_hypersf(loop, c.ntskip, is_finished)
+            if (plot_bulk or save_bulk) and loop % c.ntskip == 0:
+                self.ideal.bulkinfo.get(self.ideal.tau, self.ideal.d_ev[1], self.ideal.edmax, self.d_pi[1])
             if is_finished and not force_run_to_maxloop:
                 break
             edmax_pending = ((loop + 1) % c.ntskip == 0)

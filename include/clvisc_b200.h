@@ -272,6 +272,34 @@ int clv_hotspot_ini(const clv_params *p, void *ev, const double *parts, int n_pa
                     double width, double plateau, double sigma_eta, double edmax, void *scratch,
                     size_t scratch_bytes, void *stream);
 
+/* ------------------------------------------------------------------------
+ * Bulk-evolution diagnostics (pyvisc/bulkinfo.py, bulkinfo_h5.py,
+ * kernel_bulkinfo.cl), computed where the state lives. */
+
+/* Elements of the clv_bulk_slices output: ev lines through the grid centre
+ * along x, y, eta (4 NX, 4 NY, 4 NZ), the planes k = NZ/2, j = NY/2, i = NX/2
+ * (4 NX NY, 4 NX NZ, 4 NY NZ), then pi^xx, pi^yy, pi^tx in the transverse
+ * plane (NX NY each), in that order, (w)-interleaved as the reference's real4
+ * buffers. */
+long long clv_bulk_slices_size(const clv_params *p);
+/* get_ed and get_pimn (bulkinfo.py:62-117); pi may be NULL (ideal runs), then
+ * the pi part is not written. The pi index is the reference's
+ * i*NY*(NZ/2) + j*(NZ/2) + NZ/2. out has the precision of p. */
+int clv_bulk_slices(const clv_params *p, const void *ev, const void *pi, void *out, void *stream);
+/* Sums behind the reference's host-side diagnostics (bulkinfo.py:184-271),
+ * in double, reduced per slice in a fixed order: out[3k + 0..2] =
+ * sum over the eta slice k of T^xx, T^yy, T^tx (with veta); out[3 NZ + 0..7]
+ * in the plane k = NZ/2 with veta = 0: T^xx, T^yy, T^tx, u0 e v_r, u0 e,
+ * u0 s, pi^xx + pi^yy, pi^xx - pi^yy (the last two 0 when pi is NULL); with
+ * the reference's floors e >= 1e-10 and v^2 > 1 -> 0.999999. */
+int clv_bulk_sums(const clv_params *p, const void *ev, const void *pi, double *out, void *stream);
+/* total_energy_and_entropy (kernel_bulkinfo.cl:18-45) summed over all cells
+ * and times `volume` (tau DX DY DZ, bulkinfo_h5.py:264-277): out[0] = lab-frame
+ * energy, out[1] = entropy. scratch: clv_bulk_lab_scratch_bytes() bytes. */
+size_t clv_bulk_lab_scratch_bytes(void);
+int clv_bulk_lab_totals(const clv_params *p, const void *ev, double tau, double volume, double *out, void *scratch,
+                        size_t scratch_bytes, void *stream);
+
 /* Host-boundary layout transposes: (n, w) row-major <-> w planes of ld. */
 int clv_aos_to_soa(const clv_params *p, const void *aos, void *soa, long long n, int w, void *stream);
 int clv_soa_to_aos(const clv_params *p, const void *soa, void *aos, long long n, int w, void *stream);
