@@ -100,6 +100,9 @@ _SIGS = {
     'clv_glauber_nbinary': ([_P, _VP, _VP, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                              ctypes.c_int, ctypes.c_int, _VP], ctypes.c_int),
     'clv_hotspot_scratch_bytes': ([_P, ctypes.c_int], ctypes.c_size_t),
+    # Cooper-Frye spectra (clv_spectra_args is passed as a pointer to spectra.SpectraArgs)
+    'clv_spectra_scratch_bytes': ([ctypes.c_longlong, ctypes.c_int, ctypes.c_int, ctypes.c_int], ctypes.c_size_t),
+    'clv_spectra': ([_VP, _VP, _VP, ctypes.c_size_t, _VP], ctypes.c_int),
     # bulk-evolution diagnostics
     'clv_bulk_slices_size': ([_P], ctypes.c_longlong),
     'clv_bulk_slices': ([_P, _VP, _VP, _VP, _VP], ctypes.c_int),

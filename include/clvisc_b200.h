@@ -300,6 +300,28 @@ size_t clv_bulk_lab_scratch_bytes(void);
 int clv_bulk_lab_totals(const clv_params *p, const void *ev, double tau, double volume, double *out, void *scratch,
                         size_t scratch_bytes, void *stream);
 
+/* ------------------------------------------------------------------------
+ * Cooper-Frye smooth spectra of one hadron species on the freeze-out surface:
+ * get_sub_dNdYPtdPtdPhi + get_dNdYPtdPtdPhi (CLSmoothSpec/src/kernel_spec.cl:4-141)
+ * for an ideal surface, kernel_spec_csc.cl:4-101 with the viscous delta f when
+ * pisf is given. All pointers are device pointers in the given precision:
+ * sf = n x 8 (dSigma_0..3, vx, vy, veta, eta_s; the hypersurface buffer of
+ * clv_hypersf_append), pisf = n x 10 or NULL, y/pt/cphi/sphi the grids;
+ * out = ny x npt x nphi spectra, (y, pt, phi) row-major, in GeV fm^3 units as
+ * the reference. Sums are in double in a fixed order. */
+typedef struct clv_spectra_args {
+  int precision;                         /* 4 or 8 */
+  const void *sf, *pisf;                 /* surface elements and their pi^{mu nu} */
+  long long n;                           /* elements */
+  double mass, gspin, fermi_boson, mu;   /* the hadron: +1 baryon (Fermi), -1 (Bose); chemical potential */
+  double tfrz;                           /* freeze-out temperature [GeV] */
+  double tcoeff;                         /* 1 / (2 T^2 (e + P)) on the surface (viscous only) */
+  const void *y, *pt, *cphi, *sphi;      /* rapidities, transverse momenta, cos/sin of the azimuths */
+  int ny, npt, nphi;                     /* npt * nphi <= 1024 */
+} clv_spectra_args;
+size_t clv_spectra_scratch_bytes(long long n, int ny, int npt, int nphi);
+int clv_spectra(const clv_spectra_args *args, void *out, void *scratch, size_t scratch_bytes, void *stream);
+
 /* Host-boundary layout transposes: (n, w) row-major <-> w planes of ld. */
 int clv_aos_to_soa(const clv_params *p, const void *aos, void *soa, long long n, int w, void *stream);
 int clv_soa_to_aos(const clv_params *p, const void *soa, void *aos, long long n, int w, void *stream);

@@ -958,6 +958,56 @@ template <class real> void glauber_nbinary(const GlauberC& g, real* out, real xl
     }
 }
 
+// ===================================================== CLSmoothSpec kernels
+// Cooper-Frye: kernel_spec.cl:4-70 (ideal) and kernel_spec_csc.cl:4-88
+// (viscous delta f, its contraction kept as written), every (y, pt, phi)
+// point summed over the elements in order, in double.
+template <class real, bool VISC>
+void spectra(const real* sf, const real* pisf, long n, double mass_d, double gspin, double fb_d, double mu_d,
+             double tfrz_d, double tcoeff_d, const real* Y, const real* Pt, const real* cphi, const real* sphi,
+             int ny, int npt, int nphi, real* out) {
+  const real mass = (real)mass_d, fb = (real)fb_d, muB = (real)mu_d, tfrz = (real)tfrz_d, tcoeff = (real)tcoeff_d;
+  const double twopi = 2.0 * 3.14159265358979323846;
+  const real dof = (real)(gspin / (twopi * twopi * twopi));
+#pragma omp parallel for collapse(2) schedule(static)
+  for (int k = 0; k < ny; k++)
+    for (int l = 0; l < npt; l++) {
+      const real rapidity = Y[k], pt = Pt[l];
+      const real mt = std::sqrt(mass * mass + pt * pt);
+      for (int m = 0; m < nphi; m++) {
+        const real px = pt * cphi[m], py = pt * sphi[m];
+        double acc = 0.0;
+        for (long e = 0; e < n; e++) {
+          const real* S = sf + 8 * e;
+          const real vx = S[4], vy = S[5], vh = S[6];
+          const real ch = std::cosh(rapidity - S[7]), sh = std::sinh(rapidity - S[7]);
+          const real mtcy = mt * ch, mtsy = mt * sh;
+          if (!VISC) {
+            const real gamma = (real)(1.0 / std::sqrt(cl_max<double>(1.0E-30, 1.0 - vx * vx - vy * vy - vh * vh)));
+            const real efkt = (gamma * (mtcy - px * S[4] - py * S[5] - mtsy * S[6]) - muB) / tfrz;
+            const real volum = mtcy * S[0] - px * S[1] - py * S[2] - mtsy * S[3];
+            acc += (double)(dof * volum / (std::exp(efkt) + fb));
+          } else {
+            const real g = (real)1.0f / std::sqrt(cl_max<real>((real)1.0E-15f, (real)(1.0f - vx * vx - vy * vy - vh * vh)));
+            const real u0 = (real)1.0f * g, u1 = vx * g, u2 = vy * g, u3 = vh * g;
+            const real p0 = mtcy, p1 = -pt * cphi[m], p2 = -pt * sphi[m], p3 = -mtsy;
+            const real pu = p0 * u0 + p1 * u1 + p2 * u2 + p3 * u3;
+            double feq = 1.0 / ((double)std::exp((real)((pu - muB) / tfrz)) + (double)fb);
+            const real* pm = pisf + 10 * e;
+            const real p2pi = tcoeff * (p0 * p0 * pm[0] + p3 * p3 * pm[9] + 2.0f * p0 * (p1 * pm[1] + p2 * pm[2] + p3 * pm[3]) +
+                                        (p1 * p1 * pm[4] + 2 * p1 * p2 * pm[5] + p2 * p2 * pm[7]) +
+                                        2.0f * p3 * (p1 * pm[3] + p2 * pm[6]));
+            const double df = feq * (1.0 - (double)fb * feq) * (double)p2pi;
+            feq += std::fabs(df) > feq ? (df > 0 ? 1.0 : (df < 0 ? -1.0 : 0.0)) * feq * 0.999 : df;
+            const real pdsig = p0 * S[0] + p1 * S[1] + p2 * S[2] + p3 * S[3];
+            acc += (double)dof * (double)pdsig * feq;
+          }
+        }
+        out[((size_t)k * npt + l) * nphi + m] = (real)acc;
+      }
+    }
+}
+
 }  // namespace clvo
 
 // ================================================================= C ABI
@@ -1054,6 +1104,18 @@ DEF(double, f64)
   real clvo_thickness_##sfx(const clvo::GlauberC* g, real x, real y) { return clvo::thickness<real>(*g, x, y); }
 DEFG(float, f32)
 DEFG(double, f64)
+
+#define DEFS(real, sfx)                                                                                          \
+  void clvo_spectra_##sfx(const real* sf, const real* pisf, long n, double mass, double gspin, double fb, double mu, \
+                          double tfrz, double tcoeff, const real* Y, const real* Pt, const real* cphi,          \
+                          const real* sphi, int ny, int npt, int nphi, real* out) {                             \
+    if (pisf)                                                                                                    \
+      clvo::spectra<real, true>(sf, pisf, n, mass, gspin, fb, mu, tfrz, tcoeff, Y, Pt, cphi, sphi, ny, npt, nphi, out); \
+    else                                                                                                         \
+      clvo::spectra<real, false>(sf, pisf, n, mass, gspin, fb, mu, tfrz, tcoeff, Y, Pt, cphi, sphi, ny, npt, nphi, out); \
+  }
+DEFS(float, f32)
+DEFS(double, f64)
 
 int clvo_abi_version(void) { return 2; }
 }

@@ -89,6 +89,23 @@ def thickness(cfg, x, y, use_float32=False):
     return f(ctypes.byref(glauber_consts(cfg)), R(x), R(y))
 
 
+def spectra(sf, pisf, mass, gspin, fb, mu, tfrz, tcoeff, y, pt, phi, use_float32=True):
+    """kernel_spec.cl / kernel_spec_csc.cl on the CPU: (ny, npt, nphi)."""
+    lib = load()
+    real = np.float32 if use_float32 else np.float64
+    sfx = 'f32' if use_float32 else 'f64'
+    a = lambda x: np.ascontiguousarray(x, dtype=real)
+    sf, y, pt = a(sf), a(y), a(pt)
+    cphi, sphi = a(np.cos(phi)), a(np.sin(phi))
+    pis = None if pisf is None else a(pisf)
+    out = np.zeros((len(y), len(pt), len(phi)), real)
+    D = ctypes.c_double
+    getattr(lib, 'clvo_spectra_' + sfx)(_p(sf), _p(pis), ctypes.c_long(sf.shape[0]), D(mass), D(gspin), D(fb), D(mu),
+                                        D(tfrz), D(tcoeff), _p(y), _p(pt), _p(cphi), _p(sphi), ctypes.c_int(len(y)),
+                                        ctypes.c_int(len(pt)), ctypes.c_int(len(phi)), _p(out))
+    return out
+
+
 _lib = None
 
 
