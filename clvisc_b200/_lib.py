@@ -103,6 +103,31 @@ _SIGS = {
     # Cooper-Frye spectra (clv_spectra_args is passed as a pointer to spectra.SpectraArgs)
     'clv_spectra_scratch_bytes': ([ctypes.c_longlong, ctypes.c_int, ctypes.c_int, ctypes.c_int], ctypes.c_size_t),
     'clv_spectra': ([_VP, _VP, _VP, ctypes.c_size_t, _VP], ctypes.c_int),
+    # learned surrogate (clv_unet_conv is passed as a pointer to surrogate.UnetConv)
+    'clv_unet_conv3x3': ([_VP, _VP], ctypes.c_int),
+    'clv_unet_wgrad_scratch_bytes': ([ctypes.c_int] * 5, ctypes.c_size_t),
+    'clv_unet_wgrad3x3': ([_VP, ctypes.c_int, ctypes.c_int, _VP] + [ctypes.c_int] * 5 + [_VP, ctypes.c_int, _VP,
+                          ctypes.c_size_t, _VP], ctypes.c_int),
+    'clv_unet_rows_scratch_bytes': ([ctypes.c_int], ctypes.c_size_t),
+    'clv_unet_bias_grad': ([_VP, ctypes.c_int, ctypes.c_longlong, ctypes.c_int, _VP, _VP, ctypes.c_size_t, _VP],
+                           ctypes.c_int),
+    'clv_unet_first_fwd': ([_VP, _VP, _VP] + [ctypes.c_int] * 4 + [_VP, _VP, ctypes.c_int, ctypes.c_int, _VP],
+                           ctypes.c_int),
+    'clv_unet_first_wgrad': ([_VP, _VP] + [ctypes.c_int] * 4 + [_VP, _VP, ctypes.c_size_t, _VP], ctypes.c_int),
+    'clv_unet_head_fwd': ([_VP, ctypes.c_int, ctypes.c_int, _VP, _VP, ctypes.c_longlong, ctypes.c_int, ctypes.c_int,
+                           _VP, _VP], ctypes.c_int),
+    'clv_unet_head_bwd': ([_VP, ctypes.c_int, ctypes.c_int, _VP, _VP, _VP, ctypes.c_longlong, ctypes.c_int,
+                           ctypes.c_int, _VP, _VP, _VP, ctypes.c_size_t, _VP], ctypes.c_int),
+    'clv_unet_pool': ([_VP, ctypes.c_int, ctypes.c_int] + [ctypes.c_int] * 4 + [_VP, _VP], ctypes.c_int),
+    'clv_unet_up': ([_VP] + [ctypes.c_int] * 4 + [_VP, ctypes.c_int, ctypes.c_int, _VP], ctypes.c_int),
+    'clv_unet_skip_grad': ([_VP, ctypes.c_int, ctypes.c_int, _VP, _VP] + [ctypes.c_int] * 4 + [_VP, _VP],
+                           ctypes.c_int),
+    'clv_unet_up_grad': ([_VP, ctypes.c_int, ctypes.c_int, _VP] + [ctypes.c_int] * 4 + [_VP, _VP], ctypes.c_int),
+    'clv_unet_mse': ([_VP, _VP, _VP, ctypes.c_longlong, ctypes.c_int, ctypes.c_float, _VP, _VP, ctypes.c_int, _VP],
+                     ctypes.c_int),
+    'clv_unet_adam': ([_VP, _VP, _VP, _VP, ctypes.c_longlong, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                       ctypes.c_float, _VP], ctypes.c_int),
+    'clv_unet_pack': ([_VP, ctypes.c_int, ctypes.c_int, _VP, _VP, _VP], ctypes.c_int),
     # bulk-evolution diagnostics
     'clv_bulk_slices_size': ([_P], ctypes.c_longlong),
     'clv_bulk_slices': ([_P, _VP, _VP, _VP, _VP], ctypes.c_int),

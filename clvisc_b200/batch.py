@@ -74,7 +74,7 @@ class CLViscBatch(object):
     """Batched viscous hydro: events of one configuration on their own grids."""
 
     def __init__(self, configs, grids, handcrafted_eos=None, gpu_id=0, max_loops=-1, block_size=None,
-                 grid_blocks=None, max_registers=0):
+                 grid_blocks=None, max_registers=0, stop_at_freezeout=True):
         self.cfg = set_real(configs)
         if not torch.cuda.is_available():
             raise RuntimeError('CLViscBatch needs a CUDA device; there is no CPU path')
@@ -124,6 +124,10 @@ class CLViscBatch(object):
         self.d_prefix = torch.zeros(self.n + 1, dtype=torch.int64, device=dev)
         self.d_loops = torch.full((self.n,), -1, dtype=torch.int32, device=dev)
         self.max_loops = int(max_loops)
+        # without the freeze-out stop every event runs max_loops steps
+        self.stop_at_freezeout = bool(stop_at_freezeout)
+        if not self.stop_at_freezeout and self.max_loops < 0:
+            raise ValueError('stop_at_freezeout=False needs max_loops >= 0')
         self.hist_cap = 0
         self.d_history = torch.zeros(1, dtype=torch.float64, device=dev)
         self.block_size = block_size
@@ -214,7 +218,7 @@ class CLViscBatch(object):
         b.hist_cap = self.hist_cap
         b.tau0 = float(self.cfg.TAU0)
         b.dt = float(self.cfg.DT)
-        b.efrz = float(self.efrz)
+        b.efrz = float(self.efrz) if self.stop_at_freezeout else -1.0e300
         b.ntskip = int(self.cfg.ntskip)
         b.max_loops = self.max_loops
         return b

@@ -1,0 +1,192 @@
+// extern "C" entry points of the learned surrogate's kernels (declared in
+// include/clvisc_b200.h). No counterpart in the reference.
+#include <cstring>
+#include <string>
+
+#include "../../include/clvisc_b200.h"
+#include "clv_unet.cuh"
+
+namespace clv_host {
+int set_error(int code, const std::string& msg);
+int check_cuda(const char* where);
+}  // namespace clv_host
+
+using namespace clv::unet;
+
+namespace {
+inline cudaStream_t S(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+inline unsigned nb(long long n, int bs) { return (unsigned)((n + bs - 1) / bs); }
+inline bool al16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
+static_assert(sizeof(clv_unet_conv) == sizeof(ConvArgs), "clv_unet_conv layout");
+
+// pixel ranges of the weight-gradient split: enough blocks to fill the GPU
+int wgrad_splits(long long P, int Cin, int Cout) {
+  const long long tiles = (long long)((9 * Cin + WG_BM - 1) / WG_BM) * ((Cout + WG_BN - 1) / WG_BN);
+  long long s = (148 * 4 + tiles - 1) / tiles;
+  const long long most = (P + 1023) / 1024;
+  if (s > most) s = most;
+  if (s < 1) s = 1;
+  if (s > 256) s = 256;
+  return (int)s;
+}
+constexpr int kRowBlocks = 148 * 2;
+}  // namespace
+
+extern "C" {
+
+int clv_unet_conv3x3(const clv_unet_conv* args, void* stream) {
+  if (!args) return clv_host::set_error(CLV_ERR_INVALID, "unet_conv3x3: null args");
+  ConvArgs a;
+  memcpy(&a, args, sizeof(a));
+  if (!a.in || !a.w || !a.out || a.N < 1 || a.H < 1 || a.W < 1 || a.Cin % 32 || a.Cout % 32 || a.Cin < 32 ||
+      a.in_cs % 8 || a.in_co % 8 || a.out_cs % 2 || a.out_co % 2 || !al16(a.in) || !al16(a.w) ||
+      (a.gate && (a.gate_cs % 2 || a.gate_co % 2)))
+    return clv_host::set_error(CLV_ERR_INVALID,
+                               "unet_conv3x3: Cin and Cout must be multiples of 32, input strides/offsets of 8, "
+                               "pointers 16-byte aligned");
+  const long long P = (long long)a.N * a.H * a.W;
+  if (a.Cout % 64 == 0) {
+    dim3 grid(nb(P, CONV_BM), a.Cout / 64);
+    conv3x3_kernel<64><<<grid, 256, 0, S(stream)>>>(a);
+  } else {
+    dim3 grid(nb(P, CONV_BM), a.Cout / 32);
+    conv3x3_kernel<32><<<grid, 256, 0, S(stream)>>>(a);
+  }
+  return clv_host::check_cuda("conv3x3_kernel");
+}
+
+size_t clv_unet_wgrad_scratch_bytes(int N, int H, int W, int Cin, int Cout) {
+  const long long P = (long long)N * H * W;
+  return (size_t)wgrad_splits(P, Cin, Cout) * 9 * Cin * Cout * sizeof(float);
+}
+
+int clv_unet_wgrad3x3(const void* x, int x_cs, int x_co, const void* g, int N, int H, int W, int Cin, int Cout,
+                      float* dw, int accumulate, void* scratch, size_t scratch_bytes, void* stream) {
+  if (!x || !g || !dw || !scratch || Cin % 8 || Cout % 8 || x_cs % 8 || x_co % 8 || !al16(x) || !al16(g))
+    return clv_host::set_error(CLV_ERR_INVALID, "unet_wgrad3x3: bad argument");
+  if (scratch_bytes < clv_unet_wgrad_scratch_bytes(N, H, W, Cin, Cout))
+    return clv_host::set_error(CLV_ERR_INVALID, "unet_wgrad3x3: scratch too small");
+  WgradArgs a;
+  a.x = (const bf16*)x;
+  a.x_cs = x_cs;
+  a.x_co = x_co;
+  a.g = (const bf16*)g;
+  a.part = (float*)scratch;
+  a.N = N;
+  a.H = H;
+  a.W = W;
+  a.Cin = Cin;
+  a.Cout = Cout;
+  const long long P = (long long)N * H * W;
+  const int s = wgrad_splits(P, Cin, Cout);
+  a.pix_per_split = (P + s - 1) / s;
+  dim3 grid((9 * Cin + WG_BM - 1) / WG_BM, (Cout + WG_BN - 1) / WG_BN, s);
+  wgrad3x3_kernel<<<grid, 256, 0, S(stream)>>>(a);
+  const long long n = 9LL * Cin * Cout;
+  reduce_partials_kernel<<<nb(n, 256), 256, 0, S(stream)>>>(a.part, s, n, dw, accumulate);
+  return clv_host::check_cuda("wgrad3x3_kernel");
+}
+
+size_t clv_unet_rows_scratch_bytes(int width) { return (size_t)kRowBlocks * width * sizeof(float); }
+
+int clv_unet_bias_grad(const void* g, int g_cs, long long P, int C, float* db, void* scratch, size_t scratch_bytes,
+                       void* stream) {
+  if (!g || !db || !scratch || scratch_bytes < clv_unet_rows_scratch_bytes(C))
+    return clv_host::set_error(CLV_ERR_INVALID, "unet_bias_grad: bad argument");
+  const long long rows = (P + kRowBlocks - 1) / kRowBlocks;
+  colsum_kernel<<<kRowBlocks, 128, 0, S(stream)>>>((const bf16*)g, g_cs, P, C, rows, (float*)scratch);
+  reduce_partials_kernel<<<nb(C, 256), 256, 0, S(stream)>>>((const float*)scratch, kRowBlocks, C, db, 0);
+  return clv_host::check_cuda("colsum_kernel");
+}
+
+int clv_unet_first_fwd(const float* x, const float* w, const float* bias, int N, int H, int W, int C, void* pre,
+                       void* out, int out_cs, int out_co, void* stream) {
+  if (!x || !w || !bias || !pre || !out) return clv_host::set_error(CLV_ERR_INVALID, "unet_first_fwd: null");
+  const long long n = (long long)N * H * W * C;
+  conv_first_kernel<<<nb(n, 256), 256, 0, S(stream)>>>(x, w, bias, N, H, W, C, (bf16*)pre, (bf16*)out, out_cs, out_co);
+  return clv_host::check_cuda("conv_first_kernel");
+}
+
+int clv_unet_first_wgrad(const float* x, const void* g, int N, int H, int W, int C, float* dw, void* scratch,
+                         size_t scratch_bytes, void* stream) {
+  if (!x || !g || !dw || !scratch || scratch_bytes < clv_unet_rows_scratch_bytes(9 * C))
+    return clv_host::set_error(CLV_ERR_INVALID, "unet_first_wgrad: bad argument");
+  const long long P = (long long)N * H * W;
+  const long long rows = (P + kRowBlocks - 1) / kRowBlocks;
+  wgrad_first_kernel<<<kRowBlocks, 288, 0, S(stream)>>>(x, (const bf16*)g, N, H, W, C, rows, (float*)scratch);
+  reduce_partials_kernel<<<nb(9 * C, 256), 256, 0, S(stream)>>>((const float*)scratch, kRowBlocks, 9LL * C, dw, 0);
+  return clv_host::check_cuda("wgrad_first_kernel");
+}
+
+int clv_unet_head_fwd(const void* y, int y_cs, int y_co, const float* w, const float* b, long long P, int C, int K,
+                      float* out, void* stream) {
+  if (!y || !w || !b || !out) return clv_host::set_error(CLV_ERR_INVALID, "unet_head_fwd: null");
+  head_fwd_kernel<<<nb(P * K, 256), 256, 0, S(stream)>>>((const bf16*)y, y_cs, y_co, w, b, P, C, K, out);
+  return clv_host::check_cuda("head_fwd_kernel");
+}
+
+int clv_unet_head_bwd(const void* y, int y_cs, int y_co, const void* z, const float* g, const float* w, long long P,
+                      int C, int K, void* gz, float* dwb, void* scratch, size_t scratch_bytes, void* stream) {
+  if (!y || !z || !g || !w || !gz || !dwb || !scratch || scratch_bytes < clv_unet_rows_scratch_bytes((C + 1) * K))
+    return clv_host::set_error(CLV_ERR_INVALID, "unet_head_bwd: bad argument");
+  head_dgrad_kernel<<<nb(P * C, 256), 256, 0, S(stream)>>>(g, w, (const bf16*)z, P, C, K, (bf16*)gz);
+  const long long rows = (P + kRowBlocks - 1) / kRowBlocks;
+  head_wgrad_kernel<<<kRowBlocks, 224, 0, S(stream)>>>((const bf16*)y, y_cs, y_co, g, P, C, K, rows,
+                                                       (float*)scratch);
+  reduce_partials_kernel<<<nb((C + 1) * K, 256), 256, 0, S(stream)>>>((const float*)scratch, kRowBlocks,
+                                                                       (long long)(C + 1) * K, dwb, 0);
+  return clv_host::check_cuda("head_bwd");
+}
+
+int clv_unet_pool(const void* x, int x_cs, int x_co, int N, int H, int W, int C, void* out, void* stream) {
+  if (!x || !out || H % 2 || W % 2) return clv_host::set_error(CLV_ERR_INVALID, "unet_pool: bad argument");
+  pool_kernel<<<nb((long long)N * (H / 2) * (W / 2) * C, 256), 256, 0, S(stream)>>>((const bf16*)x, x_cs, x_co, N, H,
+                                                                                      W, C, (bf16*)out);
+  return clv_host::check_cuda("pool_kernel");
+}
+
+int clv_unet_up(const void* x, int N, int H, int W, int C, void* out, int out_cs, int out_co, void* stream) {
+  if (!x || !out) return clv_host::set_error(CLV_ERR_INVALID, "unet_up: null");
+  up_kernel<<<nb((long long)N * 4 * H * W * C, 256), 256, 0, S(stream)>>>((const bf16*)x, N, H, W, C, (bf16*)out,
+                                                                          out_cs, out_co);
+  return clv_host::check_cuda("up_kernel");
+}
+
+int clv_unet_skip_grad(const void* gcat, int gcat_cs, int gcat_co, const void* gpool, const void* z, int N, int H,
+                       int W, int C, void* gz, void* stream) {
+  if (!gcat || !z || !gz) return clv_host::set_error(CLV_ERR_INVALID, "unet_skip_grad: null");
+  skip_grad_kernel<<<nb((long long)N * H * W * C, 256), 256, 0, S(stream)>>>(
+      (const bf16*)gcat, gcat_cs, gcat_co, (const bf16*)gpool, (const bf16*)z, N, H, W, C, (bf16*)gz);
+  return clv_host::check_cuda("skip_grad_kernel");
+}
+
+int clv_unet_up_grad(const void* gcat, int gcat_cs, int gcat_co, const void* z, int N, int H, int W, int C, void* gz,
+                     void* stream) {
+  if (!gcat || !z || !gz) return clv_host::set_error(CLV_ERR_INVALID, "unet_up_grad: null");
+  up_grad_kernel<<<nb((long long)N * H * W * C, 256), 256, 0, S(stream)>>>((const bf16*)gcat, gcat_cs, gcat_co,
+                                                                           (const bf16*)z, N, H, W, C, (bf16*)gz);
+  return clv_host::check_cuda("up_grad_kernel");
+}
+
+int clv_unet_mse(const float* out, const float* target, const float* wch, long long P, int K, float scale,
+                 float* grad, float* part, int nparts, void* stream) {
+  if (!out || !target || !wch || !grad || !part || nparts < 1)
+    return clv_host::set_error(CLV_ERR_INVALID, "unet_mse: bad argument");
+  mse_kernel<<<nparts, 256, 0, S(stream)>>>(out, target, wch, P, K, scale, grad, part);
+  return clv_host::check_cuda("mse_kernel");
+}
+
+int clv_unet_adam(float* w, const float* g, float* m, float* v, long long n, float lr_t, float b1, float b2,
+                  float eps, void* stream) {
+  if (!w || !g || !m || !v) return clv_host::set_error(CLV_ERR_INVALID, "unet_adam: null");
+  adam_kernel<<<nb(n, 256), 256, 0, S(stream)>>>(w, g, m, v, n, lr_t, b1, b2, eps);
+  return clv_host::check_cuda("adam_kernel");
+}
+
+int clv_unet_pack(const float* wf, int Cin, int Cout, void* w, void* wt, void* stream) {
+  if (!wf || !w || !wt) return clv_host::set_error(CLV_ERR_INVALID, "unet_pack: null");
+  pack_weights_kernel<<<nb(9LL * Cin * Cout, 256), 256, 0, S(stream)>>>(wf, Cin, Cout, (bf16*)w, (bf16*)wt);
+  return clv_host::check_cuda("pack_weights_kernel");
+}
+
+}  // extern "C"

@@ -322,6 +322,70 @@ typedef struct clv_spectra_args {
 size_t clv_spectra_scratch_bytes(long long n, int ny, int npt, int nphi);
 int clv_spectra(const clv_spectra_args *args, void *out, void *scratch, size_t scratch_bytes, void *stream);
 
+/* ------------------------------------------------------------------------
+ * Learned surrogate (no counterpart in the reference): kernels of a U-Net on
+ * (N, H, W, C) BF16 activations, FP32 accumulation, tensor cores for the 3x3
+ * convolutions. Activations may be channel slices of a wider buffer: element
+ * (p, c) of a slice is ptr[p * stride + offset + c]. */
+
+/* 3x3 convolution with zero padding as an implicit GEMM (mma.sync BF16,
+ * FP32 accumulate): out = act(sum + bias), optionally times gelu'(gate), with
+ * the pre-activation stored in pre ([P][Cout]) when given; act is GELU when
+ * gelu != 0. w: [9][Cin][Cout] BF16 (tap = 3 (dy + 1) + (dx + 1)). The input
+ * gradient of a layer is this call on the output gradient with the weights
+ * clv_unet_pack writes to wt. Cin, Cout multiples of 32. */
+typedef struct clv_unet_conv {
+  const void *in;
+  int in_cs, in_co;
+  const void *w;
+  const float *bias;
+  void *out;
+  int out_cs, out_co;
+  void *pre;
+  const void *gate;
+  int gate_cs, gate_co;
+  int N, H, W, Cin, Cout;
+  int gelu;
+} clv_unet_conv;
+int clv_unet_conv3x3(const clv_unet_conv *args, void *stream);
+/* dw ([9][Cin][Cout] FP32) (+)= sum over pixels of x[p + tap][ci] g[p][co]
+ * (g: gradient wrt the pre-activation, [P][Cout] BF16). */
+size_t clv_unet_wgrad_scratch_bytes(int N, int H, int W, int Cin, int Cout);
+int clv_unet_wgrad3x3(const void *x, int x_cs, int x_co, const void *g, int N, int H, int W, int Cin, int Cout,
+                      float *dw, int accumulate, void *scratch, size_t scratch_bytes, void *stream);
+/* scratch of the row-reduction entry points below for `width` sums */
+size_t clv_unet_rows_scratch_bytes(int width);
+int clv_unet_bias_grad(const void *g, int g_cs, long long P, int C, float *db, void *scratch, size_t scratch_bytes,
+                       void *stream);
+/* first layer: FP32 single-channel image -> C channels (w [9][C], GELU) and its weight gradient */
+int clv_unet_first_fwd(const float *x, const float *w, const float *bias, int N, int H, int W, int C, void *pre,
+                       void *out, int out_cs, int out_co, void *stream);
+int clv_unet_first_wgrad(const float *x, const void *g, int N, int H, int W, int C, float *dw, void *scratch,
+                         size_t scratch_bytes, void *stream);
+/* head: 1x1 convolution C -> K (w [C][K], FP32 output); backward gives the
+ * gradient wrt the input's pre-activation z (times gelu'(z)) and
+ * dwb = [dW (C x K), db (K)] */
+int clv_unet_head_fwd(const void *y, int y_cs, int y_co, const float *w, const float *b, long long P, int C, int K,
+                      float *out, void *stream);
+int clv_unet_head_bwd(const void *y, int y_cs, int y_co, const void *z, const float *g, const float *w, long long P,
+                      int C, int K, void *gz, float *dwb, void *scratch, size_t scratch_bytes, void *stream);
+/* 2x2 average pooling, nearest 2x upsampling, and their gradients through
+ * the GELU that produced the pooled / upsampled activation */
+int clv_unet_pool(const void *x, int x_cs, int x_co, int N, int H, int W, int C, void *out, void *stream);
+int clv_unet_up(const void *x, int N, int H, int W, int C, void *out, int out_cs, int out_co, void *stream);
+int clv_unet_skip_grad(const void *gcat, int gcat_cs, int gcat_co, const void *gpool, const void *z, int N, int H,
+                       int W, int C, void *gz, void *stream);
+int clv_unet_up_grad(const void *gcat, int gcat_cs, int gcat_co, const void *z, int N, int H, int W, int C, void *gz,
+                     void *stream);
+/* weighted squared error: grad = 2 w_k (out - target) scale, part[b] = block sums of w_k (out - target)^2 scale */
+int clv_unet_mse(const float *out, const float *target, const float *wch, long long P, int K, float scale,
+                 float *grad, float *part, int nparts, void *stream);
+/* Adam step on FP32 master weights with the bias-corrected step lr_t */
+int clv_unet_adam(float *w, const float *g, float *m, float *v, long long n, float lr_t, float b1, float b2, float eps,
+                  void *stream);
+/* BF16 weights of a 3x3 layer for the forward (w) and input-gradient (wt) convolutions */
+int clv_unet_pack(const float *wf, int Cin, int Cout, void *w, void *wt, void *stream);
+
 /* Host-boundary layout transposes: (n, w) row-major <-> w planes of ld. */
 int clv_aos_to_soa(const clv_params *p, const void *aos, void *soa, long long n, int w, void *stream);
 int clv_soa_to_aos(const clv_params *p, const void *soa, void *aos, long long n, int w, void *stream);
