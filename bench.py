@@ -401,6 +401,10 @@ def run_gpu(args, rank, world, dist):
             line['cpu_baseline'] = {k: cb[k] for k in ('value', 'unit', 'cores', 'kind', 'sample')}
         if args.batch_events > 0 and world == 1:
             line['batch'] = run_batch(args.batch_events, one_at_a_time=not args.no_one_at_a_time)
+        if args.surrogate_train > 0 and world == 1:
+            from clvisc_b200.surrogate import run_experiment
+            line['surrogate'] = run_experiment(args.surrogate_train, args.surrogate_test, args.surrogate_epochs,
+                                               log=lambda m: print(m, file=sys.stderr, flush=True))
         print(json.dumps(line), flush=True)
 
 
@@ -416,11 +420,25 @@ def main():
                     help='events of the batched workload reported under "batch" (0: skip)')
     ap.add_argument('--no-one-at-a-time', action='store_true', help='skip the one-event-at-a-time comparison')
     ap.add_argument('--batch-only', action='store_true', help='print only the batched workload line')
+    ap.add_argument('--surrogate-train', type=int, default=0,
+                    help='training events of the learned-surrogate experiment reported under "surrogate" (0: skip)')
+    ap.add_argument('--surrogate-test', type=int, default=1000)
+    ap.add_argument('--surrogate-epochs', type=int, default=12)
+    ap.add_argument('--surrogate-only', action='store_true', help='print only the surrogate experiment line')
     ap.add_argument('--grid', type=lambda s: tuple(int(x) for x in s.split(',')), default=(NX, NY, NZ),
                     help='nx,ny,nz (default: the 385,385,115 workload)')
     args = ap.parse_args()
     world = int(os.environ.get('WORLD_SIZE', '1'))
     rank = int(os.environ.get('RANK', '0'))
+    if args.surrogate_only:
+        import torch
+        from clvisc_b200.surrogate import run_experiment
+        torch.cuda.set_device(int(os.environ.get('LOCAL_RANK', 0)))
+        out = run_experiment(args.surrogate_train or 20000, args.surrogate_test, args.surrogate_epochs,
+                             log=lambda m: print(m, file=sys.stderr, flush=True))
+        out['metric'] = 'surrogate events/h at rel. L2 error on e (128x128 (2+1)D events, tau0 + 6.4 fm)'
+        print(json.dumps(out), flush=True)
+        return
     if args.batch_only:
         import torch
         torch.cuda.set_device(int(os.environ.get('LOCAL_RANK', 0)))

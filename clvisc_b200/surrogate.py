@@ -385,3 +385,102 @@ class Surrogate(object):
             o = net.forward()
             out[i0:i0 + m] = (o.view(B, n, n, K_OUT)[:m] * self.out_scale)
         return out
+
+
+def transverse_energy(fields, eos_p, tau, dx):
+    """tau * sum over the slice of T^{tau tau} = (e + P) u0^2 - P, u0^2 = 1 + ux^2 + uy^2."""
+    e = fields[..., 0]
+    P = eos_p(e)
+    u02 = 1.0 + fields[..., 1] ** 2 + fields[..., 2] ** 2
+    return tau * dx * dx * ((e + P) * u02 - P).reshape(e.shape[0], -1).sum(dim=1)
+
+
+def table_pressure(device):
+    """P(e) of the lattice EOS table, linear interpolation on the device."""
+    from .eos import Eos, TABLE_SHAPE
+    table, meta = Eos('lattice_pce165').create_table(*TABLE_SHAPE['lattice_pce165'])
+    p = torch.from_numpy(table.reshape(-1, 4)[:, 1].astype(np.float32)).to(device)
+    e0, de = float(meta['ed_start']), float(meta['ed_step'])
+
+    def P(e):
+        x = torch.clamp((e - e0) / de, 0.0, p.numel() - 1.001)
+        i = x.floor().long()
+        r = x - i
+        return (1.0 - r) * p[i] + r * p[i + 1]
+    return P
+
+
+def run_experiment(n_train=20000, n_test=1000, epochs=12, batch=32, n=128, steps=320, gen_batch=512, lr=2e-3,
+                   residual_max=0.02, log=print):
+    """Generate events with the solver, train the surrogate, and compare it
+    with the solver on held-out events (seeds 10^5 + i for training,
+    9 10^5 + i for testing). Returns a dict of the measured numbers."""
+    dev = torch.device('cuda', 0)
+    res = {'n_train': n_train, 'n_test': n_test, 'grid': n, 'steps': steps, 'epochs': epochs, 'batch': batch}
+    t = time.perf_counter()
+    xtr, ytr = generate_events([100000 + i for i in range(n_train)], n, steps, gen_batch)
+    torch.cuda.synchronize()
+    res['generate_train_s'] = time.perf_counter() - t
+    log('generated %d training events in %.1f s' % (n_train, res['generate_train_s']))
+    # the solver on the test events, timed: initial condition to fields
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    xte, yte = generate_events([900000 + i for i in range(n_test)], n, steps, gen_batch)
+    torch.cuda.synchronize()
+    t_solver = time.perf_counter() - t
+    res['solver_s'] = t_solver
+    res['solver_events_per_h'] = n_test / t_solver * 3600.0
+    log('solver: %d test events in %.2f s' % (n_test, t_solver))
+    sur = Surrogate(batch, n)
+    t = time.perf_counter()
+    hist = sur.train(xtr, ytr, epochs=epochs, lr=lr, log=log)
+    torch.cuda.synchronize()
+    res['train_s'] = time.perf_counter() - t
+    res['loss_history'] = [round(h, 6) for h in hist]
+    # inference, timed
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    pred = sur.predict(xte)
+    torch.cuda.synchronize()
+    t_inf = time.perf_counter() - t
+    err = rel_l2(pred[..., 0], yte[..., 0])
+    # the method without the network: Bjorken cooling of the initial profile
+    tau0, tau1 = 0.6, 0.6 + steps * 0.02
+    base = rel_l2(xte * (tau0 / tau1) ** (4.0 / 3.0), yte[..., 0])
+    # fallback: transverse energy of the prediction against the linear relation
+    # the training events show between initial and final transverse energy
+    Pf = table_pressure(dev)
+    zeros = torch.zeros_like(xtr)
+    et0_tr = transverse_energy(torch.stack([xtr, zeros, zeros], -1), Pf, tau0, 0.16)
+    et1_tr = transverse_energy(ytr, Pf, tau1, 0.16)
+    A = torch.stack([et0_tr, torch.ones_like(et0_tr)], 1).double()
+    coef = torch.linalg.lstsq(A, et1_tr.double()[:, None]).solution[:, 0].float()
+    zt = torch.zeros_like(xte)
+    et_expect = coef[0] * transverse_energy(torch.stack([xte, zt, zt], -1), Pf, tau0, 0.16) + coef[1]
+    resid = (transverse_energy(pred, Pf, tau1, 0.16) - et_expect).abs() / et_expect.abs()
+    rerun = resid > residual_max
+    n_rerun = int(rerun.sum())
+    t_fb = 0.0
+    if n_rerun:
+        idx = torch.nonzero(rerun)[:, 0].cpu().numpy()
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        _, yfb = generate_events([900000 + int(i) for i in idx], n, steps, gen_batch)
+        torch.cuda.synchronize()
+        t_fb = time.perf_counter() - t
+        err = err.clone()
+        err[torch.from_numpy(idx).to(dev)] = rel_l2(yfb[..., 0], yte[torch.from_numpy(idx).to(dev)][..., 0])
+    res.update({
+        'inference_s': t_inf, 'fallback_events': n_rerun, 'fallback_s': t_fb,
+        'surrogate_events_per_h': n_test / (t_inf + t_fb) * 3600.0,
+        'speedup_vs_solver': t_solver / (t_inf + t_fb),
+        'rel_l2_e': {'mean': float(err.mean()), 'median': float(err.median()), 'p90': float(err.quantile(0.9)),
+                     'max': float(err.max()), 'frac_le_2pct': float((err <= 0.02).float().mean())},
+        'rel_l2_e_network_only': {'mean': float(rel_l2(pred[..., 0], yte[..., 0]).mean())},
+        'rel_l2_e_without_network': {'mean': float(base.mean()), 'median': float(base.median())},
+        'rel_l2_other_fields_mean': {f: float(rel_l2(pred[..., k], yte[..., k]).mean())
+                                     for k, f in enumerate(FIELDS) if k > 0},
+    })
+    log('surrogate: mean rel L2 on e %.4f (without network %.4f), %d fallbacks, %.0fx the solver'
+        % (res['rel_l2_e']['mean'], res['rel_l2_e_without_network']['mean'], n_rerun, res['speedup_vs_solver']))
+    return res
