@@ -296,8 +296,9 @@ def surrogate_cfg(n=128, steps=320):
 
 
 def generate_events(seeds, n=128, steps=320, batch=512, edmax=50.0):
-    """Initial energy density (E, n, n) and the solver's fields (E, n, n, 6)
-    after `steps` steps, from the batched solver; on the device, FP32."""
+    """Initial energy density (E, n, n), the solver's fields (E, n, n, 6)
+    after `steps` steps, from the batched solver, on the device in FP32, and a
+    mask of the events whose input and fields are all finite."""
     from .batch import CLViscBatch
     cfg = surrogate_cfg(n, steps)
     xs, ys = [], []
@@ -317,7 +318,9 @@ def generate_events(seeds, n=128, steps=320, batch=512, edmax=50.0):
         xs.append(ev0)
         ys.append(y.reshape(len(chunk), n, n, K_OUT).clone())
         del bt
-    return torch.cat(xs), torch.cat(ys)
+    x, y = torch.cat(xs), torch.cat(ys)
+    ok = torch.isfinite(x).reshape(x.shape[0], -1).all(1) & torch.isfinite(y).reshape(y.shape[0], -1).all(1)
+    return x, y, ok
 
 
 def rel_l2(pred, true):
@@ -339,7 +342,7 @@ class Surrogate(object):
         self.wch = None
 
     def fit_scales(self, y):
-        s = y.reshape(-1, K_OUT).float().std(dim=0)
+        s = y[:min(y.shape[0], 2048)].reshape(-1, K_OUT).double().std(dim=0).float()
         self.out_scale = torch.clamp(s, min=1e-6)
         # the error that matters is on e: weigh it most
         self.wch = torch.tensor([4.0, 1.0, 1.0, 1.0, 1.0, 1.0], device=y.device)
@@ -403,14 +406,15 @@ def table_pressure(device):
     e0, de = float(meta['ed_start']), float(meta['ed_step'])
 
     def P(e):
-        x = torch.clamp((e - e0) / de, 0.0, p.numel() - 1.001)
+        x = torch.nan_to_num((e - e0) / de, nan=0.0, posinf=0.0, neginf=0.0)
+        x = torch.clamp(x, 0.0, p.numel() - 1.001)
         i = x.floor().long()
         r = x - i
         return (1.0 - r) * p[i] + r * p[i + 1]
     return P
 
 
-def run_experiment(n_train=20000, n_test=1000, epochs=12, batch=32, n=128, steps=320, gen_batch=512, lr=2e-3,
+def run_experiment(n_train=20000, n_test=1000, epochs=12, batch=32, n=128, steps=320, gen_batch=1024, lr=2e-3,
                    residual_max=0.02, log=print):
     """Generate events with the solver, train the surrogate, and compare it
     with the solver on held-out events (seeds 10^5 + i for training,
@@ -418,16 +422,22 @@ def run_experiment(n_train=20000, n_test=1000, epochs=12, batch=32, n=128, steps
     dev = torch.device('cuda', 0)
     res = {'n_train': n_train, 'n_test': n_test, 'grid': n, 'steps': steps, 'epochs': epochs, 'batch': batch}
     t = time.perf_counter()
-    xtr, ytr = generate_events([100000 + i for i in range(n_train)], n, steps, gen_batch)
+    xtr, ytr, ok = generate_events([100000 + i for i in range(n_train)], n, steps, gen_batch)
     torch.cuda.synchronize()
     res['generate_train_s'] = time.perf_counter() - t
-    log('generated %d training events in %.1f s' % (n_train, res['generate_train_s']))
+    res['train_events_not_finite'] = int((~ok).sum())
+    xtr, ytr = xtr[ok], ytr[ok]
+    log('generated %d training events in %.1f s (%d not finite, left out)'
+        % (n_train, res['generate_train_s'], res['train_events_not_finite']))
     # the solver on the test events, timed: initial condition to fields
     torch.cuda.synchronize()
     t = time.perf_counter()
-    xte, yte = generate_events([900000 + i for i in range(n_test)], n, steps, gen_batch)
+    xte, yte, okte = generate_events([900000 + i for i in range(n_test)], n, steps, gen_batch)
     torch.cuda.synchronize()
     t_solver = time.perf_counter() - t
+    res['test_events_not_finite'] = int((~okte).sum())
+    test_seeds = torch.arange(n_test, device=dev)[okte]
+    xte, yte = xte[okte], yte[okte]
     res['solver_s'] = t_solver
     res['solver_events_per_h'] = n_test / t_solver * 3600.0
     log('solver: %d test events in %.2f s' % (n_test, t_solver))
@@ -436,6 +446,7 @@ def run_experiment(n_train=20000, n_test=1000, epochs=12, batch=32, n=128, steps
     hist = sur.train(xtr, ytr, epochs=epochs, lr=lr, log=log)
     torch.cuda.synchronize()
     res['train_s'] = time.perf_counter() - t
+    log('trained %d epochs in %.1f s' % (epochs, res['train_s']))
     res['loss_history'] = [round(h, 6) for h in hist]
     # inference, timed
     torch.cuda.synchronize()
@@ -463,16 +474,18 @@ def run_experiment(n_train=20000, n_test=1000, epochs=12, batch=32, n=128, steps
     t_fb = 0.0
     if n_rerun:
         idx = torch.nonzero(rerun)[:, 0].cpu().numpy()
+        seeds = test_seeds[torch.from_numpy(idx).to(dev)].cpu().numpy()
         torch.cuda.synchronize()
         t = time.perf_counter()
-        _, yfb = generate_events([900000 + int(i) for i in idx], n, steps, gen_batch)
+        _, yfb, _ = generate_events([900000 + int(i) for i in seeds], n, steps, gen_batch)
         torch.cuda.synchronize()
         t_fb = time.perf_counter() - t
         err = err.clone()
         err[torch.from_numpy(idx).to(dev)] = rel_l2(yfb[..., 0], yte[torch.from_numpy(idx).to(dev)][..., 0])
+    res['pred_not_finite'] = int((~torch.isfinite(pred)).reshape(pred.shape[0], -1).any(1).sum())
     res.update({
         'inference_s': t_inf, 'fallback_events': n_rerun, 'fallback_s': t_fb,
-        'surrogate_events_per_h': n_test / (t_inf + t_fb) * 3600.0,
+        'surrogate_events_per_h': xte.shape[0] / (t_inf + t_fb) * 3600.0,
         'speedup_vs_solver': t_solver / (t_inf + t_fb),
         'rel_l2_e': {'mean': float(err.mean()), 'median': float(err.median()), 'p90': float(err.quantile(0.9)),
                      'max': float(err.max()), 'frac_le_2pct': float((err <= 0.02).float().mean())},
