@@ -10,7 +10,7 @@ pytestmark = pytest.mark.gpu
 
 def test_surrogate_gains_over_no_network(cuda_lib):
     from clvisc_b200.surrogate import run_experiment
-    r = run_experiment(n_train=512, n_test=64, epochs=10, batch=32, n=64, steps=100, gen_batch=256,
+    r = run_experiment(n_train=512, n_test=64, epochs=10, batch=32, n=64, steps=100, gen_batch=256, lr=2e-3,
                        log=lambda m: None)
     assert r['rel_l2_e_network_only']['mean'] < 0.5 * r['rel_l2_e_without_network']['mean'], r
     assert r['loss_history'][-1] < 0.3 * r['loss_history'][0], r
