@@ -420,10 +420,11 @@ def main():
                     help='events of the batched workload reported under "batch" (0: skip)')
     ap.add_argument('--no-one-at-a-time', action='store_true', help='skip the one-event-at-a-time comparison')
     ap.add_argument('--batch-only', action='store_true', help='print only the batched workload line')
-    ap.add_argument('--surrogate-train', type=int, default=0,
-                    help='training events of the learned-surrogate experiment reported under "surrogate" (0: skip)')
-    ap.add_argument('--surrogate-test', type=int, default=1000)
-    ap.add_argument('--surrogate-epochs', type=int, default=12)
+    ap.add_argument('--surrogate-train', type=int, default=4000,
+                    help='training events of the learned-surrogate experiment reported under "surrogate" (0: skip); '
+                         'the full configuration is 20000 (--surrogate-only)')
+    ap.add_argument('--surrogate-test', type=int, default=500)
+    ap.add_argument('--surrogate-epochs', type=int, default=10)
     ap.add_argument('--surrogate-only', action='store_true', help='print only the surrogate experiment line')
     ap.add_argument('--grid', type=lambda s: tuple(int(x) for x in s.split(',')), default=(NX, NY, NZ),
                     help='nx,ny,nz (default: the 385,385,115 workload)')
@@ -434,7 +435,7 @@ def main():
         import torch
         from clvisc_b200.surrogate import run_experiment
         torch.cuda.set_device(int(os.environ.get('LOCAL_RANK', 0)))
-        out = run_experiment(args.surrogate_train or 20000, args.surrogate_test, args.surrogate_epochs,
+        out = run_experiment(args.surrogate_train, args.surrogate_test, args.surrogate_epochs,
                              log=lambda m: print(m, file=sys.stderr, flush=True))
         out['metric'] = 'surrogate events/h at rel. L2 error on e (128x128 (2+1)D events, tau0 + 6.4 fm)'
         print(json.dumps(out), flush=True)
