@@ -18,6 +18,7 @@ CLV_FLAG_OMEGA_OMEGA_COUPLING = 8
 CLV_FLAG_BULK = 16
 
 CLV_OPT_STAGE_KERNEL = 1
+CLV_OPT_TILE = 4
 CLV_OPT_CHUNK = 2
 CLV_OPT_TILED_BLOCKS = 3
 

@@ -22,6 +22,7 @@ int g_stage_kernel = 0;  // CLV_OPT_STAGE_KERNEL: 0 automatic, 1 per-cell, 2 til
 constexpr int kTiledMinNz = 24;  // fewer cells along eta: per-cell kernel
 int g_chunk = 32;        // CLV_OPT_CHUNK: x planes per tiled CTA
 int g_minb = 2;          // CLV_OPT_TILED_BLOCKS: resident tiled CTAs per SM (FP32)
+int g_tile = 0;          // CLV_OPT_TILE: 0 = 8 x 32, 1 = 16 x 16 (y, eta) tile of the fused stage
 
 int fail(int code, const char* fmt, const char* what = "") {
   char buf[256];
@@ -104,9 +105,8 @@ clv::TauConst<real> tau_const(const clv::Params& p, double tau_d) {
 inline long long ncell(const clv::Params& p) { return (long long)p.nx * p.ny * p.nz; }
 inline unsigned int nblk(long long n, int bs) { return (unsigned int)((n + bs - 1) / bs); }
 
-template <class real, bool IS, bool KT, bool CPL, int MINB>
+template <class real, bool IS, bool KT, bool CPL, int MINB, int TJ = 8, int TK = 32>
 int launch_tiled_b(const clv::Params& p, const clv::ViscBuffers<real>& v, int step, double tau, cudaStream_t s) {
-  constexpr int TJ = 8, TK = 32;
   typedef clv::TileSmem<real, TJ, TK> SM;
   auto kern = clv::visc_stage_tiled_kernel<real, IS, KT, CPL, TJ, TK, MINB>;
   static bool configured = false;
@@ -128,6 +128,11 @@ int launch_tiled(const clv::Params& p, const clv::ViscBuffers<real>& v, int step
   // default kernel does not carry their code
   const bool cpl = IS && (p.flags & (clv::FLAG_GUBSER_VISC | clv::FLAG_PIMN_OMEGA | clv::FLAG_OMEGA_OMEGA));
   if (cpl) return launch_tiled_b<real, IS, KT, IS, 1>(p, v, step, tau, s);
+  // the fused stage also comes with a 16 x 16 (y, eta) tile (CLV_OPT_TILE)
+  if (IS && KT && g_tile == 1) {
+    if (sizeof(real) == 8 || g_minb == 1) return launch_tiled_b<real, IS, KT, false, 1, 16, 16>(p, v, step, tau, s);
+    return launch_tiled_b<real, IS, KT, false, 2, 16, 16>(p, v, step, tau, s);
+  }
   if (sizeof(real) == 8 || g_minb == 1) return launch_tiled_b<real, IS, KT, false, 1>(p, v, step, tau, s);
   return launch_tiled_b<real, IS, KT, false, 2>(p, v, step, tau, s);
 }
@@ -251,6 +256,10 @@ int clv_set_option(int option, int value) {
   }
   if (option == CLV_OPT_TILED_BLOCKS && (value == 1 || value == 2)) {
     g_minb = value;
+    return CLV_OK;
+  }
+  if (option == CLV_OPT_TILE && (value == 0 || value == 1)) {
+    g_tile = value;
     return CLV_OK;
   }
   if (option == CLV_OPT_CHUNK && value >= 1 && value <= 4096) {

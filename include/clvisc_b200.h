@@ -103,6 +103,8 @@ typedef struct clv_visc_buffers {
 #define CLV_OPT_STAGE_KERNEL 1
 #define CLV_OPT_CHUNK 2
 #define CLV_OPT_TILED_BLOCKS 3
+/* (y, eta) tile of the fused tiled stage: 0 = 8 x 32 (default), 1 = 16 x 16 */
+#define CLV_OPT_TILE 4
 int clv_set_option(int option, int value);
 
 /* Library version; the low 8 bits bump on any ABI change. */

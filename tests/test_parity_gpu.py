@@ -93,17 +93,18 @@ def test_visc_parts_parity(cuda_lib, oracle_mod, use_float32, grid, stage_varian
         _compare_visc(v, o, 'parts n=%d' % n)
 
 
-@pytest.fixture(params=['auto', 'tiled', 'tiled-1blk', 'tiled-chunk5', 'per-cell'])
+@pytest.fixture(params=['auto', 'tiled', 'tiled-1blk', 'tiled-chunk5', 'tiled16', 'per-cell'])
 def stage_variant(request, cuda_lib):
     """Every viscous-stage kernel variant; restores the default afterwards."""
     from clvisc_b200 import _lib
     tiled = (_lib.CLV_OPT_STAGE_KERNEL, 2)  # tiled on every grid, short eta axes included
     opts = {'auto': [], 'tiled': [tiled], 'tiled-1blk': [tiled, (_lib.CLV_OPT_TILED_BLOCKS, 1)],
-            'tiled-chunk5': [tiled, (_lib.CLV_OPT_CHUNK, 5)],
+            'tiled-chunk5': [tiled, (_lib.CLV_OPT_CHUNK, 5)], 'tiled16': [tiled, (_lib.CLV_OPT_TILE, 1)],
             'per-cell': [(_lib.CLV_OPT_STAGE_KERNEL, 1)]}[request.param]
     for o, v in opts:
         _lib.set_option(o, v)
     yield request.param
+    _lib.set_option(_lib.CLV_OPT_TILE, 0)
     _lib.set_option(_lib.CLV_OPT_STAGE_KERNEL, 0)
     _lib.set_option(_lib.CLV_OPT_CHUNK, 32)
     _lib.set_option(_lib.CLV_OPT_TILED_BLOCKS, 2)
@@ -234,3 +235,27 @@ def test_visc_gubser_flag_parity(cuda_lib, oracle_mod, use_float32):
         scale = np.abs(w).max(axis=0, keepdims=True) + 1e-30
         err = np.abs(g.astype(np.float64) - w) / scale
         assert err.max() <= rtol, (name, err.max())
+
+
+@pytest.mark.parametrize('use_float32', [True, False])
+def test_autotune_restores_state(cuda_lib, use_float32):
+    """tune_visc times every launch shape on the run's own state and puts it
+    back: the following steps are bit for bit those of an untuned run."""
+    from clvisc_b200.autotune import reset, tune_visc
+    from clvisc_b200.visc import CLVisc
+    cfg = make_cfg(40, 37, 35, use_float32=use_float32)
+    ic = seeded_ic(cfg, seed=9)
+    runs = []
+    for tuned in (False, True):
+        v = CLVisc(cfg)
+        v.load_ini(ic)
+        v.step(0)
+        if tuned:
+            best, table = tune_visc(v, steps=2)
+            assert len(table) >= 5 and min(table.values()) > 0
+        for n in range(1, 4):
+            v.step(n)
+        runs.append((v.ideal.field_to_host(v.ideal.d_ev[1]), v.ideal.field_to_host(v.d_pi[1])))
+    reset()
+    assert_same('ev after tuning', runs[1][0], runs[0][0])
+    assert_same('pi after tuning', runs[1][1], runs[0][1])
