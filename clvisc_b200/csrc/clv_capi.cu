@@ -52,6 +52,7 @@ int to_params(const clv_params* in, clv::Params* out) {
   if ((in->ld * in->precision) % kAlign) return fail(CLV_ERR_INVALID, "ld*precision must be a multiple of 16%s");
   if (10 * in->ld >= (1ll << 40)) return fail(CLV_ERR_INVALID, "grid too large%s");
   if (!in->eos_table || in->eos_nrow < 1 || in->eos_ncol < 1) return fail(CLV_ERR_INVALID, "EOS table missing%s");
+  if (!aligned(in->eos_table)) return fail(CLV_ERR_INVALID, "EOS table must be 16-byte aligned%s");
   if (!(in->eos_ed_step > 0.0f)) return fail(CLV_ERR_INVALID, "eos_ed_step must be > 0%s");
   if (in->nxskip < 1 || in->nyskip < 1 || in->nzskip < 1) return fail(CLV_ERR_INVALID, "skips must be >= 1%s");
   clv::Params& p = *out;

@@ -119,8 +119,12 @@ template <class real> __device__ __forceinline__ real div_step(real x, int step)
 #else
 #define CLV_EOS_ATTR __noinline__
 #endif
-template <class real>
-__device__ CLV_EOS_ATTR real eos_comp(const Params& p, real eps, int c) {
+// the two texels (as texel indices) and the interpolation weight at eps
+template <class real> struct EosSpot {
+  long long t0, t1;
+  real r;
+};
+template <class real> __device__ __forceinline__ EosSpot<real> eos_spot(const Params& p, real eps) {
   const Recips<real>& rc = recips<real>(p);
   real ed_per_row = p.eos_step * p.eos_ncol;
   int row = (int)div_by<real>(eps, ed_per_row, rc.eos_epr);
@@ -133,10 +137,33 @@ __device__ CLV_EOS_ATTR real eos_comp(const Params& p, real eps, int c) {
   }
   int c0 = min(max(col, 0), p.eos_ncol - 1), r0 = min(max(row, 0), p.eos_nrow - 1);
   int c1 = min(max(col2, 0), p.eos_ncol - 1), r1 = min(max(row2, 0), p.eos_nrow - 1);
-  float lo = __ldg(p.eos + 4 * ((long long)r0 * p.eos_ncol + c0) + c);
-  float hi = __ldg(p.eos + 4 * ((long long)r1 * p.eos_ncol + c1) + c);
-  real r = div_by<real>(eps - eps_low, (real)p.eos_step, rc.eos_step);
+  EosSpot<real> s;
+  s.t0 = (long long)r0 * p.eos_ncol + c0;
+  s.t1 = (long long)r1 * p.eos_ncol + c1;
+  s.r = div_by<real>(eps - eps_low, (real)p.eos_step, rc.eos_step);
+  return s;
+}
+template <class real> __device__ __forceinline__ real eos_lerp(real r, float lo, float hi) {
   return (real)(1.0f - r) * (real)lo + r * (real)hi;
+}
+template <class real>
+__device__ CLV_EOS_ATTR real eos_comp(const Params& p, real eps, int c) {
+  const EosSpot<real> s = eos_spot<real>(p, eps);
+  float lo = __ldg(p.eos + 4 * s.t0 + c);
+  float hi = __ldg(p.eos + 4 * s.t1 + c);
+  return eos_lerp<real>(s.r, lo, hi);
+}
+// the four components (cs2, p, T, s) of the table at eps from one pair of
+// 16-byte texel reads; component c equals eos_comp(p, eps, c) bit for bit
+// (the table is 16-byte aligned: the library checks it)
+template <class real> __device__ __forceinline__ void eos_texel4(const Params& p, real eps, real out[4]) {
+  const EosSpot<real> s = eos_spot<real>(p, eps);
+  const float4 lo = __ldg(reinterpret_cast<const float4*>(p.eos) + s.t0);
+  const float4 hi = __ldg(reinterpret_cast<const float4*>(p.eos) + s.t1);
+  out[0] = eos_lerp<real>(s.r, lo.x, hi.x);
+  out[1] = eos_lerp<real>(s.r, lo.y, hi.y);
+  out[2] = eos_lerp<real>(s.r, lo.z, hi.z);
+  out[3] = eos_lerp<real>(s.r, lo.w, hi.w);
 }
 template <class real> __device__ __forceinline__ bool eos_in_table(const Params& p, real eps) {
   return eps < p.eos_start + p.eos_num * p.eos_step;

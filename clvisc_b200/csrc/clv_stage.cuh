@@ -60,21 +60,46 @@ __device__ __forceinline__ Stencil make_stencil(int q, int L, long long stride) 
   return s;
 }
 
-// update_pimn (kernel_IS.cl:501-709) for cell I: e0 and pc are the stage
-// input ev and pi at the cell, grad the velocity gradients, S10 the IS sources
-// (updated in place); writes pi_new and goodcell, returns the new pi in pinew.
-// With BULK, component 10 of pc, S10 and pinew is the bulk pressure Pi.
+// Values of one cell that the Christoffel terms, the pi update and update_ev
+// share, each evaluated once: the stage input ev (d_ev[step]) and d_ev[1] at
+// the cell, with their gamma and table pressure P(e) (no bulk part).
+template <class real> struct CellIn {
+  real e0[4], g0, p0;
+  real e1[4], g1, p1;
+};
+// e0, g0 and p0 set: fills e1, g1, p1. At stage 1 the stencil input is d_ev[1]
+// itself (same buffer), so its values are e0's; otherwise they are read.
+template <class real>
+__device__ __forceinline__ void cell_in_ev1(const Params& p, const ViscBuffers<real>& b, long long I, long long ld,
+                                            CellIn<real>& c) {
+  if (b.ev1 == b.ev_st) {
+#pragma unroll
+    for (int q = 0; q < 4; q++) c.e1[q] = c.e0[q];
+    c.g1 = c.g0;
+    c.p1 = c.p0;
+  } else {
+#pragma unroll
+    for (int q = 0; q < 4; q++) c.e1[q] = b.ev1[q * ld + I];
+    c.g1 = gamma3<real>(c.e1[1], c.e1[2], c.e1[3]);
+    c.p1 = eosP<real>(p, c.e1[0]);
+  }
+}
+
+// update_pimn (kernel_IS.cl:501-709) for cell I: c holds the stage input ev
+// and d_ev[1] at the cell, pc the stage input pi, grad the velocity gradients,
+// S10 the IS sources (updated in place); writes pi_new and goodcell, returns
+// the new pi in pinew. With BULK, component 10 of pc, S10 and pinew is the
+// bulk pressure Pi.
 template <class real, bool COUPLED, bool BULK>
 __device__ __forceinline__ void pi_update(const Params& p, const ViscBuffers<real>& b, int step,
-                                          const TauConst<real>& tc, long long I, long long ld, const real e0[4],
+                                          const TauConst<real>& tc, long long I, long long ld, const CellIn<real>& cin,
                                           const real pc[11], const real grad[3][4], real S10[11], real pinew[11]) {
   const real acu = Acu<real>::v;
   const real tau = tc.tau;
   const Recips<real>& rc = recips<real>(p);
-  real e1[4];
-#pragma unroll
-  for (int c = 0; c < 4; c++) e1[c] = b.ev1[c * ld + I];
-  real g1 = gamma3<real>(e1[1], e1[2], e1[3]);
+  const real* e0 = cin.e0;
+  const real* e1 = cin.e1;
+  real g1 = cin.g1;
   real u_old[4] = {g1 * 1.0f, g1 * e1[1], g1 * e1[2], g1 * e1[3]};
   real u_new[4], udt[4];
   real e2s0;
@@ -87,7 +112,7 @@ __device__ __forceinline__ void pi_update(const Params& p, const ViscBuffers<rea
     }
     e2s0 = b.ev2e[I];
   } else {
-    real g2 = gamma3<real>(e0[1], e0[2], e0[3]);
+    real g2 = cin.g0;
     u_new[0] = g2 * 1.0f;
     u_new[1] = g2 * e0[1];
     u_new[2] = g2 * e0[2];
@@ -111,8 +136,10 @@ __device__ __forceinline__ void pi_update(const Params& p, const ViscBuffers<rea
   for (int c = 0; c < 4; c++) DU[c] = dot4<real>(u, da[c]);
   real ed_step = (step == 1) ? e1[0] : e2s0;
   real theta = udt[0] + grad[0][1] + grad[1][2] + grad[2][3];
-  real temperature = eos_comp<real>(p, ed_step, 2);
-  real sdens = eos_comp<real>(p, ed_step, 3);
+  real tex[4];  // cs2, P, T, s at ed_step
+  eos_texel4<real>(p, ed_step, tex);
+  real temperature = tex[2];
+  real sdens = tex[3];
   real local_etaos = etaos<real>(p, temperature);
   real etav = local_etaos * sdens * CLV_HBARC;
   real one_over_taupi = temperature / (3.0f * cmax<real>(acu, local_etaos) * CLV_HBARC);
@@ -174,7 +201,7 @@ __device__ __forceinline__ void pi_update(const Params& p, const ViscBuffers<rea
     // coupling; |Pi| <= P and Pi = 0 below ZETAOS_TMIN, which keep dilute
     // cells at the edge of a fireball (|pi| >> e, far below freeze-out) from
     // running away.
-    real cs2 = eos_comp<real>(p, ed_step, 0);
+    real cs2 = tex[0];
     real local_zetaos = zetaos<real>(p, temperature);
     real zetav = local_zetaos * sdens * CLV_HBARC;
     real dcs = 1.0f / 3.0f - cs2;
@@ -187,13 +214,13 @@ __device__ __forceinline__ void pi_update(const Params& p, const ViscBuffers<rea
     real b_old = b.pi1[10 * ld + I] * u_old[0];
     b_old = (b_old + div_step(S10[10] * p.DT, step) + p.DT * one_over_taubulk * bulkNS) /
             (u_new[0] + p.DT * one_over_taubulk);
-    const real pb = eosP<real>(p, e2s0);
+    const real pb = (step == 1) ? eosP<real>(p, e2s0) : cin.p0;
     if (b_old < -pb) b_old = -pb;
     else if (b_old > pb) b_old = pb;
     if (temperature < p.ZETAOS_TMIN) b_old = 0.0f;
     pinew[10] = b_old;
   }
-  real pre = eosP<real>(p, e2s0);
+  real pre = (step == 1) ? eosP<real>(p, e2s0) : cin.p0;  // stage 2: e2s0 is e0[0]
   real T00 = (e2s0 + pre) * u_new[0] * u_new[0] - pre;
   uint8_t good = 1;
   constexpr int NPI = BULK ? 11 : 10;
@@ -207,24 +234,22 @@ __device__ __forceinline__ void pi_update(const Params& p, const ViscBuffers<rea
   b.goodcell[I] = good;
 }
 
-// update_ev (kernel_visc.cl:322-393) for cell I: pin = pi^{tau mu} at the
-// start of the step, S4 the KT sources; the new pi^{tau mu} comes from pinew
-// (fused pi update) or from pi_new_in. Also get_udiff and the edmax key.
-// With BULK, pin[4] is Pi at the start of the step and the pressure of the
-// old and the new state is P(e) + Pi.
+// update_ev (kernel_visc.cl:322-393) for cell I: cin holds d_ev[1] at the
+// cell, pin = pi^{tau mu} at the start of the step, S4 the KT sources; the new
+// pi^{tau mu} comes from pinew (fused pi update) or from pi_new_in. Also
+// get_udiff and the edmax key. With BULK, pin[4] is Pi at the start of the
+// step and the pressure of the old and the new state is P(e) + Pi.
 template <class real, bool FUSED_PI, bool BULK>
 __device__ __forceinline__ void ev_update(const Params& p, const ViscBuffers<real>& b, int step,
-                                          const TauConst<real>& tc, long long I, long long ld, const real pin[5],
-                                          const real S4[4], const real pinew[11]) {
+                                          const TauConst<real>& tc, long long I, long long ld, const CellIn<real>& cin,
+                                          const real pin[5], const real S4[4], const real pinew[11]) {
   const real acu = Acu<real>::v;
   const real tau = tc.tau;
-  real e1[4];
-#pragma unroll
-  for (int c = 0; c < 4; c++) e1[c] = b.ev1[c * ld + I];
+  const real* e1 = cin.e1;
   real ed = e1[0], vx = e1[1], vy = e1[2], vz = e1[3];
-  real pressure = eosP<real>(p, ed);
+  real pressure = cin.p1;
   if (BULK) pressure = pressure + pin[4];
-  real u0 = gamma3<real>(vx, vy, vz);
+  real u0 = cin.g1;
   real umu[4] = {u0 * 1.0f, u0 * vx, u0 * vy, u0 * vz};
   real old_time = tau - (step - 1) * p.DT;
   real T0m[4];
@@ -268,7 +293,7 @@ __device__ __forceinline__ void ev_update(const Params& p, const ViscBuffers<rea
   for (int c = 0; c < 4; c++) b.evnew[c * ld + I] = en[c];
   if (b.write_udiff) {  // get_udiff, kernel_IS.cl:714-724
     real gn = gamma3<real>(en[1], en[2], en[3]);
-    real go = gamma3<real>(e1[1], e1[2], e1[3]);
+    real go = cin.g1;
     b.udiff[0 * ld + I] = gn * 1.0f - go * 1.0f;
     b.udiff[1 * ld + I] = gn * en[1] - go * e1[1];
     b.udiff[2 * ld + I] = gn * en[2] - go * e1[2];
@@ -301,9 +326,12 @@ __device__ __forceinline__ void visc_stage_cell(const Params& p, const GridDims 
   const real acu = Acu<real>::v;
 
   // centre cell of the stage input
-  real e0[4];
+  CellIn<real> cin;
+  real* e0 = cin.e0;
 #pragma unroll
   for (int c = 0; c < 4; c++) e0[c] = b.ev_st[c * ld + I];
+  cin.g0 = gamma3<real>(e0[1], e0[2], e0[3]);
+  cin.p0 = eosP<real>(p, e0[0]);
   real pc[11];
 #pragma unroll
   for (int m = 0; m < NPI; m++) pc[m] = b.pi_st[m * ld + I];
@@ -331,7 +359,7 @@ __device__ __forceinline__ void visc_stage_cell(const Params& p, const GridDims 
 
   // Christoffel terms
   if (DO_IS) {  // kernel_IS.cl:56-65
-    real uz = e0[3] * gamma3<real>(e0[1], e0[2], e0[3]);
+    real uz = e0[3] * cin.g0;
     S10[0] -= div_by<real>(2.0f * uz * pc[pidx(0, 3)], tau, tc.rtau);
     S10[1] -= div_by<real>(uz * pc[pidx(1, 3)], tau, tc.rtau);
     S10[2] -= div_by<real>(uz * pc[pidx(2, 3)], tau, tc.rtau);
@@ -342,9 +370,9 @@ __device__ __forceinline__ void visc_stage_cell(const Params& p, const GridDims 
   }
   if (DO_KT) {  // kernel_visc.cl:24-50
     real ed = e0[0], vx = e0[1], vy = e0[2], vz = e0[3];
-    real u0 = gamma3<real>(vx, vy, vz);
+    real u0 = cin.g0;
     real bulkpi = BULK ? pc[10] : (real)0.0f;  // fills the reference's placeholder, kernel_visc.cl:31-33
-    real pressure = eosP<real>(p, ed) + bulkpi;
+    real pressure = cin.p0 + bulkpi;
     real Tzz_tilde = (ed + pressure) * u0 * u0 * vz * vz + pressure + pc[pidx(3, 3)];
     real Ttz_tilde = (ed + pressure) * u0 * u0 * vz + pc[pidx(0, 3)];
     S4[0] = S4[0] - Tzz_tilde;
@@ -379,7 +407,7 @@ __device__ __forceinline__ void visc_stage_cell(const Params& p, const GridDims 
 #pragma unroll
         for (int c = 0; c < 4; c++) grad[a][c] = 0.0f;
         if (a == 2) {
-          const real u0c = gamma3<real>(e0[1], e0[2], e0[3]);
+          const real u0c = cin.g0;
           grad[2][0] = grad[2][0] + div_by<real>(e0[3] * u0c, tau, tc.rtau);
           grad[2][1] = grad[2][1] + div_by<real>((real)0.0f * u0c, tau, tc.rtau);
           grad[2][2] = grad[2][2] + div_by<real>((real)0.0f * u0c, tau, tc.rtau);
@@ -400,7 +428,7 @@ __device__ __forceinline__ void visc_stage_cell(const Params& p, const GridDims 
       for (int c = 0; c < 4; c++) E[d][c] = (d == 2) ? e0[c] : b.ev_st[c * ld + I + st.off[d]];
     real u0[5];
 #pragma unroll
-    for (int d = 0; d < 5; d++) u0[d] = gamma3<real>(E[d][1], E[d][2], E[d][3]);
+    for (int d = 0; d < 5; d++) u0[d] = (d == 2) ? cin.g0 : gamma3<real>(E[d][1], E[d][2], E[d][3]);
 
     // face (i-1/2) uses cells 1,2 and face (i+1/2) cells 2,3 of the stencil
     real vh[2], lam[2];
@@ -419,7 +447,7 @@ __device__ __forceinline__ void visc_stage_cell(const Params& p, const GridDims 
 #pragma unroll
       for (int d = 0; d < 5; d++) {
         const long long J = I + st.off[d];
-        pr[d] = eosP<real>(p, E[d][0]);
+        pr[d] = (d == 2) ? cin.p0 : eosP<real>(p, E[d][0]);
         if (BULK) pr[d] = pr[d] + ((d == 2) ? pc[10] : b.pi_st[10 * ld + J]);
         real A = (E[d][0] + pr[d]) * u0[d];
         real u4[4] = {(real)1.0f * u0[d], E[d][1] * u0[d], E[d][2] * u0[d], E[d][3] * u0[d]};
@@ -519,8 +547,9 @@ __device__ __forceinline__ void visc_stage_cell(const Params& p, const GridDims 
   }
 
   real pinew[11];
-  if (DO_IS) pi_update<real, COUPLED, BULK>(p, b, step, tc, I, ld, e0, pc, grad, S10, pinew);
-  if (DO_KT) ev_update<real, DO_IS, BULK>(p, b, step, tc, I, ld, pin, S4, pinew);
+  cell_in_ev1<real>(p, b, I, ld, cin);
+  if (DO_IS) pi_update<real, COUPLED, BULK>(p, b, step, tc, I, ld, cin, pc, grad, S10, pinew);
+  if (DO_KT) ev_update<real, DO_IS, BULK>(p, b, step, tc, I, ld, cin, pin, S4, pinew);
 
   if (b.write_src) {
     if (DO_KT)

@@ -244,7 +244,14 @@ __global__ void __launch_bounds__(TJ * TK, MINB)
     if (inside && i < p.nx) {
       const long long I = ((long long)i * p.ny + jj) * p.nz + kk;
       const real* Cc = &s.C[0][cself];
-      real e0[4] = {Cc[RF_E * G::NC], Cc[RF_VX * G::NC], Cc[RF_VY * G::NC], Cc[RF_VZ * G::NC]};
+      CellIn<real> cin;  // the record holds gamma and P(e) of the stage input
+      real* e0 = cin.e0;
+      e0[0] = Cc[RF_E * G::NC];
+      e0[1] = Cc[RF_VX * G::NC];
+      e0[2] = Cc[RF_VY * G::NC];
+      e0[3] = Cc[RF_VZ * G::NC];
+      cin.g0 = Cc[RF_U0 * G::NC];
+      cin.p0 = Cc[RF_PR * G::NC];
       real pc[11];  // component 10 (bulk) unused: this kernel has no bulk sector
 #pragma unroll
       for (int m = 0; m < 10; m++) pc[m] = Cc[(RF_PI + m) * G::NC];
@@ -267,7 +274,7 @@ __global__ void __launch_bounds__(TJ * TK, MINB)
         for (int m = 0; m < 10; m++) S10[m] = DO_IS ? b.src[(4 + m) * ld + I] : (real)0.0f;
       }
       if (DO_IS) {  // kernel_IS.cl:56-65
-        real uz = e0[3] * gamma3<real>(e0[1], e0[2], e0[3]);
+        real uz = e0[3] * cin.g0;
         S10[0] -= div_by<real>(2.0f * uz * pc[pidx(0, 3)], tau, tc.rtau);
         S10[1] -= div_by<real>(uz * pc[pidx(1, 3)], tau, tc.rtau);
         S10[2] -= div_by<real>(uz * pc[pidx(2, 3)], tau, tc.rtau);
@@ -278,9 +285,9 @@ __global__ void __launch_bounds__(TJ * TK, MINB)
       }
       if (DO_KT) {  // kernel_visc.cl:24-50
         real ed = e0[0], vx = e0[1], vy = e0[2], vz = e0[3];
-        real u0 = gamma3<real>(vx, vy, vz);
+        real u0 = cin.g0;
         real bulkpi = 0.0f;
-        real pressure = Cc[RF_PR * G::NC] + bulkpi;
+        real pressure = cin.p0 + bulkpi;
         real Tzz_tilde = (ed + pressure) * u0 * u0 * vz * vz + pressure + pc[pidx(3, 3)];
         real Ttz_tilde = (ed + pressure) * u0 * u0 * vz + pc[pidx(0, 3)];
         S4[0] = S4[0] - Tzz_tilde;
@@ -316,6 +323,7 @@ __global__ void __launch_bounds__(TJ * TK, MINB)
       }
 
       real pinew[11];
+      cell_in_ev1<real>(p, b, I, ld, cin);
       if (DO_IS) {
         // velocity gradients, kernel_IS.cl:134-137 / 217-220 / 299-304
         real grad[3][4];
@@ -346,7 +354,7 @@ __global__ void __launch_bounds__(TJ * TK, MINB)
 #pragma unroll
           for (int c = 0; c < 4; c++) umu_prev[c] = umc[c];
         }
-        pi_update<real, COUPLED, false>(p, b, step, tc, I, ld, e0, pc, grad, S10, pinew);
+        pi_update<real, COUPLED, false>(p, b, step, tc, I, ld, cin, pc, grad, S10, pinew);
       } else {
         real u0c = Cc[RF_U0 * G::NC];
         umu_prev[0] = u0c * 1.0f;
@@ -354,7 +362,7 @@ __global__ void __launch_bounds__(TJ * TK, MINB)
         umu_prev[2] = u0c * e0[2];
         umu_prev[3] = u0c * e0[3];
       }
-      if (DO_KT) ev_update<real, DO_IS, false>(p, b, step, tc, I, ld, pin, S4, pinew);
+      if (DO_KT) ev_update<real, DO_IS, false>(p, b, step, tc, I, ld, cin, pin, S4, pinew);
       if (b.write_src) {
         if (DO_KT)
 #pragma unroll

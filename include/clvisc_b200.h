@@ -67,7 +67,7 @@ typedef struct clv_params {
   int nxskip, nyskip, nzskip;
   float eos_ed_start, eos_ed_step;
   int eos_num_ed, eos_nrow, eos_ncol;
-  const float *eos_table; /* device, eos_nrow*eos_ncol texels of (cs2, p, T, s) */
+  const float *eos_table; /* device, 16-byte aligned, eos_nrow*eos_ncol texels of (cs2, p, T, s) */
   int flags;              /* CLV_FLAG_* */
   float zetaos_max, zetaos_t0, zetaos_width, zetaos_skew; /* bulk sector (CLV_FLAG_BULK) */
   float zetaos_tmin;      /* bulk sector: Pi = 0 in cells colder than this */
