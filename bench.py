@@ -234,6 +234,14 @@ def batch_cfg(n=121):
     return set_real(cfg)
 
 
+def launch_name(shape):
+    """'tile<rows-4>x<chunk>/g<grid>' (tiled (2+1)D kernel) or
+    '<block>x<grid>/r<max_registers>' (one thread per cell)."""
+    if shape[0] == 'tile':
+        return 'tile%dx%d/g%d' % (shape[1] - 4, shape[2], shape[3])
+    return '%dx%d/r%d' % shape[1:]
+
+
 def run_batch(n_events=BATCH_EVENTS, one_at_a_time=True):
     """events/h of the batched runner against CLVisc one event at a time."""
     import numpy as np
@@ -257,13 +265,13 @@ def run_batch(n_events=BATCH_EVENTS, one_at_a_time=True):
     t = time.perf_counter()
     tuning = bt.autotune(steps=3)
     out['autotune_s'] = time.perf_counter() - t
-    out['launch'] = {'block': bt.block_size, 'grid': bt.grid_blocks, 'max_registers': bt.max_registers,
-                     'candidates_ms_per_step': {'%dx%d/r%d' % k: round(v, 4) for k, v in sorted(tuning.items())}}
-    shape = (bt.block_size, bt.grid_blocks, bt.max_registers)
+    shape = bt.launch
+    out['launch'] = {'shape': launch_name(shape),
+                     'candidates_ms_per_step': {launch_name(k): round(v, 4) for k, v in sorted(tuning.items())}}
     del bt
     torch.cuda.synchronize()
     t = time.perf_counter()
-    bt = CLViscBatch(cfg, grids, block_size=shape[0], grid_blocks=shape[1], max_registers=shape[2])
+    bt = CLViscBatch(cfg, grids, launch=shape)
     for e, ic in enumerate(ics):
         bt.load_ini(e, ic)
     t_solve = time.perf_counter()
@@ -286,7 +294,7 @@ def run_batch(n_events=BATCH_EVENTS, one_at_a_time=True):
     del bt
     torch.cuda.synchronize()
     t = time.perf_counter()
-    bt = CLViscBatch(cfg, grids, block_size=shape[0], grid_blocks=shape[1], max_registers=shape[2])
+    bt = CLViscBatch(cfg, grids, launch=shape)
     for e, (n, bb, sd) in enumerate(specs):
         bt.load_hotspot_event(e, b=bb, seed=sd, edmax=50.0)
     bt.evolve()

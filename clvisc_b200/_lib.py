@@ -21,6 +21,8 @@ CLV_OPT_STAGE_KERNEL = 1
 CLV_OPT_TILE = 4
 CLV_OPT_CHUNK = 2
 CLV_OPT_TILED_BLOCKS = 3
+CLV_OPT_TILE2D_ROWS = 5
+CLV_OPT_CHUNK2D = 6
 
 
 def set_option(option, value):
@@ -96,6 +98,8 @@ _SIGS = {
     'clv_batch_stage': ([_P, ctypes.c_int, _VP, ctypes.c_int, ctypes.c_int, ctypes.c_int, _VP], ctypes.c_int),
     'clv_batch_advance': ([_P, _VP, ctypes.c_int, _VP], ctypes.c_int),
     'clv_batch_occupancy': ([_P, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
+    'clv_batch_stage_tiled': ([_P, ctypes.c_int, _VP, ctypes.c_int, ctypes.c_int, ctypes.c_int, _VP], ctypes.c_int),
+    'clv_batch_occupancy_tiled': ([_P, ctypes.c_int, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
     # initial conditions (clv_glauber is passed as a pointer to ClvGlauber)
     'clv_glauber_ini': ([_P, _VP, _VP, _VP], ctypes.c_int),
     'clv_glauber_nbinary': ([_P, _VP, _VP, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,

@@ -19,6 +19,11 @@ replays it until every event has stopped.
     b.evolve()
     b.ev_to_host(e), b.pi_to_host(e), b.bulk_to_host(e), b.history(e), b.loops()
 
+The stage kernel is either one thread per cell for any grids
+(clv_batch_stage) or, for batches of (2+1)D events, the tiled kernel
+(clv_batch_stage_tiled: y strips of rows-4 cells marching along x); both give
+the same bits. autotune() times both families over their launch shapes.
+
 Only the viscous path is batched (no Gubser, coupling or Riemann test flags);
 freeze-out surfaces are not extracted.
 """
@@ -74,7 +79,10 @@ class CLViscBatch(object):
     """Batched viscous hydro: events of one configuration on their own grids."""
 
     def __init__(self, configs, grids, handcrafted_eos=None, gpu_id=0, max_loops=-1, block_size=None,
-                 grid_blocks=None, max_registers=0, stop_at_freezeout=True):
+                 grid_blocks=None, max_registers=0, stop_at_freezeout=True, tile=None, launch=None):
+        """launch: a shape from autotune(), ('cell', block, grid, max_registers)
+        or ('tile', rows, chunk, grid), in place of block_size, grid_blocks,
+        max_registers (one thread per cell) or tile = (rows, chunk)."""
         self.cfg = set_real(configs)
         if not torch.cuda.is_available():
             raise RuntimeError('CLViscBatch needs a CUDA device; there is no CPU path')
@@ -133,6 +141,11 @@ class CLViscBatch(object):
         self.block_size = block_size
         self.grid_blocks = grid_blocks
         self.max_registers = int(max_registers)
+        self.tile = None if tile is None else (int(tile[0]), int(tile[1]))
+        if launch is not None:
+            self._set_launch(tuple(launch))
+        if self.tile is not None and not self.all_2d:
+            raise ValueError('the tiled batch kernel takes (2+1)D events (nz = 1) only')
         self.tuning = None
         self._graph = None
         self._h_ctl = torch.zeros(ctypes.sizeof(_Ctl), dtype=torch.uint8).pin_memory()
@@ -223,10 +236,21 @@ class CLViscBatch(object):
         b.max_loops = self.max_loops
         return b
 
-    def _launch_step(self, b, bs, grid, regs):
+    @property
+    def all_2d(self):
+        return all(g[2] == 1 for g in self.grids)
+
+    def _launch_step(self, b, shape):
+        """One fused step (both stages and the stop test) with a launch shape."""
         for step in (1, 2):
-            _lib.check(self.lib.clv_batch_stage(ctypes.byref(self.params), step, ctypes.byref(b), int(bs), int(grid),
-                                                int(regs), self.stream), 'clv_batch_stage')
+            if shape[0] == 'tile':
+                _, rows, chunk, grid = shape
+                _lib.check(self.lib.clv_batch_stage_tiled(ctypes.byref(self.params), step, ctypes.byref(b), int(rows),
+                                                          int(chunk), int(grid), self.stream), 'clv_batch_stage_tiled')
+            else:
+                _, bs, grid, regs = shape
+                _lib.check(self.lib.clv_batch_stage(ctypes.byref(self.params), step, ctypes.byref(b), int(bs),
+                                                    int(grid), int(regs), self.stream), 'clv_batch_stage')
         _lib.check(self.lib.clv_batch_advance(ctypes.byref(self.params), ctypes.byref(b), 0, self.stream),
                    'clv_batch_advance')
 
@@ -238,13 +262,40 @@ class CLViscBatch(object):
                    'clv_batch_occupancy')
         return n.value
 
-    def _launch_shape(self):
+    def occupancy_tiled(self, rows):
+        """Resident tiled stage-kernel blocks per SM at `rows` threads a block."""
+        n = ctypes.c_int()
+        _lib.check(self.lib.clv_batch_occupancy_tiled(ctypes.byref(self.params), int(rows), ctypes.byref(n)),
+                   'clv_batch_occupancy_tiled')
+        return n.value
+
+    def tiles(self, rows, chunk):
+        """Work items of the tiled kernel at a (rows, chunk) shape."""
+        ti = rows - 4
+        return sum(((ny + ti - 1) // ti) * ((nx + chunk - 1) // chunk) for nx, ny, _ in self.grids)
+
+    def _set_launch(self, shape):
+        if shape[0] == 'tile':
+            self.tile = (int(shape[1]), int(shape[2]))
+            self.grid_blocks = shape[3]
+        else:
+            self.tile = None
+            self.block_size, self.grid_blocks, self.max_registers = shape[1], shape[2], int(shape[3])
+
+    @property
+    def launch(self):
+        """The launch shape evolve() uses: ('tile', rows, chunk, grid) or
+        ('cell', block, grid, max_registers)."""
+        sms = torch.cuda.get_device_properties(self.device).multi_processor_count
+        if self.tile is not None:
+            if self.grid_blocks is None:
+                self.grid_blocks = sms * max(1, self.occupancy_tiled(self.tile[0]))
+            return ('tile', self.tile[0], self.tile[1], int(self.grid_blocks))
         if self.block_size is None:
             self.block_size = 128
         if self.grid_blocks is None:
-            sms = torch.cuda.get_device_properties(self.device).multi_processor_count
             self.grid_blocks = sms * max(1, self.occupancy(self.block_size, self.max_registers))
-        return self.block_size, self.grid_blocks, self.max_registers
+        return ('cell', int(self.block_size), int(self.grid_blocks), int(self.max_registers))
 
     # ------------------------------------------------------------- evolve
     def _start(self, hist_cap):
@@ -279,20 +330,24 @@ class CLViscBatch(object):
         if hist_cap is None:
             hist_cap = (self.max_loops // c.ntskip + 2) if self.max_loops >= 0 else 4096
         b = self._start(hist_cap)
-        bs, grid, regs = self._launch_shape()
+        shape = self.launch
         k = int(steps_per_check or c.ntskip)
         if use_graph:
-            key = (bs, grid, regs, k, self.hist_cap, self.d_history.data_ptr())
+            key = (shape, k, self.hist_cap, self.d_history.data_ptr())
             if self._graph is None or self._graph_key != key:
                 self._graph = None
-                self.occupancy(bs, regs)  # loads the stage kernel before the capture
+                # loads the stage kernel (and sets its shared-memory size) before the capture
+                if shape[0] == 'tile':
+                    self.occupancy_tiled(shape[1])
+                else:
+                    self.occupancy(shape[1], shape[3])
                 s = torch.cuda.Stream(self.device)
                 s.wait_stream(torch.cuda.current_stream(self.device))
                 g = torch.cuda.CUDAGraph()
                 with torch.cuda.stream(s):
                     with torch.cuda.graph(g, stream=s):
                         for _ in range(k):
-                            self._launch_step(b, bs, grid, regs)
+                            self._launch_step(b, shape)
                 torch.cuda.current_stream(self.device).wait_stream(s)
                 self._graph, self._graph_key = g, key
             while not self._ctl().done:
@@ -300,7 +355,7 @@ class CLViscBatch(object):
         else:
             while not self._ctl().done:
                 for _ in range(k):
-                    self._launch_step(b, bs, grid, regs)
+                    self._launch_step(b, shape)
         return self._ctl().loop
 
     # ------------------------------------------------------------ results
@@ -349,37 +404,51 @@ class CLViscBatch(object):
             else:
                 getattr(self, n).copy_(v)
 
-    def autotune(self, steps=4, block_sizes=(64, 128, 256)):
-        """Choose the stage kernel's block size, grid and register cap by
-        timing `steps` steps of this batch for each candidate (state restored
-        after each); call after load_ini. Candidates: every block size, each
-        with persistent grids of 1..occupancy blocks per SM and the one-cell-
-        per-thread grid, with and (FP32) without the 128-register cap.
-        Returns {(block, grid, max_registers): ms per step}."""
+    def candidates(self, block_sizes=(64, 128, 256), rows=(64, 128), chunks=(4, 8, 16, 32)):
+        """Launch shapes autotune() times. One thread per cell: every block
+        size with persistent grids of 1..occupancy blocks per SM and the
+        one-cell-per-thread grid, with and (FP32) without the 128-register
+        cap. Tiled ((2+1)D batches only): rows x chunks, each with the grid
+        that fills the GPU once and the one-tile-per-block grid."""
         sms = torch.cuda.get_device_properties(self.device).multi_processor_count
-        hist = self.hist_cap
-        b = self._start(max(hist, steps // self.cfg.ntskip + 2))
-        snap = self._snapshot()
-        results = {}
+        out = []
         total = sum(self.sizes)
         caps = (0, 128) if self.cfg.use_float32 else (0,)
         for regs in caps:
             for bs in block_sizes:
                 occ = max(1, self.occupancy(bs, regs))
-                grids = sorted({sms * k for k in range(1, occ + 1)} | {(total + bs - 1) // bs})
-                for grid in grids:
-                    self._launch_step(b, bs, grid, regs)  # warm-up
-                    torch.cuda.synchronize(self.device)
-                    t0 = torch.cuda.Event(enable_timing=True)
-                    t1 = torch.cuda.Event(enable_timing=True)
-                    t0.record()
-                    for _ in range(steps):
-                        self._launch_step(b, bs, grid, regs)
-                    t1.record()
-                    torch.cuda.synchronize(self.device)
-                    results[(bs, grid, regs)] = t0.elapsed_time(t1) / steps
-                    self._restore(snap)
-        self.block_size, self.grid_blocks, self.max_registers = min(results, key=results.get)
+                for grid in sorted({sms * k for k in range(1, occ + 1)} | {(total + bs - 1) // bs}):
+                    out.append(('cell', bs, grid, regs))
+        if self.all_2d:
+            for r in rows:
+                fill = sms * max(1, self.occupancy_tiled(r))
+                for ch in chunks:
+                    for grid in sorted({fill, self.tiles(r, ch)}):
+                        out.append(('tile', r, ch, grid))
+        return out
+
+    def autotune(self, steps=4, cands=None):
+        """Choose the stage kernel and its launch shape by timing `steps`
+        steps of this batch for each candidate of candidates() (state
+        restored after each); call after load_ini. Returns {shape: ms per
+        step}; the fastest becomes self.launch."""
+        hist = self.hist_cap
+        b = self._start(max(hist, steps // self.cfg.ntskip + 2))
+        snap = self._snapshot()
+        results = {}
+        for shape in (cands or self.candidates()):
+            self._launch_step(b, shape)  # warm-up
+            torch.cuda.synchronize(self.device)
+            t0 = torch.cuda.Event(enable_timing=True)
+            t1 = torch.cuda.Event(enable_timing=True)
+            t0.record()
+            for _ in range(steps):
+                self._launch_step(b, shape)
+            t1.record()
+            torch.cuda.synchronize(self.device)
+            results[shape] = t0.elapsed_time(t1) / steps
+            self._restore(snap)
+        self._set_launch(min(results, key=results.get))
         self.tuning = results
         self._graph = None
         return results

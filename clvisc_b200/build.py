@@ -20,7 +20,8 @@ LIB = os.path.join(HERE, 'libclvisc_b200.so')
 OBJDIR = os.path.join(HERE, '_build')
 SOURCES = ['csrc/clv_capi.cu', 'csrc/clv_noalloc.cu', 'csrc/clv_batch.cu', 'csrc/clv_initial.cu',
            'csrc/clv_bulkinfo.cu', 'csrc/clv_spectra.cu', 'csrc/clv_unet.cu']
-DEPS = ['csrc/clv_device.cuh', 'csrc/clv_stage.cuh', 'csrc/clv_stage_tiled.cuh', 'csrc/clv_misc.cuh',
+DEPS = ['csrc/clv_device.cuh', 'csrc/clv_stage.cuh', 'csrc/clv_stage_tiled.cuh', 'csrc/clv_stage_tiled2d.cuh',
+        'csrc/clv_misc.cuh',
         'csrc/clv_hypersf.cuh', 'csrc/clv_batch.cuh', 'csrc/clv_initial.cuh',
         'csrc/clv_bulkinfo.cuh', 'csrc/clv_spectra.cuh', 'csrc/clv_unet.cuh',
         '../include/clvisc_b200.h']

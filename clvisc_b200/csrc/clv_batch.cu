@@ -106,6 +106,59 @@ int batch_stage_t(const clv_params* pp, int step, const clv_batch* b, int bs, in
   return stage_bs<real, false>(p, a, step, bs, grid, cap, s);
 }
 
+template <class real, bool BULK, int TB>
+int launch_tiled(const clv::Params& p, const clv::BatchArgs<real>& a, int step, int chunk, int grid, cudaStream_t s) {
+  typedef clv::Tile2Smem<real, BULK, TB> SM;
+  auto kern = clv::batch_tiled2d_kernel<real, BULK, TB, clv::tiled2d_minb<real, TB>()>;
+  static bool configured = false;
+  if (!configured) {
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SM)) != cudaSuccess)
+      return clv_host::check_cuda("cudaFuncSetAttribute(batch_tiled2d_kernel)");
+    configured = true;
+  }
+  if (grid <= 0) {
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, TB, sizeof(SM));
+    grid = sms * (per_sm > 0 ? per_sm : 1);
+  }
+  kern<<<grid, TB, sizeof(SM), s>>>(p, a, step, chunk);
+  return clv_host::check_cuda("batch_tiled2d_kernel");
+}
+
+template <class real>
+int batch_stage_tiled_t(const clv_params* pp, int step, const clv_batch* b, int rows, int chunk, int grid,
+                        cudaStream_t s) {
+  clv::Params p;
+  clv::BatchArgs<real> a;
+  int rc = make_args<real>(pp, b, &p, &a);
+  if (rc) return rc;
+  if (step != 1 && step != 2) return clv_host::set_error(CLV_ERR_INVALID, "batch: step must be 1 or 2");
+  if (p.flags & (clv::FLAG_GUBSER_VISC | clv::FLAG_PIMN_OMEGA | clv::FLAG_OMEGA_OMEGA | clv::FLAG_RIEMANN))
+    return clv_host::set_error(CLV_ERR_INVALID, "batch: test flags (Gubser, couplings, Riemann) are not batched");
+  if (chunk < 1 || chunk > 4096) return clv_host::set_error(CLV_ERR_INVALID, "batch: chunk must be in 1..4096");
+  const bool bulk = p.flags & clv::FLAG_BULK;
+  if (rows == 64)
+    return bulk ? launch_tiled<real, true, 64>(p, a, step, chunk, grid, s)
+                : launch_tiled<real, false, 64>(p, a, step, chunk, grid, s);
+  if (rows == 128)
+    return bulk ? launch_tiled<real, true, 128>(p, a, step, chunk, grid, s)
+                : launch_tiled<real, false, 128>(p, a, step, chunk, grid, s);
+  return clv_host::set_error(CLV_ERR_INVALID, "batch: rows must be 64 or 128");
+}
+
+template <class real, bool BULK, int TB> int occupancy_tiled(int* n) {
+  typedef clv::Tile2Smem<real, BULK, TB> SM;
+  auto kern = clv::batch_tiled2d_kernel<real, BULK, TB, clv::tiled2d_minb<real, TB>()>;
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SM)) != cudaSuccess)
+    return clv_host::check_cuda("cudaFuncSetAttribute(batch_tiled2d_kernel)");
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(n, kern, TB, sizeof(SM));
+  if (e != cudaSuccess)
+    return clv_host::set_error(CLV_ERR_CUDA, std::string("batch_occupancy_tiled: ") + cudaGetErrorString(e));
+  return CLV_OK;
+}
+
 template <class real> int batch_advance_t(const clv_params* pp, const clv_batch* b, int first, cudaStream_t s) {
   clv::Params p;
   clv::BatchArgs<real> a;
@@ -130,6 +183,30 @@ int clv_batch_advance(const clv_params* p, const clv_batch* b, int first, void* 
   if (!p) return clv_host::set_error(CLV_ERR_INVALID, "batch: null clv_params");
   if (p->precision == 4) return batch_advance_t<float>(p, b, first, S(stream));
   return batch_advance_t<double>(p, b, first, S(stream));
+}
+
+int clv_batch_stage_tiled(const clv_params* p, int step, const clv_batch* b, int rows, int chunk, int grid_blocks,
+                          void* stream) {
+  if (!p) return clv_host::set_error(CLV_ERR_INVALID, "batch: null clv_params");
+  if (p->precision == 4) return batch_stage_tiled_t<float>(p, step, b, rows, chunk, grid_blocks, S(stream));
+  return batch_stage_tiled_t<double>(p, step, b, rows, chunk, grid_blocks, S(stream));
+}
+
+int clv_batch_occupancy_tiled(const clv_params* p, int rows, int* blocks_per_sm) {
+  if (!p || !blocks_per_sm || (p->precision != 4 && p->precision != 8))
+    return clv_host::set_error(CLV_ERR_INVALID, "batch_occupancy_tiled: bad argument");
+  if (rows != 64 && rows != 128) return clv_host::set_error(CLV_ERR_INVALID, "batch_occupancy_tiled: rows must be 64 or 128");
+  const bool bulk = p->flags & CLV_FLAG_BULK;
+  int n = 0, rc;
+  if (p->precision == 4)
+    rc = rows == 64 ? (bulk ? occupancy_tiled<float, true, 64>(&n) : occupancy_tiled<float, false, 64>(&n))
+                    : (bulk ? occupancy_tiled<float, true, 128>(&n) : occupancy_tiled<float, false, 128>(&n));
+  else
+    rc = rows == 64 ? (bulk ? occupancy_tiled<double, true, 64>(&n) : occupancy_tiled<double, false, 64>(&n))
+                    : (bulk ? occupancy_tiled<double, true, 128>(&n) : occupancy_tiled<double, false, 128>(&n));
+  if (rc) return rc;
+  *blocks_per_sm = n;
+  return CLV_OK;
 }
 
 int clv_batch_occupancy(const clv_params* p, int block_size, int max_registers, int* blocks_per_sm) {

@@ -19,6 +19,7 @@
 // the event stops when it is below the freeze-out energy density.
 #pragma once
 #include "clv_stage.cuh"
+#include "clv_stage_tiled2d.cuh"
 
 namespace clv {
 
@@ -66,6 +67,45 @@ template <class real> __device__ __forceinline__ real batch_tau(double tau0, dou
   return (real)(tau0 + (double)n * dt);
 }
 
+// the stage buffers of event e (its slots of every arena) at stage `step`
+template <class real>
+__device__ __forceinline__ ViscBuffers<real> batch_buffers(const BatchArgs<real>& a, const BatchEvent& E, int e, int step,
+                                                           bool fold) {
+  // slots chosen without indexing the parameter arrays at run time (which
+  // would copy them to local memory)
+  real* const ev_st = step == 1 ? a.ev[1] : a.ev[2];
+  real* const ev_nw = step == 1 ? a.ev[2] : a.ev[1];
+  real* const pi_st = step == 1 ? a.pi[1] : a.pi[2];
+  real* const pi_nw = step == 1 ? a.pi[2] : a.pi[1];
+  ViscBuffers<real> b;
+  b.ev_st = ev_st + E.off_ev;
+  b.pi_st = pi_st + E.off_pi;
+  b.ev1 = a.ev[1] + E.off_ev;
+  b.ev2e = a.ev[2] + E.off_ev;
+  b.pi1 = a.pi[1] + E.off_pi;
+  b.pin = a.pi[1] + E.off_pi;  // fused step: pi at the start of the step is d_pi[1]
+  b.pi2in = pi_nw + E.off_pi;
+  b.evnew = ev_nw + E.off_ev;
+  b.pinew = pi_nw + E.off_pi;
+  b.src = a.src + E.off_src;
+  b.udiff = a.udiff + E.off_ev;
+  b.goodcell = a.goodcell + E.off_cell;
+  b.edmax_key = fold ? a.keys + e : nullptr;
+  b.write_src = step == 1;
+  b.write_udiff = step == 2;
+  return b;
+}
+
+template <class real> __device__ __forceinline__ TauConst<real> batch_tau_const(const Params& p, const BatchArgs<real>& a,
+                                                                               int loop, int step) {
+  TauConst<real> tc;
+  tc.tau = batch_tau<real>(a.tau0, a.dt, step == 1 ? loop : loop + 1);
+  tc.rtau = (real)1 / tc.tau;
+  tc.dzt = (real)p.DZ * tc.tau;
+  tc.rdzt = (real)1 / tc.dzt;
+  return tc;
+}
+
 // MINB > 1 caps the registers so that MINB blocks stay resident per SM
 // (MINB = 512 / BS: at most 128 registers a thread, as the single-event
 // per-cell kernel); MINB = 1 leaves the count to the compiler.
@@ -82,19 +122,9 @@ __global__ void __launch_bounds__(BS, MINB) batch_stage_kernel(Params p, BatchAr
   }
   __syncthreads();
   const int loop = ctl.loop;
-  TauConst<real> tc;
-  tc.tau = batch_tau<real>(a.tau0, a.dt, step == 1 ? loop : loop + 1);
-  tc.rtau = (real)1 / tc.tau;
-  tc.dzt = (real)p.DZ * tc.tau;
-  tc.rdzt = (real)1 / tc.dzt;
+  const TauConst<real> tc = batch_tau_const<real>(p, a, loop, step);
   const bool fold = (step == 2) && ((loop + 1) % a.ntskip == 0);
   const long long total = s_prefix[n];
-  // slots chosen without indexing the parameter arrays at run time (which
-  // would copy them to local memory)
-  real* const ev_st = step == 1 ? a.ev[1] : a.ev[2];
-  real* const ev_nw = step == 1 ? a.ev[2] : a.ev[1];
-  real* const pi_st = step == 1 ? a.pi[1] : a.pi[2];
-  real* const pi_nw = step == 1 ? a.pi[2] : a.pi[1];
   for (long long g = (long long)blockIdx.x * BS + threadIdx.x; g < total; g += (long long)gridDim.x * BS) {
     int lo = 0, hi = n;  // largest slot with prefix <= g
     while (hi - lo > 1) {
@@ -105,23 +135,55 @@ __global__ void __launch_bounds__(BS, MINB) batch_stage_kernel(Params p, BatchAr
     const int e = s_active[lo];
     const BatchEvent E = a.events[e];
     const GridDims gd{E.nx, E.ny, E.nz, E.ld};
-    ViscBuffers<real> b;
-    b.ev_st = ev_st + E.off_ev;
-    b.pi_st = pi_st + E.off_pi;
-    b.ev1 = a.ev[1] + E.off_ev;
-    b.ev2e = a.ev[2] + E.off_ev;
-    b.pi1 = a.pi[1] + E.off_pi;
-    b.pin = a.pi[1] + E.off_pi;  // fused step: pi at the start of the step is d_pi[1]
-    b.pi2in = pi_nw + E.off_pi;
-    b.evnew = ev_nw + E.off_ev;
-    b.pinew = pi_nw + E.off_pi;
-    b.src = a.src + E.off_src;
-    b.udiff = a.udiff + E.off_ev;
-    b.goodcell = a.goodcell + E.off_cell;
-    b.edmax_key = fold ? a.keys + e : nullptr;
-    b.write_src = step == 1;
-    b.write_udiff = step == 2;
+    const ViscBuffers<real> b = batch_buffers<real>(a, E, e, step, fold);
     visc_stage_cell<real, true, true, false, BULK>(p, gd, b, step, tc, g - s_prefix[lo]);
+  }
+}
+
+// The same stage for batches of (2+1)D events (every event NZ = 1) with the
+// tiled kernel of clv_stage_tiled2d.cuh: the work items are tiles of TB-4 rows
+// by `chunk` x planes; a persistent block takes tiles g = blockIdx.x,
+// blockIdx.x + gridDim.x, ... of the running events in order.
+template <class real, bool BULK, int TB, int MINB>
+__global__ void __launch_bounds__(TB, MINB) batch_tiled2d_kernel(Params p, BatchArgs<real> a, int step, int chunk) {
+  __shared__ int s_tprefix[BATCH_MAX_EVENTS + 1];  // the only static shared memory: 4 KB
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Tile2Smem<real, BULK, TB>& sm = *reinterpret_cast<Tile2Smem<real, BULK, TB>*>(smem_raw);
+  const BatchCtl ctl = *a.ctl;
+  if (ctl.done) return;
+  const int n = ctl.n_active;
+  constexpr int TI = TB - 4;  // rows of a tile
+  for (int q = threadIdx.x; q < n; q += TB) {
+    const BatchEvent E = a.events[a.active[q]];
+    s_tprefix[q + 1] = E.nz == 1 ? ((E.ny + TI - 1) / TI) * ((E.nx + chunk - 1) / chunk) : 0;  // its tiles
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {  // prefix of the tile counts (n <= 1024)
+    s_tprefix[0] = 0;
+    for (int q = 0; q < n; q++) s_tprefix[q + 1] += s_tprefix[q];
+  }
+  __syncthreads();
+  const int loop = ctl.loop;
+  const TauConst<real> tc = batch_tau_const<real>(p, a, loop, step);
+  const bool fold = (step == 2) && ((loop + 1) % a.ntskip == 0);
+  const int total = s_tprefix[n];
+  for (int g = blockIdx.x; g < total; g += gridDim.x) {  // block-uniform
+    int lo = 0, hi = n;  // largest slot with prefix <= g
+    while (hi - lo > 1) {
+      int mid = (lo + hi) >> 1;
+      if (s_tprefix[mid] <= g) lo = mid;
+      else hi = mid;
+    }
+    const int e = a.active[lo];
+    const BatchEvent E = a.events[e];
+    const GridDims gd{E.nx, E.ny, E.nz, E.ld};
+    const ViscBuffers<real> b = batch_buffers<real>(a, E, e, step, fold);
+    const int local = g - s_tprefix[lo];
+    const int nty = (E.ny + TI - 1) / TI;
+    const int ty = local % nty, tx = local / nty;
+    const int i0 = tx * chunk;
+    tile2d<real, BULK, TB>(p, gd, b, step, tc, ty * TI, i0, min(i0 + chunk, E.nx), sm);
+    __syncthreads();
   }
 }
 

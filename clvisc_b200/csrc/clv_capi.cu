@@ -10,6 +10,7 @@
 #include "clv_misc.cuh"
 #include "clv_stage.cuh"
 #include "clv_stage_tiled.cuh"
+#include "clv_stage_tiled2d.cuh"
 
 namespace clv_host {
 thread_local std::string g_err;  // message behind clv_last_error()
@@ -18,11 +19,14 @@ using clv_host::g_err;
 
 namespace {
 
-int g_stage_kernel = 0;  // CLV_OPT_STAGE_KERNEL: 0 automatic, 1 per-cell, 2 tiled where it applies
+int g_stage_kernel = 0;  // CLV_OPT_STAGE_KERNEL: 0 automatic, 1 per-cell, 2 tiled (3+1)D, 3 tiled (2+1)D
 constexpr int kTiledMinNz = 24;  // fewer cells along eta: per-cell kernel
+constexpr int kTiled2dMin = 4;   // (2+1)D tiles: at least this many cells along x and y
 int g_chunk = 32;        // CLV_OPT_CHUNK: x planes per tiled CTA
 int g_minb = 2;          // CLV_OPT_TILED_BLOCKS: resident tiled CTAs per SM (FP32)
 int g_tile = 0;          // CLV_OPT_TILE: 0 = 8 x 32, 1 = 16 x 16 (y, eta) tile of the fused stage
+int g_rows2d = 64;       // CLV_OPT_TILE2D_ROWS: threads of a (2+1)D tile block (64 or 128)
+int g_chunk2d = 8;       // CLV_OPT_CHUNK2D: x planes per (2+1)D tile
 
 int fail(int code, const char* fmt, const char* what = "") {
   char buf[256];
@@ -122,6 +126,28 @@ int launch_tiled_b(const clv::Params& p, const clv::ViscBuffers<real>& v, int st
   return cuda_check("visc_stage_tiled_kernel");
 }
 
+template <class real, bool BULK, int TB>
+int launch_tiled2d_b(const clv::Params& p, const clv::ViscBuffers<real>& v, int step, double tau, cudaStream_t s) {
+  typedef clv::Tile2Smem<real, BULK, TB> SM;
+  auto kern = clv::visc_stage_tiled2d_kernel<real, BULK, TB, clv::tiled2d_minb<real, TB>()>;
+  static bool configured = false;
+  if (!configured) {
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SM)) != cudaSuccess)
+      return cuda_check("cudaFuncSetAttribute(visc_stage_tiled2d_kernel)");
+    configured = true;
+  }
+  const int chunk = g_chunk2d;
+  dim3 grid((p.ny + TB - 5) / (TB - 4), (p.nx + chunk - 1) / chunk);
+  kern<<<grid, TB, sizeof(SM), s>>>(p, v, step, tau_const<real>(p, tau), chunk);
+  return cuda_check("visc_stage_tiled2d_kernel");
+}
+
+template <class real, bool BULK>
+int launch_tiled2d(const clv::Params& p, const clv::ViscBuffers<real>& v, int step, double tau, cudaStream_t s) {
+  if (g_rows2d == 128) return launch_tiled2d_b<real, BULK, 128>(p, v, step, tau, s);
+  return launch_tiled2d_b<real, BULK, 64>(p, v, step, tau, s);
+}
+
 template <class real, bool IS, bool KT>
 int launch_tiled(const clv::Params& p, const clv::ViscBuffers<real>& v, int step, double tau, cudaStream_t s) {
   // the coupling terms (GUBSER_VISC_TEST, PIMUNU_OMEGA_COUPLING,
@@ -155,6 +181,12 @@ int visc_stage_t(const clv::Params& p, int step, double tau, int parts, const cl
   if (kt && (!v.evnew || !v.pin || (!is && !v.pi2in))) return fail(CLV_ERR_INVALID, "visc stage: null buffer for update_ev%s");
   if (v.write_udiff && (!kt || !v.udiff)) return fail(CLV_ERR_INVALID, "visc stage: write_udiff needs CLV_PART_KT%s");
   const bool bulk = p.flags & clv::FLAG_BULK;
+  const bool cpl0 = p.flags & (clv::FLAG_GUBSER_VISC | clv::FLAG_PIMN_OMEGA | clv::FLAG_OMEGA_OMEGA);
+  // the tiled (2+1)D kernel (bulk sector, no coupling terms) when asked for:
+  // on B200 the per-cell kernel is faster on the (2+1)D grids of this code
+  const bool fit2d = p.nz == 1 && p.nx >= kTiled2dMin && p.ny >= kTiled2dMin && is && kt && !cpl0;
+  if (fit2d && g_stage_kernel == 3)
+    return bulk ? launch_tiled2d<real, true>(p, v, step, tau, s) : launch_tiled2d<real, false>(p, v, step, tau, s);
   // The tiled kernel has no bulk sector, and its 8 x 32 (y, eta) tile leaves
   // most threads idle on grids with few cells along eta ((2+1)D runs have
   // one): those runs take the per-cell kernel, which gives the same bits.
@@ -246,12 +278,20 @@ int check_cuda(const char* where) { return cuda_check(where); }
 
 extern "C" {
 
-int clv_version(void) { return 0x000103; }
+int clv_version(void) { return 0x000104; }
 const char* clv_last_error(void) { return g_err.c_str(); }
 int clv_alignment(void) { return kAlign; }
 
 int clv_set_option(int option, int value) {
-  if (option == CLV_OPT_STAGE_KERNEL && value >= 0 && value <= 2) {
+  if (option == CLV_OPT_TILE2D_ROWS && (value == 64 || value == 128)) {
+    g_rows2d = value;
+    return CLV_OK;
+  }
+  if (option == CLV_OPT_CHUNK2D && value >= 1 && value <= 4096) {
+    g_chunk2d = value;
+    return CLV_OK;
+  }
+  if (option == CLV_OPT_STAGE_KERNEL && value >= 0 && value <= 3) {
     g_stage_kernel = value;
     return CLV_OK;
   }

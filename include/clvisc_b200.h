@@ -94,17 +94,23 @@ typedef struct clv_visc_buffers {
 } clv_visc_buffers;
 
 /* Tuning options (process-wide): the viscous-stage kernel variant
- * (0 = automatic, the default: the tiled kernel on grids with at least 24
- * cells along eta and no bulk sector, else one thread per cell; 1 = one
- * thread per cell without shared memory; 2 = tiled wherever it applies),
- * the number of x planes a tiled thread block marches through, and the
- * number of tiled blocks kept resident per SM in FP32 (1 or 2; FP64 uses 1).
- * Every variant computes the same values bit for bit. */
+ * (0 = automatic, the default: on grids with at least 24 cells along eta and
+ * no bulk sector the tiled (3+1)D kernel, else one thread per cell; 1 = one
+ * thread per cell without shared memory; 2 = tiled (3+1)D wherever it
+ * applies; 3 = the tiled (2+1)D kernel for the fused stage without coupling
+ * terms on (2+1)D grids (NZ = 1, NX and NY >= 4), else as 0), the number of x planes a tiled (3+1)D thread block
+ * marches through, and the number of tiled blocks kept resident per SM in
+ * FP32 (1 or 2; FP64 uses 1). Every variant computes the same values bit for
+ * bit. */
 #define CLV_OPT_STAGE_KERNEL 1
 #define CLV_OPT_CHUNK 2
 #define CLV_OPT_TILED_BLOCKS 3
 /* (y, eta) tile of the fused tiled stage: 0 = 8 x 32 (default), 1 = 16 x 16 */
 #define CLV_OPT_TILE 4
+/* (2+1)D tiles: threads of a block (64, the default, or 128; a tile is that
+ * many rows minus 4) and x planes per tile (default 8) */
+#define CLV_OPT_TILE2D_ROWS 5
+#define CLV_OPT_CHUNK2D 6
 int clv_set_option(int option, int value);
 
 /* Library version; the low 8 bits bump on any ABI change. */
@@ -241,6 +247,15 @@ int clv_batch_stage(const clv_params *p, int step, const clv_batch *b, int block
 int clv_batch_advance(const clv_params *p, const clv_batch *b, int first, void *stream);
 /* Resident blocks per SM of the batch stage kernel at block_size threads. */
 int clv_batch_occupancy(const clv_params *p, int block_size, int max_registers, int *blocks_per_sm);
+/* The same stage for batches of (2+1)D events with the tiled kernel: work
+ * items are tiles of (rows - 4) y rows by `chunk` x planes (rows = 64 or 128
+ * threads a block), taken in order by grid_blocks persistent blocks
+ * (grid_blocks <= 0: fill the GPU once). Every event must have nz = 1: the
+ * kernel gives events with nz != 1 no tiles. Same bits as clv_batch_stage. */
+int clv_batch_stage_tiled(const clv_params *p, int step, const clv_batch *b, int rows, int chunk, int grid_blocks,
+                          void *stream);
+/* Resident blocks per SM of the tiled batch stage kernel. */
+int clv_batch_occupancy_tiled(const clv_params *p, int rows, int *blocks_per_sm);
 
 /* ------------------------------------------------------------------------
  * Initial conditions on the device. */

@@ -67,11 +67,13 @@ def test_bulk_parts_parity(cuda_lib, oracle_mod, use_float32, grid):
 
 
 @pytest.mark.parametrize('use_float32', [True, False])
-@pytest.mark.parametrize('grid', [(15, 13, 11), (23, 21, 1), (40, 37, 35)])
-@pytest.mark.parametrize('kernel', [0, 1])
+@pytest.mark.parametrize('grid', [(15, 13, 11), (23, 21, 1), (40, 37, 35), (19, 70, 1)])
+@pytest.mark.parametrize('kernel', [0, 1, 3])
 def test_bulk_fused_step_parity(cuda_lib, oracle_mod, use_float32, grid, kernel):
-    """The fused stage of evolve(); with the tiled kernel selected (0) a bulk
-    run takes the per-cell kernel, which must give the same bits."""
+    """The fused stage of evolve(); the tiled (3+1)D kernel has no bulk sector,
+    so with it selected (0) a bulk run takes the per-cell kernel (1); 3 takes
+    the tiled (2+1)D kernel, which has one, on the one-cell eta grids. All
+    give the oracle's bits."""
     from clvisc_b200 import _lib
     _lib.set_option(_lib.CLV_OPT_STAGE_KERNEL, kernel)
     try:

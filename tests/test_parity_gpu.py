@@ -93,14 +93,19 @@ def test_visc_parts_parity(cuda_lib, oracle_mod, use_float32, grid, stage_varian
         _compare_visc(v, o, 'parts n=%d' % n)
 
 
-@pytest.fixture(params=['auto', 'tiled', 'tiled-1blk', 'tiled-chunk5', 'tiled16', 'per-cell'])
+@pytest.fixture(params=['auto', 'tiled', 'tiled-1blk', 'tiled-chunk5', 'tiled16', 'per-cell', 'tiled2d',
+                        'tiled2d-128-c3'])
 def stage_variant(request, cuda_lib):
-    """Every viscous-stage kernel variant; restores the default afterwards."""
+    """Every viscous-stage kernel variant; restores the default afterwards.
+    (tiled2d: the tiled (2+1)D kernel on one-cell eta grids, 64-thread tiles
+    of 8 planes; tiled2d-128-c3: 128-thread tiles of 3 planes.)"""
     from clvisc_b200 import _lib
     tiled = (_lib.CLV_OPT_STAGE_KERNEL, 2)  # tiled on every grid, short eta axes included
     opts = {'auto': [], 'tiled': [tiled], 'tiled-1blk': [tiled, (_lib.CLV_OPT_TILED_BLOCKS, 1)],
             'tiled-chunk5': [tiled, (_lib.CLV_OPT_CHUNK, 5)], 'tiled16': [tiled, (_lib.CLV_OPT_TILE, 1)],
-            'per-cell': [(_lib.CLV_OPT_STAGE_KERNEL, 1)]}[request.param]
+            'per-cell': [(_lib.CLV_OPT_STAGE_KERNEL, 1)], 'tiled2d': [(_lib.CLV_OPT_STAGE_KERNEL, 3)],
+            'tiled2d-128-c3': [(_lib.CLV_OPT_STAGE_KERNEL, 3), (_lib.CLV_OPT_TILE2D_ROWS, 128),
+                               (_lib.CLV_OPT_CHUNK2D, 3)]}[request.param]
     for o, v in opts:
         _lib.set_option(o, v)
     yield request.param
@@ -108,10 +113,12 @@ def stage_variant(request, cuda_lib):
     _lib.set_option(_lib.CLV_OPT_STAGE_KERNEL, 0)
     _lib.set_option(_lib.CLV_OPT_CHUNK, 32)
     _lib.set_option(_lib.CLV_OPT_TILED_BLOCKS, 2)
+    _lib.set_option(_lib.CLV_OPT_TILE2D_ROWS, 64)
+    _lib.set_option(_lib.CLV_OPT_CHUNK2D, 8)
 
 
 @pytest.mark.parametrize('use_float32', [True, False])
-@pytest.mark.parametrize('grid', [(15, 13, 11), (21, 19, 1), (9, 1, 13), (40, 37, 35)])
+@pytest.mark.parametrize('grid', [(15, 13, 11), (21, 19, 1), (9, 1, 13), (40, 37, 35), (23, 131, 1)])
 def test_visc_fused_step_parity(cuda_lib, oracle_mod, use_float32, grid, stage_variant):
     """The fused per-stage kernel of evolve() against the reference order."""
     from clvisc_b200.visc import CLVisc
