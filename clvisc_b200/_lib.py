@@ -110,6 +110,8 @@ _SIGS = {
     'clv_spectra': ([_VP, _VP, _VP, ctypes.c_size_t, _VP], ctypes.c_int),
     # learned surrogate (clv_unet_conv is passed as a pointer to surrogate.UnetConv)
     'clv_unet_conv3x3': ([_VP, _VP], ctypes.c_int),
+    'clv_unet_set_conv_path': ([ctypes.c_int], ctypes.c_int),
+    'clv_unet_timeouts': ([ctypes.POINTER(ctypes.c_int), ctypes.c_int], ctypes.c_int),
     'clv_unet_wgrad_scratch_bytes': ([ctypes.c_int] * 5, ctypes.c_size_t),
     'clv_unet_wgrad3x3': ([_VP, ctypes.c_int, ctypes.c_int, _VP] + [ctypes.c_int] * 5 + [_VP, ctypes.c_int, _VP,
                           ctypes.c_size_t, _VP], ctypes.c_int),

@@ -1,7 +1,10 @@
 // extern "C" entry points of the learned surrogate's kernels (declared in
 // include/clvisc_b200.h). No counterpart in the reference.
+#include <algorithm>
 #include <cstring>
 #include <string>
+
+#include <cudaTypedefs.h>
 
 #include "../../include/clvisc_b200.h"
 #include "clv_unet.cuh"
@@ -30,6 +33,94 @@ int wgrad_splits(long long P, int Cin, int Cout) {
   return (int)s;
 }
 constexpr int kRowBlocks = 148 * 2;
+
+// clv_unet_set_conv_path: 1 tcgen05 (default), 2 tcgen05 with no-swizzle TMA operands, 0 mma.sync
+int g_conv_path = 1;
+
+// cuTensorMapEncodeTiled from the driver (through the runtime, no link-time
+// dependency on libcuda)
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+  }
+  return fn;
+}
+
+// pixel-block width of the TMA path, or 0 if the image does not tile into
+// 128-pixel blocks
+int tma_block_width(const ConvArgs& a) {
+  if (a.W % TC_BM == 0) return TC_BM;
+  if (TC_BM % a.W == 0 && a.H % (TC_BM / a.W) == 0) return a.W;
+  return 0;
+}
+
+template <int BN, bool SW> int launch_conv_tma(const ConvArgs& a, int bw, cudaStream_t s) {
+  PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+  if (!enc) return clv_host::set_error(CLV_ERR_CUDA, "unet_conv3x3: cuTensorMapEncodeTiled unavailable");
+  CUtensorMap ta, tb;
+  {  // activations [N][H][W][in_cs] BF16
+    const cuuint64_t dims[4] = {(cuuint64_t)a.in_cs, (cuuint64_t)a.W, (cuuint64_t)a.H, (cuuint64_t)a.N};
+    const cuuint64_t strides[3] = {(cuuint64_t)a.in_cs * 2, (cuuint64_t)a.W * a.in_cs * 2,
+                                   (cuuint64_t)a.H * a.W * a.in_cs * 2};
+    const cuuint32_t box[4] = {SW ? 32u : 8u, (cuuint32_t)bw, (cuuint32_t)(TC_BM / bw), 1};
+    const cuuint32_t es[4] = {1, 1, 1, 1};
+    if (enc(&ta, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<bf16*>(a.in), dims, strides, box, es,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, SW ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_NONE,
+            CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+      return clv_host::set_error(CLV_ERR_INVALID, "unet_conv3x3: activation tensor map rejected");
+  }
+  {  // weights [9 * Cin][Cout] BF16
+    const cuuint64_t dims[2] = {(cuuint64_t)a.Cout, (cuuint64_t)9 * a.Cin};
+    const cuuint64_t strides[1] = {(cuuint64_t)a.Cout * 2};
+    const cuuint32_t box[2] = {SW ? 32u : 8u, TC_BK};
+    const cuuint32_t es[2] = {1, 1};
+    if (enc(&tb, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<bf16*>(a.w), dims, strides, box, es,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, SW ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_NONE,
+            CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+      return clv_host::set_error(CLV_ERR_INVALID, "unet_conv3x3: weight tensor map rejected");
+  }
+  auto kern = conv3x3_tma_kernel<BN, SW>;
+  static int grid = 0;
+  if (!grid) {
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TmaSmem<BN>)) !=
+            cudaSuccess ||
+        cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             (int)cudaSharedmemCarveoutMaxShared) != cudaSuccess)
+      return clv_host::check_cuda("cudaFuncSetAttribute(conv3x3_tma_kernel)");
+    // persistent: shared memory (228 KB an SM, 1 KB reserved per block),
+    // threads and tensor-memory columns (512 an SM) bound the resident CTAs
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int by_smem = (228 * 1024) / ((int)sizeof(TmaSmem<BN>) + 1024);
+    const int per_sm = std::min(std::min(by_smem, 2048 / TMA_THREADS), 512 / (2 * BN));
+    grid = sms * std::max(per_sm, 1);
+  }
+  const long long tiles = (long long)a.N * (a.H / (TC_BM / bw)) * (a.W / bw) * (a.Cout / BN);
+  kern<<<(unsigned)std::min<long long>(grid, tiles), TMA_THREADS, sizeof(TmaSmem<BN>), s>>>(ta, tb, a, bw);
+  return clv_host::check_cuda("conv3x3_tma_kernel");
+}
+
+template <int BN> int launch_conv_tc(const ConvArgs& a, long long P, cudaStream_t s) {
+  auto kern = conv3x3_tc_kernel<BN>;
+  static bool configured = false;
+  if (!configured) {
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TcSmem<BN>)) !=
+        cudaSuccess)
+      return clv_host::check_cuda("cudaFuncSetAttribute(conv3x3_tc_kernel)");
+    configured = true;
+  }
+  dim3 grid(nb(P, TC_BM), a.Cout / BN);
+  kern<<<grid, 128, sizeof(TcSmem<BN>), s>>>(a);
+  return clv_host::check_cuda("conv3x3_tc_kernel");
+}
 }  // namespace
 
 extern "C" {
@@ -45,6 +136,23 @@ int clv_unet_conv3x3(const clv_unet_conv* args, void* stream) {
                                "unet_conv3x3: Cin and Cout must be multiples of 32, input strides/offsets of 8, "
                                "pointers 16-byte aligned");
   const long long P = (long long)a.N * a.H * a.W;
+  if (g_conv_path >= 1) {
+    // images that tile into 128-pixel blocks: operands by TMA; others: cp.async
+    const int bw = tma_block_width(a);
+    if (bw && g_conv_path == 1) {
+      if (a.Cout % 128 == 0) return launch_conv_tma<128, true>(a, bw, S(stream));
+      if (a.Cout % 64 == 0) return launch_conv_tma<64, true>(a, bw, S(stream));
+      return launch_conv_tma<32, true>(a, bw, S(stream));
+    }
+    if (bw) {
+      if (a.Cout % 128 == 0) return launch_conv_tma<128, false>(a, bw, S(stream));
+      if (a.Cout % 64 == 0) return launch_conv_tma<64, false>(a, bw, S(stream));
+      return launch_conv_tma<32, false>(a, bw, S(stream));
+    }
+    if (a.Cout % 128 == 0) return launch_conv_tc<128>(a, P, S(stream));
+    if (a.Cout % 64 == 0) return launch_conv_tc<64>(a, P, S(stream));
+    return launch_conv_tc<32>(a, P, S(stream));
+  }
   if (a.Cout % 64 == 0) {
     dim3 grid(nb(P, CONV_BM), a.Cout / 64);
     conv3x3_kernel<64><<<grid, 256, 0, S(stream)>>>(a);
@@ -181,6 +289,24 @@ int clv_unet_adam(float* w, const float* g, float* m, float* v, long long n, flo
   if (!w || !g || !m || !v) return clv_host::set_error(CLV_ERR_INVALID, "unet_adam: null");
   adam_kernel<<<nb(n, 256), 256, 0, S(stream)>>>(w, g, m, v, n, lr_t, b1, b2, eps);
   return clv_host::check_cuda("adam_kernel");
+}
+
+int clv_unet_set_conv_path(int path) {
+  if (path < 0 || path > 2) return clv_host::set_error(CLV_ERR_INVALID, "unet_set_conv_path: 0, 1 or 2");
+  g_conv_path = path;
+  return CLV_OK;
+}
+
+int clv_unet_timeouts(int* count, int reset) {
+  if (!count) return clv_host::set_error(CLV_ERR_INVALID, "unet_timeouts: null");
+  if (cudaMemcpyFromSymbol(count, g_tc_timeouts, sizeof(int)) != cudaSuccess)
+    return clv_host::check_cuda("unet_timeouts");
+  if (reset) {
+    const int zero = 0;
+    if (cudaMemcpyToSymbol(g_tc_timeouts, &zero, sizeof(int)) != cudaSuccess)
+      return clv_host::check_cuda("unet_timeouts");
+  }
+  return CLV_OK;
 }
 
 int clv_unet_pack(const float* wf, int Cin, int Cout, void* w, void* wt, void* stream) {

@@ -1,8 +1,10 @@
 // Kernels of the learned surrogate: a U-Net on (N, H, W, C) BF16 activations
 // with FP32 accumulation.
 //
-// conv3x3_kernel is an implicit GEMM on the tensor cores (mma.sync
-// m16n8k16, BF16 in, FP32 accumulate): rows are output pixels, columns output
+// conv3x3_tma_kernel and conv3x3_tc_kernel (the default path) are implicit
+// GEMMs on the 5th-generation tensor cores (tcgen05.mma, accumulator in tensor
+// memory), described at the kernels; conv3x3_kernel is the same GEMM on
+// mma.sync m16n8k16 (BF16 in, FP32 accumulate), kept as a selectable variant: rows are output pixels, columns output
 // channels, the reduction runs over (tap, input channel) in chunks of 32,
 // staged through shared memory with cp.async double buffering (zero fill at
 // the image border). Its epilogue adds the bias and applies GELU, writes the
@@ -18,6 +20,7 @@
 // Activations may be channel slices of a wider buffer (the U-Net's
 // concatenations): element (p, c) of a slice is ptr[p * stride + offset + c].
 #pragma once
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <stdint.h>
 
@@ -191,6 +194,434 @@ template <int BN> __global__ void __launch_bounds__(256) conv3x3_kernel(ConvArgs
         *reinterpret_cast<__nv_bfloat162*>(a.out + p * a.out_cs + a.out_co + c) = __floats2bfloat162_rn(v0, v1);
       }
     }
+}
+
+// ------------------------------------------------- conv 3x3, tcgen05 path
+// The same implicit GEMM on the 5th-generation tensor cores, for images that
+// do not tile into 128-pixel blocks (conv3x3_tma_kernel takes the others). A
+// CTA of 128 threads owns 128 output pixels x BN output channels; the FP32
+// accumulator (128 lanes x BN columns) lives in tensor memory. Per K chunk of
+// 32 (one tap, 32 input channels) the threads stage, with cp.async into a ring
+// of TC_STAGES buffers TC_AHEAD chunks ahead, the A tile (pixels x channels,
+// K-major 8x16-byte core matrices, zero fill at the image border) and the B
+// tile (weights rows of [tap][Cin][Cout], MN-major core matrices); one thread
+// issues two tcgen05.mma (M 128, N BN, K 16, BF16 in, FP32 accumulate) and
+// commits them to the stage's mbarrier; a stage is refilled once the MMAs
+// that read it are done. The epilogue reads the accumulator with tcgen05.ld
+// (warp w: lanes 32w..32w+31, one pixel a thread) and applies the same bias /
+// gate / GELU as conv3x3_kernel. Every mbarrier wait is bounded; a wait that
+// runs out counts in g_tc_timeouts and the kernel stops issuing, waits
+// (bounded) for the MMAs it issued and frees its tensor memory.
+#ifndef CLV_TC_STAGES
+#define CLV_TC_STAGES 4
+#endif
+#ifndef CLV_TC_AHEAD
+#define CLV_TC_AHEAD 2
+#endif
+constexpr int TC_BM = 128, TC_BK = 32, TC_STAGES = CLV_TC_STAGES, TC_AHEAD = CLV_TC_AHEAD;
+static_assert(TC_AHEAD >= 1 && TC_AHEAD < TC_STAGES, "pipeline depth");
+
+__device__ int g_tc_timeouts;  // bounded waits that ran out (read by clv_unet_timeouts)
+
+// shared-memory matrix descriptor: byte offsets lbo (leading-dimension
+// stride) and sbo (stride-dimension stride), descriptor version 1 (sm_100),
+// layout 0 (no swizzle) or 4 (64-byte swizzle)
+__device__ __forceinline__ uint64_t tc_smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo, uint32_t layout = 0) {
+  return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46) | ((uint64_t)layout << 61);
+}
+// instruction descriptor of kind::f16: BF16 A and B, FP32 D, A K-major,
+// B MN-major, M x N
+__host__ __device__ constexpr uint32_t tc_idesc(int M, int N) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | (1u << 16) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+__device__ __forceinline__ bool tc_wait(uint32_t bar, uint32_t parity) {
+  for (int i = 0; i < (1 << 22); i++) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.b32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (ok) return true;
+  }
+  return false;
+}
+__device__ __forceinline__ void tc_mma(uint32_t dtm, uint64_t da, uint64_t db, uint32_t idesc, uint32_t accum) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(dtm),
+      "l"(da), "l"(db), "r"(idesc), "r"(accum));
+}
+__device__ __forceinline__ void tc_commit(uint32_t bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory"); }
+
+// the epilogue of one pixel (thread) over 8 accumulator columns starting at
+// output channel c0: bias, gate, pre-activation, GELU, BF16 store
+__device__ __forceinline__ void tc_epilogue8(const ConvArgs& a, long long p, int c0, const uint32_t (&v)[8]) {
+#pragma unroll
+  for (int jj = 0; jj < 8; jj += 2) {
+    const int c = c0 + jj;
+    if (c >= a.Cout) continue;
+    float v0 = __uint_as_float(v[jj]), v1 = __uint_as_float(v[jj + 1]);
+    if (a.bias) {
+      v0 += a.bias[c];
+      v1 += a.bias[c + 1];
+    }
+    if (a.gate) {
+      const __nv_bfloat162 gz = *reinterpret_cast<const __nv_bfloat162*>(a.gate + p * a.gate_cs + a.gate_co + c);
+      v0 *= gelu_grad(__bfloat162float(gz.x));
+      v1 *= gelu_grad(__bfloat162float(gz.y));
+    }
+    if (a.pre) *reinterpret_cast<__nv_bfloat162*>(a.pre + p * a.Cout + c) = __floats2bfloat162_rn(v0, v1);
+    if (a.gelu) {
+      v0 = gelu_f(v0);
+      v1 = gelu_f(v1);
+    }
+    *reinterpret_cast<__nv_bfloat162*>(a.out + p * a.out_cs + a.out_co + c) = __floats2bfloat162_rn(v0, v1);
+  }
+}
+__device__ __forceinline__ void tc_ld8(uint32_t taddr, uint32_t (&v)[8]) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];\n"
+               : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
+               : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+}
+
+template <int BN> struct TcSmem {
+  bf16 A[TC_STAGES][TC_BM * TC_BK];
+  bf16 B[TC_STAGES][BN * TC_BK];
+  uint64_t bar[TC_STAGES];
+  uint32_t tmem;
+};
+
+template <int BN> __global__ void __launch_bounds__(128) conv3x3_tc_kernel(ConvArgs a) {
+  static_assert(BN == 32 || BN == 64 || BN == 128, "BN");
+  constexpr int TCOLS = BN;                    // tensor-memory columns (a power of two >= 32)
+  constexpr uint32_t LBO_A = TC_BM / 8 * 128;  // A: K-adjacent core matrices (8 channels apart)
+  constexpr uint32_t LBO_B = BN / 8 * 128;     // B: K-adjacent core matrices (8 rows apart)
+  constexpr uint32_t IDESC = tc_idesc(TC_BM, BN);
+  extern __shared__ __align__(1024) unsigned char tc_raw[];
+  TcSmem<BN>& s = *reinterpret_cast<TcSmem<BN>*>(tc_raw);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const long long P = (long long)a.N * a.H * a.W;
+  const long long m0 = (long long)blockIdx.x * TC_BM;
+  const int n0 = blockIdx.y * BN;
+  const int cpt = a.Cin / TC_BK;  // K chunks per tap
+  const int kchunks = 9 * cpt;
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(&s.tmem)),
+                 "r"(TCOLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
+  }
+  if (tid == 0) {
+#pragma unroll
+    for (int st = 0; st < TC_STAGES; st++)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&s.bar[st])) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = s.tmem;
+
+  // this thread's A row (pixel m0 + tid)
+  const long long ap = m0 + tid;
+  int an = 0, ah = 0, aw = 0;
+  if (ap < P) {
+    an = (int)(ap / ((long long)a.H * a.W));
+    const int rem = (int)(ap % ((long long)a.H * a.W));
+    ah = rem / a.W;
+    aw = rem % a.W;
+  }
+  auto load = [&](int chunk, int st) {
+    const int tap = chunk / cpt, c0 = (chunk % cpt) * TC_BK;
+    const int hh = ah + tap / 3 - 1, ww = aw + tap % 3 - 1;
+    const bool ok = ap < P && hh >= 0 && hh < a.H && ww >= 0 && ww < a.W;
+    const bf16* src = ok ? a.in + ((long long)(an * a.H + hh) * a.W + ww) * a.in_cs + a.in_co + c0 : a.in;
+    unsigned char* A = reinterpret_cast<unsigned char*>(s.A[st]);
+#pragma unroll
+    for (int v = 0; v < TC_BK / 8; v++)  // core matrix (row group tid/8, channel group v), row tid%8
+      cp_async16(A + v * LBO_A + (tid >> 3) * 128 + (tid & 7) * 16, ok ? src + v * 8 : a.in, ok);
+    unsigned char* B = reinterpret_cast<unsigned char*>(s.B[st]);
+#pragma unroll
+    for (int q = tid; q < BN * TC_BK / 8; q += 128) {  // weight row kk, output channels ng*8 .. ng*8+7
+      const int kk = q / (BN / 8), ng = q % (BN / 8);
+      const int col = n0 + ng * 8;
+      const bool okb = col < a.Cout;
+      const bf16* bsrc = okb ? a.w + ((long long)(tap * a.Cin + c0 + kk)) * a.Cout + col : a.w;
+      cp_async16(B + (kk >> 3) * LBO_B + ng * 128 + (kk & 7) * 16, bsrc, okb);
+    }
+  };
+
+  bool live = true;  // no bounded wait has run out
+#pragma unroll
+  for (int c = 0; c < TC_AHEAD; c++) {
+    if (c < kchunks) load(c, c);
+    cp_async_commit();
+  }
+  for (int ch = 0; ch < kchunks; ch++) {
+    const int st = ch % TC_STAGES;
+    const int nxt = ch + TC_AHEAD;
+    if (nxt < kchunks) {
+      // the stage of chunk nxt was last read by the MMAs of chunk old
+      const int old = nxt - TC_STAGES;
+      if (old >= 0 && live && !tc_wait(smem_u32(&s.bar[old % TC_STAGES]), (old / TC_STAGES) & 1)) {
+        live = false;
+        atomicAdd(&g_tc_timeouts, 1);
+      }
+      if (live) load(nxt, nxt % TC_STAGES);
+    }
+    cp_async_commit();
+    cp_async_wait<TC_AHEAD>();  // chunk ch has landed
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    __syncthreads();
+    if (tid == 0 && live) {
+      tc_fence_after();
+      const uint32_t sa = smem_u32(s.A[st]), sb = smem_u32(s.B[st]);
+#pragma unroll
+      for (int kh = 0; kh < TC_BK / 16; kh++)
+        tc_mma(tmem, tc_smem_desc(sa + kh * 2 * LBO_A, LBO_A, 128), tc_smem_desc(sb + kh * 2 * LBO_B, LBO_B, 128),
+               IDESC, (ch > 0 || kh > 0) ? 1u : 0u);
+      tc_commit(smem_u32(&s.bar[st]));
+    }
+  }
+  cp_async_wait<0>();
+  // the last chunk's commit completes when every MMA of the tile has
+  const int last = kchunks - 1;
+  bool ready = tc_wait(smem_u32(&s.bar[last % TC_STAGES]), (last / TC_STAGES) & 1);
+  if (!ready) atomicAdd(&g_tc_timeouts, 1);
+  tc_fence_after();
+  live = live && ready;
+  live = __syncthreads_and(live);
+
+  if (live) {
+    const long long p = m0 + warp * 32 + lane;
+    const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
+#pragma unroll 1
+    for (int c8 = 0; c8 < BN / 8; c8++) {
+      uint32_t v[8];
+      tc_ld8(trow + c8 * 8, v);
+      if (p < P) tc_epilogue8(a, p, n0 + c8 * 8, v);
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(TCOLS));
+  }
+}
+
+// ------------------------------------------ conv 3x3, TMA + tcgen05 path
+// For images that tile evenly into blocks of 128 pixels (W divides 128 and H
+// is a multiple of 128 / W, or W is a multiple of 128). Persistent and warp
+// specialised: a CTA of 6 warps takes tiles (a (128 / bw) x bw pixel block of
+// one image, BN output channels) blockIdx.x, blockIdx.x + gridDim.x, ...
+//   * warp 0 (one thread) loads each K chunk (one tap, 32 input channels)
+//     with the tensor memory accelerator into a ring of TC_STAGES stages, the
+//     image border as TMA's zero fill. With SW (the default), one box of
+//     [32 channels, bw, 128 / bw, 1] of the activation tensor at the tap's
+//     offset lands as the K-major operand in the 64-byte swizzled layout
+//     (128 pixel rows of 64 bytes; 8-row atoms 512 bytes apart) and BN / 32
+//     boxes of [32 output channels, 32 rows] of the weights as the MN-major
+//     operand in the same swizzle; without SW, boxes 16 bytes wide fill the
+//     no-swizzle core-matrix layouts (four [8, bw, 128 / bw, 1] activation
+//     boxes, BN / 8 [8, 32] weight boxes);
+//   * warp 1 (one thread) issues the chunk's two tcgen05.mma (M 128, N BN,
+//     K 16) into one of two tensor-memory accumulators, commits them to the
+//     stage's empty barrier and, after a tile's last chunk, to the
+//     accumulator's full barrier;
+//   * warps 2-5 drain a full accumulator (warp w: lanes 32 (w % 4) ..,
+//     one pixel a thread) through the bias / gate / GELU epilogue while the
+//     next tile accumulates in the other one, then free it.
+// Every wait is bounded (g_tc_timeouts); a role whose wait runs out stops.
+constexpr int TMA_THREADS = 192;
+
+template <int BN> struct TmaSmem {
+  bf16 A[TC_STAGES][TC_BM * TC_BK];
+  bf16 B[TC_STAGES][BN * TC_BK];
+  uint64_t full[TC_STAGES], empty[TC_STAGES], acc_full[2], acc_empty[2];
+  uint32_t tmem;
+};
+
+__device__ __forceinline__ void tma_load4(uint32_t dst, const void* map, int c0, int c1, int c2, int c3, uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], [%6];\n" ::"r"(
+          dst),
+      "l"(map), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(bar)
+      : "memory");
+}
+__device__ __forceinline__ void tma_load2(uint32_t dst, const void* map, int c0, int c1, uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n" ::"r"(dst),
+      "l"(map), "r"(c0), "r"(c1), "r"(bar)
+      : "memory");
+}
+
+template <int BN, bool SW>
+__global__ void __launch_bounds__(TMA_THREADS)
+    conv3x3_tma_kernel(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUtensorMap tb, ConvArgs a, int bw) {
+  static_assert(BN == 32 || BN == 64 || BN == 128, "BN");
+  constexpr int TCOLS = 2 * BN;  // two accumulators
+  constexpr uint32_t A_BYTES = TC_BM * TC_BK * 2, B_BYTES = BN * TC_BK * 2;
+  // no swizzle: A 8-channel groups (LBO) 2048 B apart, 8-row groups (SBO) 128 B; B 8-row groups (LBO) 128 B,
+  // 8-channel groups (SBO) 512 B. 64-byte swizzle: A 8-row atoms (SBO) 512 B apart, K step of 16 channels
+  // +32 B; B 32-channel groups (LBO) 2048 B apart, 8-row atoms (SBO) 512 B, K step of 16 rows +1024 B
+  constexpr uint32_t LAYOUT = SW ? 4u : 0u;
+  constexpr uint32_t LBO_A = SW ? 16 : TC_BM * 16, SBO_A = SW ? 512 : 128;
+  constexpr uint32_t LBO_B = SW ? 2048 : 128, SBO_B = SW ? 512 : TC_BK * 16;
+  constexpr uint32_t KSTEP_A = SW ? 32 : 2 * TC_BM * 16, KSTEP_B = SW ? 1024 : 2 * 128;
+  constexpr uint32_t IDESC = tc_idesc(TC_BM, BN);
+  extern __shared__ __align__(1024) unsigned char tma_raw[];
+  TmaSmem<BN>& s = *reinterpret_cast<TmaSmem<BN>*>(tma_raw);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int bh = TC_BM / bw;
+  const int tiles_w = a.W / bw, tiles_h = a.H / bh;
+  const int ntn = a.Cout / BN;
+  const long long ntiles = (long long)a.N * tiles_h * tiles_w * ntn;
+  const int cpt = a.Cin / TC_BK, kchunks = 9 * cpt;
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(&s.tmem)),
+                 "r"(TCOLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
+  }
+  if (tid == 32) {
+#pragma unroll
+    for (int st = 0; st < TC_STAGES; st++) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&s.full[st])) : "memory");
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&s.empty[st])) : "memory");
+    }
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&s.acc_full[q])) : "memory");
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 128;\n" ::"r"(smem_u32(&s.acc_empty[q])) : "memory");
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = s.tmem;
+
+  // tile q -> (image, pixel block, output-channel block); channel blocks of
+  // one pixel block are consecutive, so they share its activations in L2
+  auto tile = [&](long long q, int& img, int& h0, int& w0, int& n0) {
+    n0 = (int)(q % ntn) * BN;
+    q /= ntn;
+    w0 = (int)(q % tiles_w) * bw;
+    q /= tiles_w;
+    h0 = (int)(q % tiles_h) * bh;
+    img = (int)(q / tiles_h);
+  };
+
+  if (warp == 0) {
+    if (lane == 0) {  // TMA producer
+      long long it = 0;
+      bool ok = true;
+      for (long long q = blockIdx.x; q < ntiles && ok; q += gridDim.x) {
+        int img, h0, w0, n0;
+        tile(q, img, h0, w0, n0);
+        for (int ch = 0; ch < kchunks; ch++, it++) {
+          const int st = (int)(it % TC_STAGES);
+          const long long j = it / TC_STAGES;
+          if (j >= 1 && !tc_wait(smem_u32(&s.empty[st]), (uint32_t)((j - 1) & 1))) {
+            ok = false;
+            atomicAdd(&g_tc_timeouts, 1);
+            break;
+          }
+          const int tap = ch / cpt, c0 = (ch % cpt) * TC_BK;
+          const uint32_t fb = smem_u32(&s.full[st]);
+          asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(fb), "r"(A_BYTES + B_BYTES)
+                       : "memory");
+          const uint32_t sa = smem_u32(s.A[st]), sb = smem_u32(s.B[st]);
+          if (SW) {
+            tma_load4(sa, &ta, a.in_co + c0, w0 + tap % 3 - 1, h0 + tap / 3 - 1, img, fb);
+#pragma unroll
+            for (int ng = 0; ng < BN / 32; ng++) tma_load2(sb + ng * 2048, &tb, n0 + 32 * ng, tap * a.Cin + c0, fb);
+          } else {
+#pragma unroll
+            for (int g = 0; g < TC_BK / 8; g++)
+              tma_load4(sa + g * TC_BM * 16, &ta, a.in_co + c0 + 8 * g, w0 + tap % 3 - 1, h0 + tap / 3 - 1, img, fb);
+#pragma unroll
+            for (int ng = 0; ng < BN / 8; ng++)
+              tma_load2(sb + ng * TC_BK * 16, &tb, n0 + 8 * ng, tap * a.Cin + c0, fb);
+          }
+        }
+      }
+      // the loads in flight land before the CTA can exit
+      for (long long c = it - 1; c >= 0 && c >= it - TC_STAGES; c--)
+        tc_wait(smem_u32(&s.full[c % TC_STAGES]), (uint32_t)((c / TC_STAGES) & 1));
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {  // MMA issuer
+      long long it = 0;
+      int t = 0;
+      bool ok = true;
+      for (long long q = blockIdx.x; q < ntiles && ok; q += gridDim.x, t++) {
+        const int acc = t & 1;
+        if (t >= 2 && !tc_wait(smem_u32(&s.acc_empty[acc]), (uint32_t)(((t >> 1) - 1) & 1))) {
+          ok = false;
+          atomicAdd(&g_tc_timeouts, 1);
+          break;
+        }
+        tc_fence_after();
+        const uint32_t dtm = tmem + acc * BN;
+        for (int ch = 0; ch < kchunks; ch++, it++) {
+          const int st = (int)(it % TC_STAGES);
+          if (!tc_wait(smem_u32(&s.full[st]), (uint32_t)((it / TC_STAGES) & 1))) {
+            ok = false;
+            atomicAdd(&g_tc_timeouts, 1);
+            break;
+          }
+          tc_fence_after();
+          const uint32_t sa = smem_u32(s.A[st]), sb = smem_u32(s.B[st]);
+#pragma unroll
+          for (int kh = 0; kh < TC_BK / 16; kh++)
+            tc_mma(dtm, tc_smem_desc(sa + kh * KSTEP_A, LBO_A, SBO_A, LAYOUT),
+                   tc_smem_desc(sb + kh * KSTEP_B, LBO_B, SBO_B, LAYOUT), IDESC, (ch > 0 || kh > 0) ? 1u : 0u);
+          tc_commit(smem_u32(&s.empty[st]));
+        }
+        if (ok) tc_commit(smem_u32(&s.acc_full[acc]));
+      }
+    }
+  } else {  // epilogue warps 2-5
+    const int quarter = warp & 3;  // tensor-memory lanes 32 quarter .. 32 quarter + 31
+    const int r = quarter * 32 + lane;
+    int t = 0;
+    for (long long q = blockIdx.x; q < ntiles; q += gridDim.x, t++) {
+      const int acc = t & 1;
+      const bool ok = __all_sync(0xffffffffu, tc_wait(smem_u32(&s.acc_full[acc]), (uint32_t)((t >> 1) & 1)));
+      if (!ok) {
+        if (lane == 0) atomicAdd(&g_tc_timeouts, 1);
+        break;
+      }
+      tc_fence_after();
+      int img, h0, w0, n0;
+      tile(q, img, h0, w0, n0);
+      const long long p = ((long long)img * a.H + h0 + r / bw) * a.W + w0 + r % bw;
+      const uint32_t trow = tmem + ((uint32_t)(quarter * 32) << 16) + acc * BN;
+#pragma unroll 1
+      for (int c8 = 0; c8 < BN / 8; c8++) {
+        uint32_t v[8];
+        tc_ld8(trow + c8 * 8, v);
+        tc_epilogue8(a, p, n0 + c8 * 8, v);
+      }
+      tc_fence_before();
+      asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(&s.acc_empty[acc])) : "memory");
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(TCOLS));
+  }
 }
 
 // ------------------------------------------------------------ wgrad 3x3

@@ -365,6 +365,15 @@ typedef struct clv_unet_conv {
   int gelu;
 } clv_unet_conv;
 int clv_unet_conv3x3(const clv_unet_conv *args, void *stream);
+/* Tensor-core path of clv_unet_conv3x3 (process-wide): 1 = tcgen05.mma with
+ * the accumulator in tensor memory (the default; operands by TMA in the
+ * 64-byte swizzled layout when the image tiles into 128-pixel blocks, else by
+ * cp.async), 2 = the same with no-swizzle TMA operands, 0 = mma.sync. */
+int clv_unet_set_conv_path(int path);
+/* Bounded waits of the tcgen05 convolutions that ran out since the last
+ * reset (0 in a healthy run; a tile whose wait ran out writes no output).
+ * Reads device memory: synchronises with the device. */
+int clv_unet_timeouts(int *count, int reset);
 /* dw ([9][Cin][Cout] FP32) (+)= sum over pixels of x[p + tap][ci] g[p][co]
  * (g: gradient wrt the pre-activation, [P][Cout] BF16). */
 size_t clv_unet_wgrad_scratch_bytes(int N, int H, int W, int Cin, int Cout);

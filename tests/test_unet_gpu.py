@@ -1,5 +1,6 @@
-"""The surrogate's CUDA kernels (BF16 tensor-core convolutions, FP32
-accumulation) against the float64 oracle (oracle/unet_oracle.py, itself
+"""The surrogate's CUDA kernels (BF16 tensor-core convolutions on tcgen05 with
+the accumulator in tensor memory and TMA- or cp.async-staged operands, or on
+mma.sync; FP32 accumulation) against the float64 oracle (oracle/unet_oracle.py, itself
 checked by finite differences): single layers with channel slices, bias,
 GELU and gate; the weight gradient; the whole network's output and every
 parameter's gradient; and training that lowers the loss. BF16 activations and
@@ -30,8 +31,24 @@ def _rel(a, b):
     return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30)
 
 
-@pytest.mark.parametrize('cin,cout,gelu,gate', [(64, 96, True, False), (96, 64, False, True), (32, 256, True, True)])
-def test_conv3x3_layer(cuda_lib, cin, cout, gelu, gate):
+@pytest.fixture(params=[1, 2, 0], ids=['tcgen05', 'tcgen05-noswizzle', 'mma.sync'])
+def conv_path(request, cuda_lib):
+    from clvisc_b200 import _lib
+    lib = _lib.load()
+    _lib.check(lib.clv_unet_set_conv_path(request.param), 'set_conv_path')
+    yield request.param
+    _lib.check(lib.clv_unet_set_conv_path(1), 'set_conv_path')
+
+
+def _timeouts(lib):
+    n = ctypes.c_int()
+    assert lib.clv_unet_timeouts(ctypes.byref(n), 1) == 0
+    return n.value
+
+
+@pytest.mark.parametrize('cin,cout,gelu,gate', [(64, 96, True, False), (96, 64, False, True), (32, 256, True, True),
+                                                (384, 128, True, False), (128, 32, False, False)])
+def test_conv3x3_layer(cuda_lib, conv_path, cin, cout, gelu, gate):
     from clvisc_b200 import _lib
     from clvisc_b200.surrogate import UnetConv
     lib = _lib.load()
@@ -61,6 +78,42 @@ def test_conv3x3_layer(cuda_lib, cin, cout, gelu, gate):
     y = U.gelu(z) if gelu else z
     assert _rel(_np(out)[..., 2:], y) < 1e-2
     assert (out[..., :2] == 0).all()  # outside the output slice: untouched
+    assert _timeouts(lib) == 0
+
+
+@pytest.mark.parametrize('N,H,W', [(3, 10, 13), (2, 8, 32), (1, 2, 256)])
+def test_conv3x3_paths_agree(cuda_lib, N, H, W):
+    """The tcgen05 paths and mma.sync give the same convolution up to the
+    order of the FP32 accumulation (BF16 outputs: a few units in the last
+    place), for every output-channel tile width: on a ragged pixel count (not
+    a multiple of the 128-pixel tile: operands by cp.async) and on images that
+    tile into 128-pixel blocks of 4 x 32 and 1 x 128 pixels (operands by TMA,
+    swizzled and not)."""
+    from clvisc_b200 import _lib
+    from clvisc_b200.surrogate import UnetConv
+    lib = _lib.load()
+    rng = np.random.default_rng(3)
+    outs = {}
+    for cout in (32, 64, 128, 192):
+        cin = 64
+        xb = _bf(rng.normal(0, 1, (N, H, W, cin))).cuda()
+        w = _bf(rng.normal(0, 0.1, (9, cin, cout))).cuda()
+        bias = torch.from_numpy(rng.normal(0, 0.1, cout).astype(np.float32)).cuda()
+        for path in (1, 2, 0):
+            _lib.check(lib.clv_unet_set_conv_path(path), 'set_conv_path')
+            out = torch.zeros((N, H, W, cout), dtype=torch.bfloat16, device='cuda')
+            a = UnetConv()
+            a.in_, a.in_cs, a.in_co = xb.data_ptr(), cin, 0
+            a.w, a.bias = w.data_ptr(), bias.data_ptr()
+            a.out, a.out_cs, a.out_co = out.data_ptr(), cout, 0
+            a.N, a.H, a.W, a.Cin, a.Cout, a.gelu = N, H, W, cin, cout, 1
+            _lib.check(lib.clv_unet_conv3x3(ctypes.byref(a), None), 'conv')
+            torch.cuda.synchronize()
+            outs[(cout, path)] = _np(out)
+        _lib.check(lib.clv_unet_set_conv_path(1), 'set_conv_path')
+        assert _rel(outs[(cout, 1)], outs[(cout, 0)]) < 4e-3, cout
+        assert _rel(outs[(cout, 2)], outs[(cout, 0)]) < 4e-3, cout
+    assert _timeouts(lib) == 0
 
 
 @pytest.mark.parametrize('cin,cout', [(32, 32), (96, 64), (128, 256)])
@@ -92,7 +145,7 @@ def net_and_ref(cuda_lib):
     return net, x, target
 
 
-def test_unet_forward_and_gradients(net_and_ref):
+def test_unet_forward_and_gradients(net_and_ref, conv_path):
     net, x, target = net_and_ref
     wch = torch.tensor([4.0, 1, 1, 1, 1, 1], device='cuda')
     net.forward(torch.from_numpy(x).cuda())
