@@ -262,6 +262,42 @@ __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence:
 // the epilogue of one pixel (thread) over 8 accumulator columns starting at
 // output channel c0: bias, gate, pre-activation, GELU, BF16 store
 __device__ __forceinline__ void tc_epilogue8(const ConvArgs& a, long long p, int c0, const uint32_t (&v)[8]) {
+  // 16-byte accesses when every row of 8 channels starts 16-byte aligned
+  const bool vec = c0 + 8 <= a.Cout && ((a.out_cs | a.out_co) & 7) == 0 &&
+                   ((reinterpret_cast<uintptr_t>(a.out) | reinterpret_cast<uintptr_t>(a.pre) |
+                     reinterpret_cast<uintptr_t>(a.gate)) & 15) == 0 &&
+                   (!a.gate || ((a.gate_cs | a.gate_co) & 7) == 0);
+  if (vec) {
+    float f[8];
+#pragma unroll
+    for (int jj = 0; jj < 8; jj++) f[jj] = __uint_as_float(v[jj]);
+    if (a.bias)
+#pragma unroll
+      for (int jj = 0; jj < 8; jj++) f[jj] += a.bias[c0 + jj];
+    if (a.gate) {
+      const uint4 g4 = *reinterpret_cast<const uint4*>(a.gate + p * a.gate_cs + a.gate_co + c0);
+      const __nv_bfloat162* gz = reinterpret_cast<const __nv_bfloat162*>(&g4);
+#pragma unroll
+      for (int jj = 0; jj < 4; jj++) {
+        f[2 * jj] *= gelu_grad(__bfloat162float(gz[jj].x));
+        f[2 * jj + 1] *= gelu_grad(__bfloat162float(gz[jj].y));
+      }
+    }
+    uint4 o;
+    __nv_bfloat162* ob = reinterpret_cast<__nv_bfloat162*>(&o);
+    if (a.pre) {
+#pragma unroll
+      for (int jj = 0; jj < 4; jj++) ob[jj] = __floats2bfloat162_rn(f[2 * jj], f[2 * jj + 1]);
+      *reinterpret_cast<uint4*>(a.pre + p * a.Cout + c0) = o;
+    }
+    if (a.gelu)
+#pragma unroll
+      for (int jj = 0; jj < 8; jj++) f[jj] = gelu_f(f[jj]);
+#pragma unroll
+    for (int jj = 0; jj < 4; jj++) ob[jj] = __floats2bfloat162_rn(f[2 * jj], f[2 * jj + 1]);
+    *reinterpret_cast<uint4*>(a.out + p * a.out_cs + a.out_co + c0) = o;
+    return;
+  }
 #pragma unroll
   for (int jj = 0; jj < 8; jj += 2) {
     const int c = c0 + jj;
