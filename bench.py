@@ -129,19 +129,41 @@ def read_peaks():
         return 6650.0, 'fallback'
 
 
-def read_traffic():
-    """DRAM bytes per cell-update of the stage kernel from the committed ncu
-    summary (profiles/visc_stage_*.txt, line 'dram_bytes_per_cell_update: X')."""
+def read_profile_value(key):
+    """A per-cell-update figure of the stage kernel from the committed ncu
+    summary (profiles/visc_stage_*.txt, a line 'key: X'), or None."""
     d = os.path.join(ROOT, 'profiles')
     try:
         for fn in sorted(os.listdir(d)):
             if fn.startswith('visc_stage') and fn.endswith('.txt'):
                 for ln in open(os.path.join(d, fn)):
-                    if ln.startswith('dram_bytes_per_cell_update:'):
+                    if ln.startswith(key + ':'):
                         return float(ln.split(':')[1])
     except OSError:
         pass
     return None
+
+
+def read_traffic():
+    """DRAM bytes per cell-update of the stage kernel (committed ncu summary)."""
+    return read_profile_value('dram_bytes_per_cell_update')
+
+
+def issue_roofline(cell_updates_per_s, sm_mhz):
+    """Warp instructions issued per second by the stage kernel (instructions
+    per cell-update from the committed ncu summary, divided by 32, times
+    cell-updates/s) against the SMs' issue peak: 4 schedulers x 1 warp
+    instruction per cycle x the SM count x the SM clock sampled in the timed
+    region."""
+    import torch
+    inst = read_profile_value('instructions_per_cell_update')
+    if inst is None or not sm_mhz:
+        return None
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    achieved = inst / 32.0 * cell_updates_per_s
+    peak = 4.0 * sms * sm_mhz * 1e6
+    return {'achieved': achieved, 'peak': peak, 'unit': 'warp instructions/s', 'frac': achieved / peak,
+            'instructions_per_cell_update': inst, 'sm_mhz': sm_mhz}
 
 
 def cpu_baseline(steps=2, warmup=0, nx=NX, ny=NY, nz=NZ):
@@ -404,6 +426,7 @@ def run_gpu(args, rank, world, dist):
                          'kernel': 'visc_stage_tiled_kernel<float,IS,KT> (2 launches per step)'},
             'clocks': clocks.summary(),
         }
+        line['roofline']['issue'] = issue_roofline(value / world, line['clocks'].get('sm_mhz'))
         if not args.no_cpu_baseline:
             cb = cpu_baseline(steps=2)
             line['cpu_baseline'] = {k: cb[k] for k in ('value', 'unit', 'cores', 'kind', 'sample')}
