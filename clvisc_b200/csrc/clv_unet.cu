@@ -34,7 +34,8 @@ int wgrad_splits(long long P, int Cin, int Cout) {
 }
 constexpr int kRowBlocks = 148 * 2;
 
-// clv_unet_set_conv_path: 1 tcgen05 (default), 2 tcgen05 with no-swizzle TMA operands, 0 mma.sync
+// clv_unet_set_conv_path: 1 tcgen05 convolutions (default), 2 the same with no-swizzle TMA operands,
+// 3 tcgen05 convolutions and weight gradient, 0 mma.sync
 int g_conv_path = 1;
 
 // cuTensorMapEncodeTiled from the driver (through the runtime, no link-time
@@ -108,6 +109,56 @@ template <int BN, bool SW> int launch_conv_tma(const ConvArgs& a, int bw, cudaSt
   return clv_host::check_cuda("conv3x3_tma_kernel");
 }
 
+// the weight gradient on tcgen05 when the pixels tile into 32-pixel blocks
+// (bw = min(W, 32) columns) and the channel counts are multiples of 32;
+// returns -1 when it does not apply
+int wgrad_tma(const WgradArgs& a, float* dw, int accumulate, int max_splits, cudaStream_t s) {
+  const int bw = a.W >= WGT_BK ? WGT_BK : a.W;
+  if (a.W % bw || WGT_BK % bw || a.H % (WGT_BK / bw) || a.Cin % 32 || a.Cout % 32) return -1;
+  PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+  if (!enc) return -1;
+  const int bh = WGT_BK / bw;
+  CUtensorMap tg, tx;
+  const cuuint32_t box[4] = {32, (cuuint32_t)bw, (cuuint32_t)bh, 1};
+  const cuuint32_t es[4] = {1, 1, 1, 1};
+  {
+    const cuuint64_t dims[4] = {(cuuint64_t)a.Cout, (cuuint64_t)a.W, (cuuint64_t)a.H, (cuuint64_t)a.N};
+    const cuuint64_t strides[3] = {(cuuint64_t)a.Cout * 2, (cuuint64_t)a.W * a.Cout * 2,
+                                   (cuuint64_t)a.H * a.W * a.Cout * 2};
+    if (enc(&tg, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<bf16*>(a.g), dims, strides, box, es,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+      return clv_host::set_error(CLV_ERR_INVALID, "unet_wgrad3x3: gradient tensor map rejected");
+  }
+  {
+    const cuuint64_t dims[4] = {(cuuint64_t)a.x_cs, (cuuint64_t)a.W, (cuuint64_t)a.H, (cuuint64_t)a.N};
+    const cuuint64_t strides[3] = {(cuuint64_t)a.x_cs * 2, (cuuint64_t)a.W * a.x_cs * 2,
+                                   (cuuint64_t)a.H * a.W * a.x_cs * 2};
+    if (enc(&tx, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<bf16*>(a.x), dims, strides, box, es,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+      return clv_host::set_error(CLV_ERR_INVALID, "unet_wgrad3x3: activation tensor map rejected");
+  }
+  static bool configured = false;
+  if (!configured) {
+    if (cudaFuncSetAttribute(wgrad3x3_tma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sizeof(WgTmaSmem)) != cudaSuccess)
+      return clv_host::check_cuda("cudaFuncSetAttribute(wgrad3x3_tma_kernel)");
+    configured = true;
+  }
+  const long long nchunks = (long long)a.N * (a.H / bh) * (a.W / bw);
+  const long long cps = (nchunks + max_splits - 1) / max_splits;
+  const int splits = (int)((nchunks + cps - 1) / cps);  // every split has pixel blocks
+  const int blocks = 9 * ((a.Cout + WGT_BM - 1) / WGT_BM) * ((a.Cin + WGT_BN - 1) / WGT_BN);
+  WgradArgs b = a;
+  wgrad3x3_tma_kernel<<<dim3(blocks, splits), 128, sizeof(WgTmaSmem), s>>>(tg, tx, b, bw, (int)cps);
+  int rc = clv_host::check_cuda("wgrad3x3_tma_kernel");
+  if (rc) return rc;
+  const long long n = 9LL * a.Cin * a.Cout;
+  reduce_partials_kernel<<<nb(n, 256), 256, 0, s>>>(a.part, splits, n, dw, accumulate);
+  return clv_host::check_cuda("reduce_partials_kernel");
+}
+
 template <int BN> int launch_conv_tc(const ConvArgs& a, long long P, cudaStream_t s) {
   auto kern = conv3x3_tc_kernel<BN>;
   static bool configured = false;
@@ -139,7 +190,7 @@ int clv_unet_conv3x3(const clv_unet_conv* args, void* stream) {
   if (g_conv_path >= 1) {
     // images that tile into 128-pixel blocks: operands by TMA; others: cp.async
     const int bw = tma_block_width(a);
-    if (bw && g_conv_path == 1) {
+    if (bw && g_conv_path != 2) {
       if (a.Cout % 128 == 0) return launch_conv_tma<128, true>(a, bw, S(stream));
       if (a.Cout % 64 == 0) return launch_conv_tma<64, true>(a, bw, S(stream));
       return launch_conv_tma<32, true>(a, bw, S(stream));
@@ -187,6 +238,10 @@ int clv_unet_wgrad3x3(const void* x, int x_cs, int x_co, const void* g, int N, i
   a.Cout = Cout;
   const long long P = (long long)N * H * W;
   const int s = wgrad_splits(P, Cin, Cout);
+  if (g_conv_path == 3) {  // tcgen05 where the pixels tile into 32-pixel blocks
+    const int rc = wgrad_tma(a, dw, accumulate, s, S(stream));
+    if (rc != -1) return rc;
+  }
   a.pix_per_split = (P + s - 1) / s;
   dim3 grid((9 * Cin + WG_BM - 1) / WG_BM, (Cout + WG_BN - 1) / WG_BN, s);
   wgrad3x3_kernel<<<grid, 256, 0, S(stream)>>>(a);
@@ -292,7 +347,7 @@ int clv_unet_adam(float* w, const float* g, float* m, float* v, long long n, flo
 }
 
 int clv_unet_set_conv_path(int path) {
-  if (path < 0 || path > 2) return clv_host::set_error(CLV_ERR_INVALID, "unet_set_conv_path: 0, 1 or 2");
+  if (path < 0 || path > 3) return clv_host::set_error(CLV_ERR_INVALID, "unet_set_conv_path: 0, 1, 2 or 3");
   g_conv_path = path;
   return CLV_OK;
 }

@@ -763,6 +763,141 @@ __global__ void __launch_bounds__(256) wgrad3x3_kernel(WgradArgs a) {
 }
 
 // out[i] (+)= sum_s part[s][i], in s order
+// ------------------------------------------ wgrad 3x3, TMA + tcgen05 path
+// (selected by clv_unet_set_conv_path(3): on the surrogate's layers, whose
+// output channels are often 32 or 64 of the 128-row MMA, it is slower than
+// wgrad3x3_kernel.) The weight gradient on the 5th-generation tensor cores, for images whose
+// pixels tile into blocks of 32 (bw = min(W, 32) columns x 32 / bw rows): per
+// tap, D[co][ci] = sum over pixels p of g[p][co] x[p + tap][ci], M = 128
+// output channels (rows beyond Cout are TMA zero fill), N = up to 128 input
+// channels, K = 32-pixel blocks. Both operands are MN-major in the 64-byte
+// swizzled layout: [32 channels, bw, 32 / bw, 1] boxes of g and of x shifted
+// by the tap (the image border as zero fill). A CTA of 128 threads takes one
+// (tap, channel block) and a contiguous range of pixel blocks (split K):
+// thread 0 loads with TMA into TC_STAGES stages, thread 32 issues the
+// tcgen05.mma and commits each stage back, and all four warps write the
+// accumulator (one output channel a thread) as an FP32 partial
+// [split][tap][ci][co] that reduce_partials_kernel adds in a fixed order.
+constexpr int WGT_BM = 128, WGT_BN = 128, WGT_BK = 32;
+
+struct WgTmaSmem {
+  bf16 A[TC_STAGES][WGT_BM * WGT_BK];
+  bf16 B[TC_STAGES][WGT_BN * WGT_BK];
+  uint64_t full[TC_STAGES], empty[TC_STAGES], done;
+  uint32_t tmem;
+};
+
+__global__ void __launch_bounds__(128)
+    wgrad3x3_tma_kernel(const __grid_constant__ CUtensorMap tg, const __grid_constant__ CUtensorMap tx, WgradArgs a,
+                        int bw, int chunks_per_split) {
+  constexpr uint32_t LBO = 2048, SBO = 512, KSTEP = 1024, LAYOUT = 4;  // MN-major, 64-byte swizzle
+  extern __shared__ __align__(1024) unsigned char wgt_raw[];
+  WgTmaSmem& s = *reinterpret_cast<WgTmaSmem*>(wgt_raw);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int mblocks = (a.Cout + WGT_BM - 1) / WGT_BM;
+  int t = blockIdx.x;
+  const int tap = t % 9;
+  t /= 9;
+  const int co0 = (t % mblocks) * WGT_BM, ci0 = (t / mblocks) * WGT_BN;
+  const int nn = min(WGT_BN, a.Cin - ci0);  // a multiple of 32
+  const int split = blockIdx.y;
+  const int bh = WGT_BK / bw;
+  const int per_row = a.W / bw, per_img = per_row * (a.H / bh);
+  const long long nchunks = (long long)a.N * per_img;
+  const long long c0 = (long long)split * chunks_per_split;
+  const long long c1 = min(nchunks, c0 + chunks_per_split);
+  const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | (1u << 15) | (1u << 16) | ((uint32_t)(nn >> 3) << 17) |
+                         ((uint32_t)(WGT_BM >> 4) << 24);
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(&s.tmem)),
+                 "r"(WGT_BN));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
+  }
+  if (tid == 32) {
+#pragma unroll
+    for (int st = 0; st < TC_STAGES; st++) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&s.full[st])) : "memory");
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&s.empty[st])) : "memory");
+    }
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&s.done)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = s.tmem;
+
+  if (tid == 0) {  // TMA producer
+    long long it = 0;
+    for (long long c = c0; c < c1; c++, it++) {
+      const int st = (int)(it % TC_STAGES);
+      const long long j = it / TC_STAGES;
+      if (j >= 1 && !tc_wait(smem_u32(&s.empty[st]), (uint32_t)((j - 1) & 1))) {
+        atomicAdd(&g_tc_timeouts, 1);
+        break;
+      }
+      const int img = (int)(c / per_img), q = (int)(c % per_img);
+      const int h0 = (q / per_row) * bh, w0 = (q % per_row) * bw;
+      const uint32_t fb = smem_u32(&s.full[st]);
+      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(fb),
+                   "r"((uint32_t)(WGT_BM + nn) * WGT_BK * 2)
+                   : "memory");
+      const uint32_t sa = smem_u32(s.A[st]), sb = smem_u32(s.B[st]);
+#pragma unroll
+      for (int i = 0; i < WGT_BM / 32; i++) tma_load4(sa + i * LBO, &tg, co0 + 32 * i, w0, h0, img, fb);
+      for (int i = 0; i < nn / 32; i++)
+        tma_load4(sb + i * LBO, &tx, a.x_co + ci0 + 32 * i, w0 + tap % 3 - 1, h0 + tap / 3 - 1, img, fb);
+    }
+    // the loads in flight land before the CTA can exit
+    for (long long c = it - 1; c >= 0 && c >= it - TC_STAGES; c--)
+      tc_wait(smem_u32(&s.full[c % TC_STAGES]), (uint32_t)((c / TC_STAGES) & 1));
+  } else if (tid == 32) {  // MMA issuer
+    long long it = 0;
+    bool ok = true;
+    for (long long c = c0; c < c1; c++, it++) {
+      const int st = (int)(it % TC_STAGES);
+      if (!tc_wait(smem_u32(&s.full[st]), (uint32_t)((it / TC_STAGES) & 1))) {
+        ok = false;
+        atomicAdd(&g_tc_timeouts, 1);
+        break;
+      }
+      tc_fence_after();
+      const uint32_t sa = smem_u32(s.A[st]), sb = smem_u32(s.B[st]);
+#pragma unroll
+      for (int kh = 0; kh < WGT_BK / 16; kh++)
+        tc_mma(tmem, tc_smem_desc(sa + kh * KSTEP, LBO, SBO, LAYOUT), tc_smem_desc(sb + kh * KSTEP, LBO, SBO, LAYOUT),
+               idesc, (it > 0 || kh > 0) ? 1u : 0u);
+      tc_commit(smem_u32(&s.empty[st]));
+    }
+    if (ok && c1 > c0) tc_commit(smem_u32(&s.done));
+  }
+  bool ready = c1 > c0 ? tc_wait(smem_u32(&s.done), 0) : true;
+  tc_fence_after();
+  ready = __syncthreads_and(ready);
+  if (!ready && tid == 0) atomicAdd(&g_tc_timeouts, 1);
+  if (ready) {
+    const int co = co0 + warp * 32 + lane;
+    const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
+    float* out = a.part + ((long long)split * 9 + tap) * a.Cin * a.Cout;
+#pragma unroll 1
+    for (int c8 = 0; c8 < nn / 8; c8++) {
+      uint32_t v[8];
+      tc_ld8(trow + c8 * 8, v);
+      if (co < a.Cout)
+#pragma unroll
+        for (int jj = 0; jj < 8; jj++)
+          out[(long long)(ci0 + c8 * 8 + jj) * a.Cout + co] = c1 > c0 ? __uint_as_float(v[jj]) : 0.0f;
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(WGT_BN));
+  }
+}
+
 __global__ void reduce_partials_kernel(const float* part, int S, long long n, float* out, int accumulate) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;

@@ -365,10 +365,13 @@ typedef struct clv_unet_conv {
   int gelu;
 } clv_unet_conv;
 int clv_unet_conv3x3(const clv_unet_conv *args, void *stream);
-/* Tensor-core path of clv_unet_conv3x3 (process-wide): 1 = tcgen05.mma with
+/* Tensor-core paths (process-wide): 1 = clv_unet_conv3x3 on tcgen05.mma with
  * the accumulator in tensor memory (the default; operands by TMA in the
  * 64-byte swizzled layout when the image tiles into 128-pixel blocks, else by
- * cp.async), 2 = the same with no-swizzle TMA operands, 0 = mma.sync. */
+ * cp.async) and clv_unet_wgrad3x3 on mma.sync; 2 = the same with no-swizzle
+ * TMA operands; 3 = as 1, and clv_unet_wgrad3x3 on tcgen05 too where the
+ * pixels tile into 32-pixel blocks (slower than mma.sync on the surrogate's
+ * layers); 0 = mma.sync for both. */
 int clv_unet_set_conv_path(int path);
 /* Bounded waits of the tcgen05 convolutions that ran out since the last
  * reset (0 in a healthy run; a tile whose wait ran out writes no output).

@@ -31,7 +31,7 @@ def _rel(a, b):
     return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30)
 
 
-@pytest.fixture(params=[1, 2, 0], ids=['tcgen05', 'tcgen05-noswizzle', 'mma.sync'])
+@pytest.fixture(params=[1, 2, 3, 0], ids=['tcgen05', 'tcgen05-noswizzle', 'tcgen05-wgrad', 'mma.sync'])
 def conv_path(request, cuda_lib):
     from clvisc_b200 import _lib
     lib = _lib.load()
@@ -116,12 +116,15 @@ def test_conv3x3_paths_agree(cuda_lib, N, H, W):
     assert _timeouts(lib) == 0
 
 
-@pytest.mark.parametrize('cin,cout', [(32, 32), (96, 64), (128, 256)])
-def test_wgrad3x3(cuda_lib, cin, cout):
+@pytest.mark.parametrize('cin,cout', [(32, 32), (96, 64), (128, 256), (192, 32)])
+@pytest.mark.parametrize('N,H,W', [(3, 16, 24), (2, 8, 32), (2, 8, 16), (1, 2, 64)])
+def test_wgrad3x3(cuda_lib, conv_path, cin, cout, N, H, W):
+    """Weight gradient against the oracle; with the tcgen05 path, images whose
+    pixels tile into 32-pixel blocks (W = 32, 16, 64 here) take the TMA +
+    tcgen05 kernel, the others (W = 24) the mma.sync kernel."""
     from clvisc_b200 import _lib
     lib = _lib.load()
     rng = np.random.default_rng(7)
-    N, H, W = 3, 16, 24
     xb = _bf(rng.normal(0, 1, (N, H, W, cin + 64))).cuda()
     g = _bf(rng.normal(0, 1, (N, H, W, cout))).cuda()
     dw = torch.zeros(9 * cin * cout, device='cuda')
@@ -133,6 +136,7 @@ def test_wgrad3x3(cuda_lib, cin, cout):
     torch.cuda.synchronize()
     want = U.conv3x3_wgrad(_np(xb)[..., 64:], _np(g))
     assert _rel(dw.cpu().numpy().reshape(9, cin, cout), want) < 1e-5
+    assert _timeouts(lib) == 0
 
 
 @pytest.fixture(scope='module')
