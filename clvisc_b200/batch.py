@@ -407,15 +407,17 @@ class CLViscBatch(object):
     def candidates(self, block_sizes=(64, 128, 256), rows=(64, 128), chunks=(4, 8, 16, 32)):
         """Launch shapes autotune() times. One thread per cell: every block
         size with persistent grids of 1..occupancy blocks per SM and the
-        one-cell-per-thread grid, with and (FP32) without the 128-register
-        cap. Tiled ((2+1)D batches only): rows x chunks, each with the grid
+        one-cell-per-thread grid, without and (FP32) with a 128-register cap
+        (and a 168-register cap below 256 threads). Tiled ((2+1)D batches only): rows x chunks, each with the grid
         that fills the GPU once and the one-tile-per-block grid."""
         sms = torch.cuda.get_device_properties(self.device).multi_processor_count
         out = []
         total = sum(self.sizes)
-        caps = (0, 128) if self.cfg.use_float32 else (0,)
+        caps = (0, 128, 168) if self.cfg.use_float32 else (0,)
         for regs in caps:
             for bs in block_sizes:
+                if regs == 168 and bs == 256:
+                    continue
                 occ = max(1, self.occupancy(bs, regs))
                 for grid in sorted({sms * k for k in range(1, occ + 1)} | {(total + bs - 1) // bs}):
                     out.append(('cell', bs, grid, regs))

@@ -71,13 +71,20 @@ int launch_stage(const clv::Params& p, const clv::BatchArgs<real>& a, int step, 
   return clv_host::check_cuda("batch_stage_kernel");
 }
 
-// the 128-register cap is offered in FP32 only (FP64 spills heavily under it)
+// the register caps are offered in FP32 only (FP64 spills heavily under
+// them): 128 registers a thread (512 threads per SM) or, for 64- and
+// 128-thread blocks, 168 (384 threads per SM)
 template <class real> constexpr int capped_minb(int bs) { return sizeof(real) == 4 ? 512 / bs : 1; }
+template <class real> constexpr int capped168_minb(int bs) { return sizeof(real) == 4 ? 384 / bs : 1; }
 
 template <class real, bool BULK>
-int stage_bs(const clv::Params& p, const clv::BatchArgs<real>& a, int step, int bs, int grid, bool cap,
+int stage_bs(const clv::Params& p, const clv::BatchArgs<real>& a, int step, int bs, int grid, int cap,
              cudaStream_t s) {
   if (cap && sizeof(real) == 8) return clv_host::set_error(CLV_ERR_INVALID, "batch: max_registers is FP32 only");
+  if (cap == 168 && bs == 256)
+    return clv_host::set_error(CLV_ERR_INVALID, "batch: max_registers 168 needs 64- or 128-thread blocks");
+  if (bs == 64 && cap == 168) return launch_stage<real, BULK, 64, capped168_minb<real>(64)>(p, a, step, grid, s);
+  if (bs == 128 && cap == 168) return launch_stage<real, BULK, 128, capped168_minb<real>(128)>(p, a, step, grid, s);
   if (bs == 64)
     return cap ? launch_stage<real, BULK, 64, capped_minb<real>(64)>(p, a, step, grid, s)
                : launch_stage<real, BULK, 64, 1>(p, a, step, grid, s);
@@ -100,8 +107,9 @@ int batch_stage_t(const clv_params* pp, int step, const clv_batch* b, int bs, in
   if (step != 1 && step != 2) return clv_host::set_error(CLV_ERR_INVALID, "batch: step must be 1 or 2");
   if (p.flags & (clv::FLAG_GUBSER_VISC | clv::FLAG_PIMN_OMEGA | clv::FLAG_OMEGA_OMEGA | clv::FLAG_RIEMANN))
     return clv_host::set_error(CLV_ERR_INVALID, "batch: test flags (Gubser, couplings, Riemann) are not batched");
-  if (max_regs != 0 && max_regs != 128) return clv_host::set_error(CLV_ERR_INVALID, "batch: max_registers must be 0 or 128");
-  const bool cap = max_regs == 128;
+  if (max_regs != 0 && max_regs != 128 && max_regs != 168)
+    return clv_host::set_error(CLV_ERR_INVALID, "batch: max_registers must be 0, 128 or 168");
+  const int cap = max_regs;
   if (p.flags & clv::FLAG_BULK) return stage_bs<real, true>(p, a, step, bs, grid, cap, s);
   return stage_bs<real, false>(p, a, step, bs, grid, cap, s);
 }
@@ -214,18 +222,20 @@ int clv_batch_occupancy(const clv_params* p, int block_size, int max_registers, 
     return clv_host::set_error(CLV_ERR_INVALID, "batch_occupancy: bad argument");
   if (block_size != 64 && block_size != 128 && block_size != 256)
     return clv_host::set_error(CLV_ERR_INVALID, "batch_occupancy: block_size must be 64, 128 or 256");
-  if (max_registers != 0 && (max_registers != 128 || p->precision != 4))
-    return clv_host::set_error(CLV_ERR_INVALID, "batch_occupancy: max_registers must be 0 (or 128 in FP32)");
+  if (max_registers != 0 && ((max_registers != 128 && max_registers != 168) || p->precision != 4 ||
+                             (max_registers == 168 && block_size == 256)))
+    return clv_host::set_error(CLV_ERR_INVALID,
+                               "batch_occupancy: max_registers must be 0 (or 128, or 168 below 256 threads, in FP32)");
   const bool bulk = p->flags & CLV_FLAG_BULK;
-  const bool cap = max_registers == 128;
+  const bool cap = max_registers == 128, cap168 = max_registers == 168;
   int n = 0;
   cudaError_t e = cudaSuccess;
   const void* f = nullptr;
 #define CLV_K(real, B, BS, M) f = reinterpret_cast<const void*>(clv::batch_stage_kernel<real, B, BS, M>)
 #define CLV_PICK(real, B)                                                  \
   do {                                                                     \
-    if (block_size == 64) { if (cap) CLV_K(real, B, 64, capped_minb<real>(64)); else CLV_K(real, B, 64, 1); }     \
-    else if (block_size == 128) { if (cap) CLV_K(real, B, 128, capped_minb<real>(128)); else CLV_K(real, B, 128, 1); } \
+    if (block_size == 64) { if (cap168) CLV_K(real, B, 64, capped168_minb<real>(64)); else if (cap) CLV_K(real, B, 64, capped_minb<real>(64)); else CLV_K(real, B, 64, 1); }     \
+    else if (block_size == 128) { if (cap168) CLV_K(real, B, 128, capped168_minb<real>(128)); else if (cap) CLV_K(real, B, 128, capped_minb<real>(128)); else CLV_K(real, B, 128, 1); } \
     else { if (cap) CLV_K(real, B, 256, capped_minb<real>(256)); else CLV_K(real, B, 256, 1); } \
   } while (0)
   if (p->precision == 4) {

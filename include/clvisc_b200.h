@@ -235,7 +235,8 @@ typedef struct clv_batch {
  * persistent launch of grid_blocks blocks of block_size (64, 128 or 256)
  * threads; grid_blocks <= 0 sizes the grid to fill the GPU once.
  * max_registers: 0 lets the compiler choose; 128 (FP32 only) caps the
- * registers a thread so that 512 threads stay resident per SM. Reads tau and
+ * registers a thread so that 512 threads stay resident per SM; 168 (FP32,
+ * 64- or 128-thread blocks) so that 384 do. Reads tau and
  * the running list from the device, so it can be captured in a CUDA graph. */
 int clv_batch_stage(const clv_params *p, int step, const clv_batch *b, int block_size, int grid_blocks,
                     int max_registers, void *stream);
