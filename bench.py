@@ -39,7 +39,7 @@ ALG_BYTES_PER_CELL_UPDATE = 312
 SLAB_NZ = 16  # CPU-baseline sample: a 385 x 385 x 16 eta slab of the event
 
 
-def make_cfg(nz=NZ, out='/tmp/clv_bench', nx=NX, ny=NY):
+def make_cfg(nz=NZ, out='/tmp/clv_bench', nx=NX, ny=NY, fp64=False):
     from clvisc_b200.config import read_config, set_real
     cfg = read_config([])
     cfg.NX, cfg.NY, cfg.NZ = nx, ny, nz
@@ -48,7 +48,7 @@ def make_cfg(nz=NZ, out='/tmp/clv_bench', nx=NX, ny=NY):
     cfg.DT = DT
     cfg.TAU0 = 0.6
     cfg.eos_type = 'lattice_pce165'
-    cfg.use_float32 = True
+    cfg.use_float32 = not fp64
     cfg.ETAOS_XMIN, cfg.ETAOS_YMIN, cfg.ETAOS_LEFT_SLOP, cfg.ETAOS_RIGHT_SLOP = 0.18, 0.08, 0.0, 0.0
     cfg.TFRZ = 0.137
     cfg.ntskip = 20
@@ -346,6 +346,30 @@ def run_batch(n_events=BATCH_EVENTS, one_at_a_time=True):
     return out
 
 
+def evolve_to_freezeout(args, nx, ny, nz):
+    """The whole event: CLVisc.evolve from the initial condition until the
+    maximum energy density is below freeze-out, with the T = 0.137 GeV
+    hypersurface extracted every ntskip steps and written (visc.py:473-560);
+    wall time around construction, load_ini and evolve."""
+    import torch
+    from clvisc_b200.visc import CLVisc
+    cfg = make_cfg(nz=nz, nx=nx, ny=ny, out='/tmp/clv_bench_evolve', fp64=args.fp64)
+    ic = initial_condition(seed=5, nx=nx, ny=ny, nz=nz)
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    # this event's surface (about 1.6 M elements) exceeds the reference's
+    # capacity of 1.5 M, which this library reports instead of truncating
+    v = CLVisc(cfg, hypersf_capacity=4000000)
+    v.load_ini(ic)
+    v.evolve(max_loops=4000, save_hypersf=True, save_bulk=False)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t
+    steps = int(round((float(v.ideal.tau) - cfg.TAU0) / cfg.DT))
+    return {'wall_s': wall, 'steps': steps, 'tau_end': float(v.ideal.tau),
+            'hypersurface_elements': int(v.ideal.num_of_sf),
+            'cell_updates_per_s': nx * ny * nz * steps / wall}
+
+
 def run_gpu(args, rank, world, dist):
     import numpy as np
     import torch
@@ -353,7 +377,7 @@ def run_gpu(args, rank, world, dist):
     dev = int(os.environ.get('LOCAL_RANK', 0))
     torch.cuda.set_device(dev)
     nx, ny, nz = args.grid
-    cfg = make_cfg(nz=nz, nx=nx, ny=ny, out='/tmp/clv_bench_r%d' % rank)
+    cfg = make_cfg(nz=nz, nx=nx, ny=ny, out='/tmp/clv_bench_r%d' % rank, fp64=args.fp64)
     ic = initial_condition(seed=5, nx=nx, ny=ny, nz=nz)
     v = CLVisc(cfg, gpu_id=dev)
     v.load_ini(ic)
@@ -406,14 +430,20 @@ def run_gpu(args, rank, world, dist):
     d2h = out.nbytes / args.steps
 
     peak, peak_kind = read_peaks()
-    achieved = value / world * ALG_BYTES_PER_CELL_UPDATE / 1e9
-    traffic = read_traffic()
+    # FP64 moves twice the bytes; the committed traffic and instruction
+    # figures are the FP32 kernel's
+    alg = ALG_BYTES_PER_CELL_UPDATE * (2 if args.fp64 else 1)
+    achieved = value / world * alg / 1e9
+    traffic = None if args.fp64 else read_traffic()
+    prec = 'FP64' if args.fp64 else 'FP32'
+    real = 'double' if args.fp64 else 'float'
     if rank == 0:
         line = {
             'metric': METRIC, 'value': value, 'unit': UNIT, 'n_gpus': world, 'steps': args.steps,
             'warmup': args.warmup, 'ms_per_step': ms / args.steps, 'higher_is_better': True, 'scaling': 'weak',
-            'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic',
-            'config': {'workload': 'viscous 385x385x115 Pb+Pb b=8 fm seed 5, FP32, lattice EOS, dtau=0.01',
+            'vs_baseline': None, 'dtype': 'f64' if args.fp64 else 'f32', 'data': 'synthetic',
+            'config': {'workload': 'viscous %dx%dx%d Pb+Pb b=8 fm seed 5, %s, lattice EOS, dtau=0.01'
+                                   % (nx, ny, nz, prec),
                        'cells': cells, 'l2': 'inputs larger than L2 (state 0.95 GB per stage)',
                        'parallelism': 'replicas x%d' % world},
             'e2e': {'value': e2e, 'unit': UNIT, 'h2d_bytes_per_step': h2d, 'd2h_bytes_per_step': d2h,
@@ -422,12 +452,15 @@ def run_gpu(args, rank, world, dist):
             'roofline': {'bound': 'hbm', 'achieved': achieved, 'peak': peak, 'unit': 'GB/s',
                          'frac': achieved / peak, 'peak_kind': peak_kind,
                          'traffic': None if traffic is None else traffic * cells / 2,
-                         'alg_bytes_per_launch': ALG_BYTES_PER_CELL_UPDATE * cells / 2,
-                         'kernel': 'visc_stage_tiled_kernel<float,IS,KT> (2 launches per step)'},
+                         'alg_bytes_per_launch': alg * cells / 2,
+                         'kernel': 'visc_stage_tiled_kernel<%s,IS,KT> (2 launches per step)' % real},
             'clocks': clocks.summary(),
         }
-        line['roofline']['issue'] = issue_roofline(value / world, line['clocks'].get('sm_mhz'))
-        if not args.no_cpu_baseline:
+        line['roofline']['issue'] = None if args.fp64 else issue_roofline(value / world,
+                                                                          line['clocks'].get('sm_mhz'))
+        if args.evolve and world == 1:
+            line['evolve'] = evolve_to_freezeout(args, nx, ny, nz)
+        if not args.no_cpu_baseline and not args.fp64:
             cb = cpu_baseline(steps=2)
             line['cpu_baseline'] = {k: cb[k] for k in ('value', 'unit', 'cores', 'kind', 'sample')}
         if args.batch_events > 0 and world == 1:
@@ -457,6 +490,9 @@ def main():
     ap.add_argument('--surrogate-test', type=int, default=500)
     ap.add_argument('--surrogate-epochs', type=int, default=10)
     ap.add_argument('--surrogate-only', action='store_true', help='print only the surrogate experiment line')
+    ap.add_argument('--fp64', action='store_true', help='the same workload in double precision')
+    ap.add_argument('--evolve', action='store_true',
+                    help='also evolve the whole event to freeze-out with the hypersurface (reported under "evolve")')
     ap.add_argument('--grid', type=lambda s: tuple(int(x) for x in s.split(',')), default=(NX, NY, NZ),
                     help='nx,ny,nz (default: the 385,385,115 workload)')
     args = ap.parse_args()
