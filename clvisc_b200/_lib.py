@@ -111,6 +111,8 @@ _SIGS = {
     # learned surrogate (clv_unet_conv is passed as a pointer to surrogate.UnetConv)
     'clv_unet_conv3x3': ([_VP, _VP], ctypes.c_int),
     'clv_unet_set_conv_path': ([ctypes.c_int], ctypes.c_int),
+    'clv_write_table': ([ctypes.c_char_p, ctypes.c_char_p, _VP, ctypes.c_int, ctypes.c_longlong, ctypes.c_int],
+                        ctypes.c_int),
     'clv_unet_timeouts': ([ctypes.POINTER(ctypes.c_int), ctypes.c_int], ctypes.c_int),
     'clv_unet_wgrad_scratch_bytes': ([ctypes.c_int] * 5, ctypes.c_size_t),
     'clv_unet_wgrad3x3': ([_VP, ctypes.c_int, ctypes.c_int, _VP] + [ctypes.c_int] * 5 + [_VP, ctypes.c_int, _VP,
@@ -172,6 +174,20 @@ def check(rc, what):
     if rc != 0:
         msg = _lib.clv_last_error().decode() if _lib is not None else ''
         raise RuntimeError('%s failed: %s (%d) %s' % (what, CLV_ERR.get(rc, 'error'), rc, msg))
+
+
+def write_table(path, header, rows):
+    """numpy.savetxt(path, rows, fmt='%.6e', header=header), byte for byte,
+    by the library's parallel writer; rows is a (n, cols) float32 or float64
+    array."""
+    import numpy as np
+    a = np.ascontiguousarray(rows)
+    if a.dtype not in (np.float32, np.float64) or a.ndim != 2:
+        raise ValueError('write_table takes a 2-D float32 or float64 array')
+    lib = load()
+    check(lib.clv_write_table(path.encode(), None if header is None else header.encode(),
+                              a.ctypes.data_as(ctypes.c_void_p), a.dtype.itemsize, a.shape[0], a.shape[1]),
+          'clv_write_table')
 
 
 def ptr(t):

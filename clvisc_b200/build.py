@@ -19,7 +19,7 @@ ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, 'libclvisc_b200.so')
 OBJDIR = os.path.join(HERE, '_build')
 SOURCES = ['csrc/clv_capi.cu', 'csrc/clv_noalloc.cu', 'csrc/clv_batch.cu', 'csrc/clv_initial.cu',
-           'csrc/clv_bulkinfo.cu', 'csrc/clv_spectra.cu', 'csrc/clv_unet.cu']
+           'csrc/clv_bulkinfo.cu', 'csrc/clv_spectra.cu', 'csrc/clv_unet.cu', 'csrc/clv_io.cu']
 DEPS = ['csrc/clv_device.cuh', 'csrc/clv_stage.cuh', 'csrc/clv_stage_tiled.cuh', 'csrc/clv_stage_tiled2d.cuh',
         'csrc/clv_misc.cuh',
         'csrc/clv_hypersf.cuh', 'csrc/clv_batch.cuh', 'csrc/clv_initial.cuh',

@@ -253,10 +253,10 @@ class CLIdeal(object):
         self.num_of_sf = self.read_num_of_sf()
         if save_hypersf:
             hypersf, sf_txyz = self.hypersf_to_host()
-            np.savetxt(os.path.join(self.cfg.fPathOut, 'hypersf.dat'), hypersf, fmt='%.6e',
-                       header='Tfrz=%.6e ; other rows: dS0, dS1, dS2, dS3, vx, vy, veta, etas' % self.cfg.TFRZ)
-            np.savetxt(os.path.join(self.cfg.fPathOut, 'sf_txyz.dat'), sf_txyz, fmt='%.6e',
-                       header='(t, x, y, z) the time-space coordinates of hypersf elements')
+            _lib.write_table(os.path.join(self.cfg.fPathOut, 'hypersf.dat'),
+                             'Tfrz=%.6e ; other rows: dS0, dS1, dS2, dS3, vx, vy, veta, etas' % self.cfg.TFRZ, hypersf)
+            _lib.write_table(os.path.join(self.cfg.fPathOut, 'sf_txyz.dat'),
+                             '(t, x, y, z) the time-space coordinates of hypersf elements', sf_txyz)
         if save_bulk:
             self.bulkinfo.save(viscous_on=viscous_on)
 

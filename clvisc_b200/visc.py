@@ -168,7 +168,7 @@ class CLVisc(object):
             pi_onsf = self.d_pi_sf[:num_of_sf].cpu().numpy()
         out_path = os.path.join(self.cfg.fPathOut, 'pimnsf.dat')
         comment_line = 'one_o_2TsqrEplusP=%.6e ' % const_for_deltaf + 'pi00 01 02 03 11 12 13 22 23 33'
-        np.savetxt(out_path, pi_onsf.reshape(num_of_sf, 10), fmt='%.6e', header=comment_line)
+        _lib.write_table(out_path, comment_line, pi_onsf.reshape(num_of_sf, 10))
 
     def save(self, save_hypersf=True, save_bulk=False, save_pi=False, save_vorticity=False):
         """visc.py:423-462 (vorticity output is not part of this backend)."""

@@ -420,6 +420,16 @@ int clv_unet_pack(const float *wf, int Cin, int Cout, void *w, void *wt, void *s
 int clv_aos_to_soa(const clv_params *p, const void *aos, void *soa, long long n, int w, void *stream);
 int clv_soa_to_aos(const clv_params *p, const void *soa, void *aos, long long n, int w, void *stream);
 
+/* ------------------------------------------------------------------------
+ * Output tables. The text files of the reference (hypersf.dat, sf_txyz.dat,
+ * pimnsf.dat, written by numpy.savetxt(fmt='%.6e', header=...),
+ * ideal.py:304-312, visc.py:413-419), written from a host array of rows x
+ * cols reals (precision 4 or 8) with the same bytes: '# ' + header + '\n'
+ * (no header line if header is null), then each row's values as %.6e
+ * separated by one space and ended by '\n'; NaN as "nan". Host code only:
+ * the rows are formatted by parallel host threads. */
+int clv_write_table(const char *path, const char *header, const void *data, int precision, long long rows, int cols);
+
 #ifdef __cplusplus
 }
 #endif
