@@ -149,7 +149,7 @@ int wgrad_tma(const WgradArgs& a, float* dw, int accumulate, int max_splits, cud
   const long long nchunks = (long long)a.N * (a.H / bh) * (a.W / bw);
   const long long cps = (nchunks + max_splits - 1) / max_splits;
   const int splits = (int)((nchunks + cps - 1) / cps);  // every split has pixel blocks
-  const int blocks = 9 * ((a.Cout + WGT_BM - 1) / WGT_BM) * ((a.Cin + WGT_BN - 1) / WGT_BN);
+  const int blocks = ((9 * a.Cin + WGT_BM - 1) / WGT_BM) * ((a.Cout + WGT_BN - 1) / WGT_BN);
   WgradArgs b = a;
   wgrad3x3_tma_kernel<<<dim3(blocks, splits), 128, sizeof(WgTmaSmem), s>>>(tg, tx, b, bw, (int)cps);
   int rc = clv_host::check_cuda("wgrad3x3_tma_kernel");

@@ -764,20 +764,20 @@ __global__ void __launch_bounds__(256) wgrad3x3_kernel(WgradArgs a) {
 
 // out[i] (+)= sum_s part[s][i], in s order
 // ------------------------------------------ wgrad 3x3, TMA + tcgen05 path
-// (selected by clv_unet_set_conv_path(3): on the surrogate's layers, whose
-// output channels are often 32 or 64 of the 128-row MMA, it is slower than
-// wgrad3x3_kernel.) The weight gradient on the 5th-generation tensor cores, for images whose
-// pixels tile into blocks of 32 (bw = min(W, 32) columns x 32 / bw rows): per
-// tap, D[co][ci] = sum over pixels p of g[p][co] x[p + tap][ci], M = 128
-// output channels (rows beyond Cout are TMA zero fill), N = up to 128 input
-// channels, K = 32-pixel blocks. Both operands are MN-major in the 64-byte
-// swizzled layout: [32 channels, bw, 32 / bw, 1] boxes of g and of x shifted
-// by the tap (the image border as zero fill). A CTA of 128 threads takes one
-// (tap, channel block) and a contiguous range of pixel blocks (split K):
+// (selected by clv_unet_set_conv_path(3).) The weight gradient on the
+// 5th-generation tensor cores, for images whose pixels tile into blocks of 32
+// (bw = min(W, 32) columns x 32 / bw rows):
+// D[(tap, ci)][co] = sum over pixels p of x[p + tap][ci] g[p][co], the rows
+// r = tap * Cin + ci of the [9 Cin][Cout] result in tiles of M = 128 (four
+// 32-channel groups, each a [32 channels, bw, 32 / bw, 1] box of x shifted by
+// its tap, the image border as zero fill), N = up to 128 output channels
+// ([32, bw, 32 / bw, 1] boxes of g), K = 32-pixel blocks; both operands are
+// MN-major in the 64-byte swizzled layout. A CTA of 128 threads takes one
+// (row tile, channel tile) and a contiguous range of pixel blocks (split K):
 // thread 0 loads with TMA into TC_STAGES stages, thread 32 issues the
 // tcgen05.mma and commits each stage back, and all four warps write the
-// accumulator (one output channel a thread) as an FP32 partial
-// [split][tap][ci][co] that reduce_partials_kernel adds in a fixed order.
+// accumulator (one row a thread) as an FP32 partial [split][9 Cin][Cout] that
+// reduce_partials_kernel adds in a fixed order.
 constexpr int WGT_BM = 128, WGT_BN = 128, WGT_BK = 32;
 
 struct WgTmaSmem {
@@ -794,12 +794,11 @@ __global__ void __launch_bounds__(128)
   extern __shared__ __align__(1024) unsigned char wgt_raw[];
   WgTmaSmem& s = *reinterpret_cast<WgTmaSmem*>(wgt_raw);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int mblocks = (a.Cout + WGT_BM - 1) / WGT_BM;
-  int t = blockIdx.x;
-  const int tap = t % 9;
-  t /= 9;
-  const int co0 = (t % mblocks) * WGT_BM, ci0 = (t / mblocks) * WGT_BN;
-  const int nn = min(WGT_BN, a.Cin - ci0);  // a multiple of 32
+  const int rows = 9 * a.Cin;
+  const int mblocks = (rows + WGT_BM - 1) / WGT_BM;
+  const int m0 = (blockIdx.x % mblocks) * WGT_BM, co0 = (blockIdx.x / mblocks) * WGT_BN;
+  const int nn = min(WGT_BN, a.Cout - co0);        // a multiple of 32
+  const int groups = min(4, (rows - m0) / 32);     // 32-row groups with data
   const int split = blockIdx.y;
   const int bh = WGT_BK / bw;
   const int per_row = a.W / bw, per_img = per_row * (a.H / bh);
@@ -841,13 +840,14 @@ __global__ void __launch_bounds__(128)
       const int h0 = (q / per_row) * bh, w0 = (q % per_row) * bw;
       const uint32_t fb = smem_u32(&s.full[st]);
       asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(fb),
-                   "r"((uint32_t)(WGT_BM + nn) * WGT_BK * 2)
+                   "r"((uint32_t)(groups * 32 + nn) * WGT_BK * 2)
                    : "memory");
       const uint32_t sa = smem_u32(s.A[st]), sb = smem_u32(s.B[st]);
-#pragma unroll
-      for (int i = 0; i < WGT_BM / 32; i++) tma_load4(sa + i * LBO, &tg, co0 + 32 * i, w0, h0, img, fb);
-      for (int i = 0; i < nn / 32; i++)
-        tma_load4(sb + i * LBO, &tx, a.x_co + ci0 + 32 * i, w0 + tap % 3 - 1, h0 + tap / 3 - 1, img, fb);
+      for (int gi = 0; gi < groups; gi++) {  // rows m0 + 32 gi ..: one tap, 32 input channels
+        const int r0 = m0 + 32 * gi, tap = r0 / a.Cin, ci = r0 % a.Cin;
+        tma_load4(sa + gi * LBO, &tx, a.x_co + ci, w0 + tap % 3 - 1, h0 + tap / 3 - 1, img, fb);
+      }
+      for (int ng = 0; ng < nn / 32; ng++) tma_load4(sb + ng * LBO, &tg, co0 + 32 * ng, w0, h0, img, fb);
     }
     // the loads in flight land before the CTA can exit
     for (long long c = it - 1; c >= 0 && c >= it - TC_STAGES; c--)
@@ -877,17 +877,27 @@ __global__ void __launch_bounds__(128)
   ready = __syncthreads_and(ready);
   if (!ready && tid == 0) atomicAdd(&g_tc_timeouts, 1);
   if (ready) {
-    const int co = co0 + warp * 32 + lane;
+    const int r = m0 + warp * 32 + lane;  // (tap, ci) row of this thread
     const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
-    float* out = a.part + ((long long)split * 9 + tap) * a.Cin * a.Cout;
+    float* out = a.part + ((long long)split * rows + r) * a.Cout + co0;
 #pragma unroll 1
     for (int c8 = 0; c8 < nn / 8; c8++) {
       uint32_t v[8];
       tc_ld8(trow + c8 * 8, v);
-      if (co < a.Cout)
-#pragma unroll
-        for (int jj = 0; jj < 8; jj++)
-          out[(long long)(ci0 + c8 * 8 + jj) * a.Cout + co] = c1 > c0 ? __uint_as_float(v[jj]) : 0.0f;
+      if (r < rows) {
+        float4 lo, hi;
+        const bool any = c1 > c0;
+        lo.x = any ? __uint_as_float(v[0]) : 0.0f;
+        lo.y = any ? __uint_as_float(v[1]) : 0.0f;
+        lo.z = any ? __uint_as_float(v[2]) : 0.0f;
+        lo.w = any ? __uint_as_float(v[3]) : 0.0f;
+        hi.x = any ? __uint_as_float(v[4]) : 0.0f;
+        hi.y = any ? __uint_as_float(v[5]) : 0.0f;
+        hi.z = any ? __uint_as_float(v[6]) : 0.0f;
+        hi.w = any ? __uint_as_float(v[7]) : 0.0f;
+        *reinterpret_cast<float4*>(out + c8 * 8) = lo;
+        *reinterpret_cast<float4*>(out + c8 * 8 + 4) = hi;
+      }
     }
   }
   tc_fence_before();
