@@ -109,8 +109,8 @@ template <int BN, bool SW> int launch_conv_tma(const ConvArgs& a, int bw, cudaSt
   return clv_host::check_cuda("conv3x3_tma_kernel");
 }
 
-// the weight gradient on tcgen05 when the pixels tile into 32-pixel blocks
-// (bw = min(W, 32) columns) and the channel counts are multiples of 32;
+// the weight gradient on tcgen05 when the pixels tile into 64-pixel blocks
+// (bw = min(W, 64) columns) and the channel counts are multiples of 32;
 // returns -1 when it does not apply
 int wgrad_tma(const WgradArgs& a, float* dw, int accumulate, int max_splits, cudaStream_t s) {
   const int bw = a.W >= WGT_BK ? WGT_BK : a.W;

@@ -766,31 +766,33 @@ __global__ void __launch_bounds__(256) wgrad3x3_kernel(WgradArgs a) {
 // ------------------------------------------ wgrad 3x3, TMA + tcgen05 path
 // (selected by clv_unet_set_conv_path(3).) The weight gradient on the
 // 5th-generation tensor cores, for images whose pixels tile into blocks of 32
-// (bw = min(W, 32) columns x 32 / bw rows):
+// (bw = min(W, 64) columns x 64 / bw rows):
 // D[(tap, ci)][co] = sum over pixels p of x[p + tap][ci] g[p][co], the rows
 // r = tap * Cin + ci of the [9 Cin][Cout] result in tiles of M = 128 (four
-// 32-channel groups, each a [32 channels, bw, 32 / bw, 1] box of x shifted by
+// 32-channel groups, each a [32 channels, bw, 64 / bw, 1] box of x shifted by
 // its tap, the image border as zero fill), N = up to 128 output channels
-// ([32, bw, 32 / bw, 1] boxes of g), K = 32-pixel blocks; both operands are
+// ([32, bw, 64 / bw, 1] boxes of g), K = 64-pixel blocks; both operands are
 // MN-major in the 64-byte swizzled layout. A CTA of 128 threads takes one
 // (row tile, channel tile) and a contiguous range of pixel blocks (split K):
-// thread 0 loads with TMA into TC_STAGES stages, thread 32 issues the
+// thread 0 loads with TMA into WGT_STAGES stages, thread 32 issues the
 // tcgen05.mma and commits each stage back, and all four warps write the
 // accumulator (one row a thread) as an FP32 partial [split][9 Cin][Cout] that
 // reduce_partials_kernel adds in a fixed order.
-constexpr int WGT_BM = 128, WGT_BN = 128, WGT_BK = 32;
+constexpr int WGT_BM = 128, WGT_BN = 128, WGT_BK = 64, WGT_STAGES = 3;
 
 struct WgTmaSmem {
-  bf16 A[TC_STAGES][WGT_BM * WGT_BK];
-  bf16 B[TC_STAGES][WGT_BN * WGT_BK];
-  uint64_t full[TC_STAGES], empty[TC_STAGES], done;
+  bf16 A[WGT_STAGES][WGT_BM * WGT_BK];
+  bf16 B[WGT_STAGES][WGT_BN * WGT_BK];
+  uint64_t full[WGT_STAGES], empty[WGT_STAGES], done;
   uint32_t tmem;
 };
 
 __global__ void __launch_bounds__(128)
     wgrad3x3_tma_kernel(const __grid_constant__ CUtensorMap tg, const __grid_constant__ CUtensorMap tx, WgradArgs a,
                         int bw, int chunks_per_split) {
-  constexpr uint32_t LBO = 2048, SBO = 512, KSTEP = 1024, LAYOUT = 4;  // MN-major, 64-byte swizzle
+  // MN-major, 64-byte swizzle: 32-channel groups (one box each) WGT_BK x 64 B apart, 8-row atoms 512 B,
+  // K step of 16 pixel rows 1024 B
+  constexpr uint32_t LBO = WGT_BK * 64, SBO = 512, KSTEP = 1024, LAYOUT = 4;
   extern __shared__ __align__(1024) unsigned char wgt_raw[];
   WgTmaSmem& s = *reinterpret_cast<WgTmaSmem*>(wgt_raw);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -815,7 +817,7 @@ __global__ void __launch_bounds__(128)
   }
   if (tid == 32) {
 #pragma unroll
-    for (int st = 0; st < TC_STAGES; st++) {
+    for (int st = 0; st < WGT_STAGES; st++) {
       asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&s.full[st])) : "memory");
       asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&s.empty[st])) : "memory");
     }
@@ -830,8 +832,8 @@ __global__ void __launch_bounds__(128)
   if (tid == 0) {  // TMA producer
     long long it = 0;
     for (long long c = c0; c < c1; c++, it++) {
-      const int st = (int)(it % TC_STAGES);
-      const long long j = it / TC_STAGES;
+      const int st = (int)(it % WGT_STAGES);
+      const long long j = it / WGT_STAGES;
       if (j >= 1 && !tc_wait(smem_u32(&s.empty[st]), (uint32_t)((j - 1) & 1))) {
         atomicAdd(&g_tc_timeouts, 1);
         break;
@@ -850,14 +852,14 @@ __global__ void __launch_bounds__(128)
       for (int ng = 0; ng < nn / 32; ng++) tma_load4(sb + ng * LBO, &tg, co0 + 32 * ng, w0, h0, img, fb);
     }
     // the loads in flight land before the CTA can exit
-    for (long long c = it - 1; c >= 0 && c >= it - TC_STAGES; c--)
-      tc_wait(smem_u32(&s.full[c % TC_STAGES]), (uint32_t)((c / TC_STAGES) & 1));
+    for (long long c = it - 1; c >= 0 && c >= it - WGT_STAGES; c--)
+      tc_wait(smem_u32(&s.full[c % WGT_STAGES]), (uint32_t)((c / WGT_STAGES) & 1));
   } else if (tid == 32) {  // MMA issuer
     long long it = 0;
     bool ok = true;
     for (long long c = c0; c < c1; c++, it++) {
-      const int st = (int)(it % TC_STAGES);
-      if (!tc_wait(smem_u32(&s.full[st]), (uint32_t)((it / TC_STAGES) & 1))) {
+      const int st = (int)(it % WGT_STAGES);
+      if (!tc_wait(smem_u32(&s.full[st]), (uint32_t)((it / WGT_STAGES) & 1))) {
         ok = false;
         atomicAdd(&g_tc_timeouts, 1);
         break;
