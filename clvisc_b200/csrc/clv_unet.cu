@@ -34,8 +34,9 @@ int wgrad_splits(long long P, int Cin, int Cout) {
 }
 constexpr int kRowBlocks = 148 * 2;
 
-// clv_unet_set_conv_path: 1 tcgen05 convolutions (default), 2 the same with no-swizzle TMA operands,
-// 3 tcgen05 convolutions and weight gradient, 0 mma.sync
+// clv_unet_set_conv_path: 1 tcgen05 convolutions and weight gradient (default), 2 tcgen05 convolutions
+// with no-swizzle TMA operands and the mma.sync weight gradient, 3 tcgen05 convolutions and the mma.sync
+// weight gradient, 0 mma.sync for both
 int g_conv_path = 1;
 
 // cuTensorMapEncodeTiled from the driver (through the runtime, no link-time
@@ -147,9 +148,19 @@ int wgrad_tma(const WgradArgs& a, float* dw, int accumulate, int max_splits, cud
     configured = true;
   }
   const long long nchunks = (long long)a.N * (a.H / bh) * (a.W / bw);
-  const long long cps = (nchunks + max_splits - 1) / max_splits;
-  const int splits = (int)((nchunks + cps - 1) / cps);  // every split has pixel blocks
   const int blocks = ((9 * a.Cin + WGT_BM - 1) / WGT_BM) * ((a.Cout + WGT_BN - 1) / WGT_BN);
+  // one wave of resident CTAs (two an SM: shared memory), within the scratch
+  // the caller sized for max_splits
+  static int resident = 0;
+  if (!resident) {
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    resident = std::max(1, sms) * std::max(1, (228 * 1024) / ((int)sizeof(WgTmaSmem) + 1024));
+  }
+  const long long want = std::max(1, std::min(max_splits, resident / blocks));
+  const long long cps = (nchunks + want - 1) / want;
+  const int splits = (int)((nchunks + cps - 1) / cps);  // every split has pixel blocks
   WgradArgs b = a;
   wgrad3x3_tma_kernel<<<dim3(blocks, splits), 128, sizeof(WgTmaSmem), s>>>(tg, tx, b, bw, (int)cps);
   int rc = clv_host::check_cuda("wgrad3x3_tma_kernel");
@@ -238,7 +249,7 @@ int clv_unet_wgrad3x3(const void* x, int x_cs, int x_co, const void* g, int N, i
   a.Cout = Cout;
   const long long P = (long long)N * H * W;
   const int s = wgrad_splits(P, Cin, Cout);
-  if (g_conv_path == 3) {  // tcgen05 where the pixels tile into 32-pixel blocks
+  if (g_conv_path == 1) {  // tcgen05 where the pixels tile into 64-pixel blocks
     const int rc = wgrad_tma(a, dw, accumulate, s, S(stream));
     if (rc != -1) return rc;
   }

@@ -764,7 +764,8 @@ __global__ void __launch_bounds__(256) wgrad3x3_kernel(WgradArgs a) {
 
 // out[i] (+)= sum_s part[s][i], in s order
 // ------------------------------------------ wgrad 3x3, TMA + tcgen05 path
-// (selected by clv_unet_set_conv_path(3).) The weight gradient on the
+// (the default path; wgrad3x3_kernel takes images that do not tile and the
+// mma.sync paths.) The weight gradient on the
 // 5th-generation tensor cores, for images whose pixels tile into blocks of 32
 // (bw = min(W, 64) columns x 64 / bw rows):
 // D[(tap, ci)][co] = sum over pixels p of x[p + tap][ci] g[p][co], the rows

@@ -366,13 +366,13 @@ typedef struct clv_unet_conv {
   int gelu;
 } clv_unet_conv;
 int clv_unet_conv3x3(const clv_unet_conv *args, void *stream);
-/* Tensor-core paths (process-wide): 1 = clv_unet_conv3x3 on tcgen05.mma with
- * the accumulator in tensor memory (the default; operands by TMA in the
+/* Tensor-core paths (process-wide). 1 (the default): clv_unet_conv3x3 on
+ * tcgen05.mma with the accumulator in tensor memory (operands by TMA in the
  * 64-byte swizzled layout when the image tiles into 128-pixel blocks, else by
- * cp.async) and clv_unet_wgrad3x3 on mma.sync; 2 = the same with no-swizzle
- * TMA operands; 3 = as 1, and clv_unet_wgrad3x3 on tcgen05 too where the
- * pixels tile into 32-pixel blocks (slower than mma.sync on the surrogate's
- * layers); 0 = mma.sync for both. */
+ * cp.async) and clv_unet_wgrad3x3 on tcgen05 with TMA operands where the
+ * pixels tile into 64-pixel blocks (else mma.sync); 3 = the same convolution
+ * with the weight gradient on mma.sync; 2 = as 3 with no-swizzle TMA
+ * operands; 0 = mma.sync for both. */
 int clv_unet_set_conv_path(int path);
 /* Bounded waits of the tcgen05 convolutions that ran out since the last
  * reset (0 in a healthy run; a tile whose wait ran out writes no output).

@@ -31,7 +31,7 @@ def _rel(a, b):
     return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30)
 
 
-@pytest.fixture(params=[1, 2, 3, 0], ids=['tcgen05', 'tcgen05-noswizzle', 'tcgen05-wgrad', 'mma.sync'])
+@pytest.fixture(params=[1, 2, 3, 0], ids=['tcgen05', 'tcgen05-noswizzle', 'tcgen05-conv-only', 'mma.sync'])
 def conv_path(request, cuda_lib):
     from clvisc_b200 import _lib
     lib = _lib.load()
@@ -119,9 +119,9 @@ def test_conv3x3_paths_agree(cuda_lib, N, H, W):
 @pytest.mark.parametrize('cin,cout', [(32, 32), (96, 64), (128, 256), (192, 32)])
 @pytest.mark.parametrize('N,H,W', [(3, 16, 24), (2, 8, 32), (2, 8, 16), (1, 2, 64)])
 def test_wgrad3x3(cuda_lib, conv_path, cin, cout, N, H, W):
-    """Weight gradient against the oracle; with the tcgen05 weight-gradient
-    path, images whose pixels tile into 64-pixel blocks (W = 32, 16, 64 here)
-    take the TMA + tcgen05 kernel, the others (W = 24) the mma.sync kernel."""
+    """Weight gradient against the oracle; on the default path, images whose
+    pixels tile into 64-pixel blocks (W = 32, 16, 64 here) take the TMA +
+    tcgen05 kernel, the others (W = 24) the mma.sync kernel."""
     from clvisc_b200 import _lib
     lib = _lib.load()
     rng = np.random.default_rng(7)
