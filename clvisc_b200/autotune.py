@@ -1,7 +1,7 @@
 """Autotuner of the fused viscous stage's launch shape for one event.
 
 The tiled stage kernel takes its (y, eta) tile from a compile-time set
-(8 x 32 or 16 x 16, CLV_OPT_TILE) and its x extent per block at run time
+(8 x 32, 16 x 16 or 8 x 16, CLV_OPT_TILE) and its x extent per block at run time
 (CLV_OPT_CHUNK); the per-cell kernel is the alternative on any grid. Every
 variant computes the same bits. tune_visc() times each candidate for a few
 fused steps on the run's own state, saved before and restored after each, and
@@ -30,7 +30,7 @@ def candidates(nz, use_float32=True):
     cells along eta."""
     out = [dict(DEFAULTS, kernel=1)]
     blocks = (2, 1) if use_float32 else (1,)
-    for tile in (0, 1):
+    for tile in (0, 1, 2):
         for chunk in (16, 24, 32, 48):
             for b in blocks[:1]:
                 out.append({'kernel': 2, 'tile': tile, 'chunk': chunk, 'blocks': b})

@@ -24,7 +24,7 @@ constexpr int kTiledMinNz = 24;  // fewer cells along eta: per-cell kernel
 constexpr int kTiled2dMin = 4;   // (2+1)D tiles: at least this many cells along x and y
 int g_chunk = 32;        // CLV_OPT_CHUNK: x planes per tiled CTA
 int g_minb = 2;          // CLV_OPT_TILED_BLOCKS: resident tiled CTAs per SM (FP32)
-int g_tile = 0;          // CLV_OPT_TILE: 0 = 8 x 32, 1 = 16 x 16 (y, eta) tile of the fused stage
+int g_tile = 0;          // CLV_OPT_TILE: 0 = 8 x 32, 1 = 16 x 16, 2 = 8 x 16 (y, eta) tile of the fused stage
 int g_rows2d = 64;       // CLV_OPT_TILE2D_ROWS: threads of a (2+1)D tile block (64 or 128)
 int g_chunk2d = 8;       // CLV_OPT_CHUNK2D: x planes per (2+1)D tile
 
@@ -155,7 +155,13 @@ int launch_tiled(const clv::Params& p, const clv::ViscBuffers<real>& v, int step
   // default kernel does not carry their code
   const bool cpl = IS && (p.flags & (clv::FLAG_GUBSER_VISC | clv::FLAG_PIMN_OMEGA | clv::FLAG_OMEGA_OMEGA));
   if (cpl) return launch_tiled_b<real, IS, KT, IS, 1>(p, v, step, tau, s);
-  // the fused stage also comes with a 16 x 16 (y, eta) tile (CLV_OPT_TILE)
+  // the fused stage also comes with 16 x 16 and 8 x 16 (y, eta) tiles
+  // (CLV_OPT_TILE); the 128-thread 8 x 16 tile keeps 4 CTAs an SM at 128
+  // registers (FP32; 2 at 255 with CLV_OPT_TILED_BLOCKS = 1, and in FP64)
+  if (IS && KT && g_tile == 2) {
+    if (sizeof(real) == 8 || g_minb == 1) return launch_tiled_b<real, IS, KT, false, 2, 8, 16>(p, v, step, tau, s);
+    return launch_tiled_b<real, IS, KT, false, 4, 8, 16>(p, v, step, tau, s);
+  }
   if (IS && KT && g_tile == 1) {
     if (sizeof(real) == 8 || g_minb == 1) return launch_tiled_b<real, IS, KT, false, 1, 16, 16>(p, v, step, tau, s);
     return launch_tiled_b<real, IS, KT, false, 2, 16, 16>(p, v, step, tau, s);
@@ -299,7 +305,7 @@ int clv_set_option(int option, int value) {
     g_minb = value;
     return CLV_OK;
   }
-  if (option == CLV_OPT_TILE && (value == 0 || value == 1)) {
+  if (option == CLV_OPT_TILE && value >= 0 && value <= 2) {
     g_tile = value;
     return CLV_OK;
   }

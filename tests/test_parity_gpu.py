@@ -93,8 +93,8 @@ def test_visc_parts_parity(cuda_lib, oracle_mod, use_float32, grid, stage_varian
         _compare_visc(v, o, 'parts n=%d' % n)
 
 
-@pytest.fixture(params=['auto', 'tiled', 'tiled-1blk', 'tiled-chunk5', 'tiled16', 'per-cell', 'tiled2d',
-                        'tiled2d-128-c3'])
+@pytest.fixture(params=['auto', 'tiled', 'tiled-1blk', 'tiled-chunk5', 'tiled16', 'tiled8x16', 'tiled8x16-1blk',
+                        'per-cell', 'tiled2d', 'tiled2d-128-c3'])
 def stage_variant(request, cuda_lib):
     """Every viscous-stage kernel variant; restores the default afterwards.
     (tiled2d: the tiled (2+1)D kernel on one-cell eta grids, 64-thread tiles
@@ -103,6 +103,8 @@ def stage_variant(request, cuda_lib):
     tiled = (_lib.CLV_OPT_STAGE_KERNEL, 2)  # tiled on every grid, short eta axes included
     opts = {'auto': [], 'tiled': [tiled], 'tiled-1blk': [tiled, (_lib.CLV_OPT_TILED_BLOCKS, 1)],
             'tiled-chunk5': [tiled, (_lib.CLV_OPT_CHUNK, 5)], 'tiled16': [tiled, (_lib.CLV_OPT_TILE, 1)],
+            'tiled8x16': [tiled, (_lib.CLV_OPT_TILE, 2)],
+            'tiled8x16-1blk': [tiled, (_lib.CLV_OPT_TILE, 2), (_lib.CLV_OPT_TILED_BLOCKS, 1)],
             'per-cell': [(_lib.CLV_OPT_STAGE_KERNEL, 1)], 'tiled2d': [(_lib.CLV_OPT_STAGE_KERNEL, 3)],
             'tiled2d-128-c3': [(_lib.CLV_OPT_STAGE_KERNEL, 3), (_lib.CLV_OPT_TILE2D_ROWS, 128),
                                (_lib.CLV_OPT_CHUNK2D, 3)]}[request.param]
