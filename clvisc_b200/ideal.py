@@ -73,8 +73,19 @@ def add_visc_params(c, p):
     p.zetaos_tmin = float_literal(getattr(c, 'ZETAOS_TMIN', 0.1))
     if bulk:
         flags |= _lib.CLV_FLAG_BULK
+    if fast_arithmetic(c):
+        flags |= _lib.CLV_FLAG_FAST
     p.flags = flags
     return bulk
+
+
+def fast_arithmetic(c):
+    """Whether the fused viscous stage runs in the tolerance arithmetic
+    (CLV_FLAG_FAST): cfg.arithmetic 'fast', or 'auto' (the default) in FP32."""
+    mode = str(getattr(c, 'arithmetic', 'auto')).lower()
+    if mode not in ('auto', 'fast', 'exact'):
+        raise ValueError("cfg.arithmetic must be 'auto', 'fast' or 'exact', not %r" % mode)
+    return mode == 'fast' or (mode == 'auto' and bool(c.use_float32))
 
 
 def load_eos(cfg, handcrafted_eos, device):
@@ -200,6 +211,17 @@ class CLIdeal(object):
         aos = torch.empty((self.size, w), dtype=self.dtype, device=self.device)
         self._call('clv_soa_to_aos', _lib.ptr(t), _lib.ptr(aos), self.size, w, self.stream)
         return aos.cpu().numpy()
+
+    def field_from_host(self, t, arr):
+        """numpy (cells, w) -> the first w planes of an SoA field (the inverse
+        of field_to_host), e.g. d_ev[2] or d_pi[1] for a test's initial state."""
+        w = int(np.asarray(arr).shape[1])
+        if w > t.shape[0]:
+            raise ValueError('field has %d planes, array has %d columns' % (t.shape[0], w))
+        host = torch.from_numpy(np.ascontiguousarray(arr, dtype=self.cfg.real).reshape(self.size, w))
+        dev = host.to(self.device)
+        self._call('clv_aos_to_soa', _lib.ptr(dev), _lib.ptr(t), self.size, w, self.stream)
+        torch.cuda.current_stream(self.device).synchronize()
 
     def stepUpdate(self, step, jet_eloss_src=None):
         """One Runge-Kutta stage (ideal.py:211-255): d_ev[3-step] from
