@@ -39,9 +39,10 @@ ALG_BYTES_PER_CELL_UPDATE = 312
 SLAB_NZ = 16  # CPU-baseline sample: a 385 x 385 x 16 eta slab of the event
 
 
-def make_cfg(nz=NZ, out='/tmp/clv_bench', nx=NX, ny=NY, fp64=False):
+def make_cfg(nz=NZ, out='/tmp/clv_bench', nx=NX, ny=NY, fp64=False, arithmetic='auto'):
     from clvisc_b200.config import read_config, set_real
     cfg = read_config([])
+    cfg.arithmetic = arithmetic
     cfg.NX, cfg.NY, cfg.NZ = nx, ny, nz
     cfg.DX = cfg.DY = DX
     cfg.DZ = DZ
@@ -377,7 +378,7 @@ def run_gpu(args, rank, world, dist):
     dev = int(os.environ.get('LOCAL_RANK', 0))
     torch.cuda.set_device(dev)
     nx, ny, nz = args.grid
-    cfg = make_cfg(nz=nz, nx=nx, ny=ny, out='/tmp/clv_bench_r%d' % rank, fp64=args.fp64)
+    cfg = make_cfg(nz=nz, nx=nx, ny=ny, out='/tmp/clv_bench_r%d' % rank, fp64=args.fp64, arithmetic=args.arithmetic)
     ic = initial_condition(seed=5, nx=nx, ny=ny, nz=nz)
     v = CLVisc(cfg, gpu_id=dev)
     v.load_ini(ic)
@@ -491,6 +492,8 @@ def main():
     ap.add_argument('--surrogate-epochs', type=int, default=12)
     ap.add_argument('--surrogate-only', action='store_true', help='print only the surrogate experiment line')
     ap.add_argument('--fp64', action='store_true', help='the same workload in double precision')
+    ap.add_argument('--arithmetic', default='auto', choices=['auto', 'fast', 'exact'],
+                    help='fused-stage arithmetic (auto: fast in FP32, exact in FP64)')
     ap.add_argument('--evolve', action='store_true',
                     help='also evolve the whole event to freeze-out with the hypersurface (reported under "evolve")')
     ap.add_argument('--grid', type=lambda s: tuple(int(x) for x in s.split(',')), default=(NX, NY, NZ),

@@ -16,6 +16,7 @@ CLV_FLAG_GUBSER_VISC_TEST = 2
 CLV_FLAG_PIMN_OMEGA_COUPLING = 4
 CLV_FLAG_OMEGA_OMEGA_COUPLING = 8
 CLV_FLAG_BULK = 16
+CLV_FLAG_FAST = 32
 
 CLV_OPT_STAGE_KERNEL = 1
 CLV_OPT_TILE = 4
@@ -49,6 +50,8 @@ class ClvParams(ctypes.Structure):
         ('flags', ctypes.c_int),
         ('zetaos_max', ctypes.c_float), ('zetaos_t0', ctypes.c_float), ('zetaos_width', ctypes.c_float),
         ('zetaos_skew', ctypes.c_float), ('zetaos_tmin', ctypes.c_float),
+        ('opt_stage_kernel', ctypes.c_int), ('opt_chunk', ctypes.c_int), ('opt_tiled_blocks', ctypes.c_int),
+        ('opt_tile', ctypes.c_int),
     ]
 
 
@@ -88,6 +91,8 @@ _SIGS = {
     'clv_max_ed': ([_P, _VP, _VP, _VP], ctypes.c_int),
     'clv_max_ed_read': ([_P, _VP, ctypes.POINTER(ctypes.c_double), _VP], ctypes.c_int),
     'clv_hypersf_scratch_bytes': ([_P], ctypes.c_size_t),
+    'clv_status': ([_P, _VP, _VP, ctypes.c_int, _VP, _VP, ctypes.c_longlong, _VP, _VP, _VP], ctypes.c_int),
+    'clv_params_size': ([], ctypes.c_size_t),
     'clv_hypersf_append': ([_P, ctypes.c_int, ctypes.c_double, ctypes.c_double, _VP, _VP, _VP, _VP, _VP, _VP, _VP,
                             ctypes.c_longlong, _VP, _VP, ctypes.c_size_t, _VP], ctypes.c_int),
     'clv_hypersf_append_noalloc': ([_P, ctypes.c_int, ctypes.c_double, ctypes.c_double, _VP, _VP, _VP, _VP, _VP,

@@ -2,7 +2,9 @@
 
 The library is compiled without fused multiply-add contraction and with IEEE
 division and square root, so each kernel's arithmetic matches a plain
-evaluation of the reference OpenCL source in the same precision. The
+evaluation of the reference OpenCL source in the same precision; the one
+exception is clv_fast.cu, the tolerance-arithmetic stage (CLV_FLAG_FAST),
+compiled with contraction and approximate division and square root. The
 translation units compile in parallel into objects under _build/ and are then
 linked into one shared library.
 
@@ -19,17 +21,26 @@ ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, 'libclvisc_b200.so')
 OBJDIR = os.path.join(HERE, '_build')
 SOURCES = ['csrc/clv_capi.cu', 'csrc/clv_noalloc.cu', 'csrc/clv_batch.cu', 'csrc/clv_initial.cu',
-           'csrc/clv_bulkinfo.cu', 'csrc/clv_spectra.cu', 'csrc/clv_unet.cu', 'csrc/clv_io.cu']
+           'csrc/clv_bulkinfo.cu', 'csrc/clv_spectra.cu', 'csrc/clv_unet.cu', 'csrc/clv_io.cu',
+           'csrc/clv_fast.cu']
 DEPS = ['csrc/clv_device.cuh', 'csrc/clv_stage.cuh', 'csrc/clv_stage_tiled.cuh', 'csrc/clv_stage_tiled2d.cuh',
         'csrc/clv_misc.cuh',
         'csrc/clv_hypersf.cuh', 'csrc/clv_batch.cuh', 'csrc/clv_initial.cuh',
-        'csrc/clv_bulkinfo.cuh', 'csrc/clv_spectra.cuh', 'csrc/clv_unet.cuh',
+        'csrc/clv_bulkinfo.cuh', 'csrc/clv_spectra.cuh', 'csrc/clv_unet.cuh', 'csrc/clv_fast.h',
         '../include/clvisc_b200.h']
 
 NVCC_FLAGS = [
     '-gencode', 'arch=compute_100a,code=sm_100a',
     '-O3', '-lineinfo', '-std=c++17',
     '--fmad=false', '-prec-div=true', '-prec-sqrt=true', '-ftz=false',
+    '-Xcompiler', '-fPIC',
+]
+# the tolerance-arithmetic stage (CLV_FLAG_FAST): contraction and approximate
+# division / square root in its own translation unit
+FAST_FLAGS = [
+    '-gencode', 'arch=compute_100a,code=sm_100a',
+    '-O3', '-lineinfo', '-std=c++17',
+    '--fmad=true', '-prec-div=false', '-prec-sqrt=false', '-ftz=false',
     '-Xcompiler', '-fPIC',
 ]
 
@@ -56,7 +67,8 @@ def build(force=False, verbose=False, extra=()):
 
     def compile_one(src_obj):
         src, obj = src_obj
-        cmd = [nvcc()] + NVCC_FLAGS + list(extra) + ['-c', '-o', obj, os.path.join(HERE, src)]
+        flags = FAST_FLAGS if src.endswith('clv_fast.cu') else NVCC_FLAGS
+        cmd = [nvcc()] + flags + list(extra) + ['-c', '-o', obj, os.path.join(HERE, src)]
         if verbose:
             print(' '.join(cmd), flush=True)
         r = subprocess.run(cmd, cwd=HERE, capture_output=True, text=True)

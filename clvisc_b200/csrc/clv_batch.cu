@@ -16,6 +16,13 @@ namespace {
 
 inline cudaStream_t S(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 
+// the current device (launch set-up is cached per device), or -1
+constexpr int kMaxDevices = 64;
+inline int current_device() {
+  int d = 0;
+  return (cudaGetDevice(&d) == cudaSuccess && d >= 0 && d < kMaxDevices) ? d : -1;
+}
+
 static_assert(sizeof(clv_batch_event) == sizeof(clv::BatchEvent), "clv_batch_event layout");
 static_assert(sizeof(clv_batch_ctl) == sizeof(clv::BatchCtl), "clv_batch_ctl layout");
 
@@ -118,11 +125,13 @@ template <class real, bool BULK, int TB>
 int launch_tiled(const clv::Params& p, const clv::BatchArgs<real>& a, int step, int chunk, int grid, cudaStream_t s) {
   typedef clv::Tile2Smem<real, BULK, TB> SM;
   auto kern = clv::batch_tiled2d_kernel<real, BULK, TB, clv::tiled2d_minb<real, TB>()>;
-  static bool configured = false;
-  if (!configured) {
+  static bool configured[kMaxDevices] = {};  // launch attributes are per device
+  const int cdev = current_device();
+  if (cdev < 0) return clv_host::check_cuda("cudaGetDevice");
+  if (!configured[cdev]) {
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SM)) != cudaSuccess)
       return clv_host::check_cuda("cudaFuncSetAttribute(batch_tiled2d_kernel)");
-    configured = true;
+    configured[cdev] = true;
   }
   if (grid <= 0) {
     int dev = 0, sms = 0, per_sm = 0;

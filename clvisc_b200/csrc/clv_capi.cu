@@ -11,6 +11,7 @@
 #include "clv_stage.cuh"
 #include "clv_stage_tiled.cuh"
 #include "clv_stage_tiled2d.cuh"
+#include "clv_fast.h"
 
 namespace clv_host {
 thread_local std::string g_err;  // message behind clv_last_error()
@@ -45,6 +46,7 @@ int cuda_check(const char* where) {
 inline cudaStream_t S(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 
 constexpr int kAlign = 16;
+constexpr int kMaxDev = 64;  // devices tracked by the per-device launch set-up
 inline bool aligned(const void* q) { return (reinterpret_cast<uintptr_t>(q) % kAlign) == 0; }
 
 int to_params(const clv_params* in, clv::Params* out) {
@@ -72,6 +74,10 @@ int to_params(const clv_params* in, clv::Params* out) {
   p.flags = in->flags;
   p.ZETAOS_MAX = in->zetaos_max; p.ZETAOS_T0 = in->zetaos_t0;
   p.ZETAOS_WIDTH = in->zetaos_width; p.ZETAOS_SKEW = in->zetaos_skew; p.ZETAOS_TMIN = in->zetaos_tmin;
+  p.opt[0] = in->opt_stage_kernel; p.opt[1] = in->opt_chunk; p.opt[2] = in->opt_tiled_blocks; p.opt[3] = in->opt_tile;
+  if (in->opt_stage_kernel < 0 || in->opt_stage_kernel > 4 || in->opt_chunk < 0 || in->opt_chunk > 4096 ||
+      in->opt_tiled_blocks < 0 || in->opt_tiled_blocks > 2 || in->opt_tile < 0 || in->opt_tile > 3)
+    return fail(CLV_ERR_INVALID, "opt_* fields out of range%s");
   if ((in->flags & CLV_FLAG_BULK) && (!(in->zetaos_width > 0.0f) || !(in->zetaos_max >= 0.0f)))
     return fail(CLV_ERR_INVALID, "bulk sector: zetaos_width must be > 0 and zetaos_max >= 0%s");
   // correctly rounded reciprocals in each precision (host IEEE arithmetic, no
@@ -110,17 +116,31 @@ clv::TauConst<real> tau_const(const clv::Params& p, double tau_d) {
 inline long long ncell(const clv::Params& p) { return (long long)p.nx * p.ny * p.nz; }
 inline unsigned int nblk(long long n, int bs) { return (unsigned int)((n + bs - 1) / bs); }
 
+// the stage launch choices of a run: its own opt_* fields where set, else the
+// process-wide settings of clv_set_option
+clv::StageOpts stage_opts(const clv::Params& p) {
+  clv::StageOpts o;
+  o.stage_kernel = p.opt[0] ? p.opt[0] - 1 : g_stage_kernel;
+  o.chunk = p.opt[1] ? p.opt[1] : g_chunk;
+  o.minb = p.opt[2] ? p.opt[2] : g_minb;
+  o.tile = p.opt[3] ? p.opt[3] - 1 : g_tile;
+  return o;
+}
+
 template <class real, bool IS, bool KT, bool CPL, int MINB, int TJ = 8, int TK = 32>
-int launch_tiled_b(const clv::Params& p, const clv::ViscBuffers<real>& v, int step, double tau, cudaStream_t s) {
+int launch_tiled_b(const clv::Params& p, const clv::ViscBuffers<real>& v, int step, double tau, cudaStream_t s,
+                   const clv::StageOpts& o) {
   typedef clv::TileSmem<real, TJ, TK> SM;
   auto kern = clv::visc_stage_tiled_kernel<real, IS, KT, CPL, TJ, TK, MINB>;
-  static bool configured = false;
-  if (!configured) {
+  static bool configured[kMaxDev] = {};  // the attribute is per device
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDev) return cuda_check("cudaGetDevice");
+  if (!configured[dev]) {
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SM)) != cudaSuccess)
       return cuda_check("cudaFuncSetAttribute(visc_stage_tiled_kernel)");
-    configured = true;
+    configured[dev] = true;
   }
-  const int chunk = g_chunk;
+  const int chunk = o.chunk;
   dim3 grid((p.nz + TK - 1) / TK, (p.ny + TJ - 1) / TJ, (p.nx + chunk - 1) / chunk);
   kern<<<grid, TJ * TK, sizeof(SM), s>>>(p, v, step, tau_const<real>(p, tau), chunk);
   return cuda_check("visc_stage_tiled_kernel");
@@ -130,11 +150,13 @@ template <class real, bool BULK, int TB>
 int launch_tiled2d_b(const clv::Params& p, const clv::ViscBuffers<real>& v, int step, double tau, cudaStream_t s) {
   typedef clv::Tile2Smem<real, BULK, TB> SM;
   auto kern = clv::visc_stage_tiled2d_kernel<real, BULK, TB, clv::tiled2d_minb<real, TB>()>;
-  static bool configured = false;
-  if (!configured) {
+  static bool configured[kMaxDev] = {};  // the attribute is per device
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDev) return cuda_check("cudaGetDevice");
+  if (!configured[dev]) {
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SM)) != cudaSuccess)
       return cuda_check("cudaFuncSetAttribute(visc_stage_tiled2d_kernel)");
-    configured = true;
+    configured[dev] = true;
   }
   const int chunk = g_chunk2d;
   dim3 grid((p.ny + TB - 5) / (TB - 4), (p.nx + chunk - 1) / chunk);
@@ -149,25 +171,28 @@ int launch_tiled2d(const clv::Params& p, const clv::ViscBuffers<real>& v, int st
 }
 
 template <class real, bool IS, bool KT>
-int launch_tiled(const clv::Params& p, const clv::ViscBuffers<real>& v, int step, double tau, cudaStream_t s) {
+int launch_tiled(const clv::Params& p, const clv::ViscBuffers<real>& v, int step, double tau, cudaStream_t s,
+                 const clv::StageOpts& o) {
   // the coupling terms (GUBSER_VISC_TEST, PIMUNU_OMEGA_COUPLING,
   // OMEGA_OMEGA_COUPLING) live in a separate instantiation so that the
   // default kernel does not carry their code
   const bool cpl = IS && (p.flags & (clv::FLAG_GUBSER_VISC | clv::FLAG_PIMN_OMEGA | clv::FLAG_OMEGA_OMEGA));
-  if (cpl) return launch_tiled_b<real, IS, KT, IS, 1>(p, v, step, tau, s);
+  if (cpl) return launch_tiled_b<real, IS, KT, IS, 1>(p, v, step, tau, s, o);
   // the fused stage also comes with 16 x 16 and 8 x 16 (y, eta) tiles
   // (CLV_OPT_TILE); the 128-thread 8 x 16 tile keeps 4 CTAs an SM at 128
   // registers (FP32; 2 at 255 with CLV_OPT_TILED_BLOCKS = 1, and in FP64)
-  if (IS && KT && g_tile == 2) {
-    if (sizeof(real) == 8 || g_minb == 1) return launch_tiled_b<real, IS, KT, false, 2, 8, 16>(p, v, step, tau, s);
-    return launch_tiled_b<real, IS, KT, false, 4, 8, 16>(p, v, step, tau, s);
+  constexpr bool dbl = sizeof(real) == 8;
+  if (IS && KT && o.tile == 2) {
+    if (dbl || o.minb == 1) return launch_tiled_b<real, IS, KT, false, 2, 8, 16>(p, v, step, tau, s, o);
+    if constexpr (!dbl) return launch_tiled_b<real, IS, KT, false, 4, 8, 16>(p, v, step, tau, s, o);
   }
-  if (IS && KT && g_tile == 1) {
-    if (sizeof(real) == 8 || g_minb == 1) return launch_tiled_b<real, IS, KT, false, 1, 16, 16>(p, v, step, tau, s);
-    return launch_tiled_b<real, IS, KT, false, 2, 16, 16>(p, v, step, tau, s);
+  if (IS && KT && o.tile == 1) {
+    if (dbl || o.minb == 1) return launch_tiled_b<real, IS, KT, false, 1, 16, 16>(p, v, step, tau, s, o);
+    if constexpr (!dbl) return launch_tiled_b<real, IS, KT, false, 2, 16, 16>(p, v, step, tau, s, o);
   }
-  if (sizeof(real) == 8 || g_minb == 1) return launch_tiled_b<real, IS, KT, false, 1>(p, v, step, tau, s);
-  return launch_tiled_b<real, IS, KT, false, 2>(p, v, step, tau, s);
+  if (dbl || o.minb == 1) return launch_tiled_b<real, IS, KT, false, 1>(p, v, step, tau, s, o);
+  if constexpr (!dbl) return launch_tiled_b<real, IS, KT, false, 2>(p, v, step, tau, s, o);
+  return CLV_ERR_INVALID;  // not reached
 }
 
 template <class real>
@@ -181,6 +206,7 @@ int visc_stage_t(const clv::Params& p, int step, double tau, int parts, const cl
   v.edmax_key = (typename clv::KeyT<real>::type*)b->edmax_key;
   v.write_src = b->write_src; v.write_udiff = b->write_udiff;
   const bool is = parts & CLV_PART_IS, kt = parts & CLV_PART_KT;
+  const clv::StageOpts o = stage_opts(p);
   if (!v.ev_st || !v.pi_st || !v.ev1 || !v.src) return fail(CLV_ERR_INVALID, "visc stage: null stencil/src buffer%s");
   if (is && (!v.pi1 || !v.pinew || !v.udiff || !v.goodcell || (step == 1 && !v.ev2e)))
     return fail(CLV_ERR_INVALID, "visc stage: null buffer for the pi update%s");
@@ -188,18 +214,20 @@ int visc_stage_t(const clv::Params& p, int step, double tau, int parts, const cl
   if (v.write_udiff && (!kt || !v.udiff)) return fail(CLV_ERR_INVALID, "visc stage: write_udiff needs CLV_PART_KT%s");
   const bool bulk = p.flags & clv::FLAG_BULK;
   const bool cpl0 = p.flags & (clv::FLAG_GUBSER_VISC | clv::FLAG_PIMN_OMEGA | clv::FLAG_OMEGA_OMEGA);
+  // tolerance arithmetic (CLV_FLAG_FAST) for the fused stage
+  if ((p.flags & clv::FLAG_FAST) && is && kt) return clv_fastpath::visc_stage<real>(p, v, step, tau_const<real>(p, tau), o, s);
   // the tiled (2+1)D kernel (bulk sector, no coupling terms) when asked for:
   // on B200 the per-cell kernel is faster on the (2+1)D grids of this code
   const bool fit2d = p.nz == 1 && p.nx >= kTiled2dMin && p.ny >= kTiled2dMin && is && kt && !cpl0;
-  if (fit2d && g_stage_kernel == 3)
+  if (fit2d && o.stage_kernel == 3)
     return bulk ? launch_tiled2d<real, true>(p, v, step, tau, s) : launch_tiled2d<real, false>(p, v, step, tau, s);
   // The tiled kernel has no bulk sector, and its 8 x 32 (y, eta) tile leaves
   // most threads idle on grids with few cells along eta ((2+1)D runs have
   // one): those runs take the per-cell kernel, which gives the same bits.
-  if (!bulk && (g_stage_kernel == 2 || (g_stage_kernel == 0 && p.nz >= kTiledMinNz))) {
-    if (is && kt) return launch_tiled<real, true, true>(p, v, step, tau, s);
-    if (is) return launch_tiled<real, true, false>(p, v, step, tau, s);
-    return launch_tiled<real, false, true>(p, v, step, tau, s);
+  if (!bulk && (o.stage_kernel == 2 || (o.stage_kernel == 0 && p.nz >= kTiledMinNz))) {
+    if (is && kt) return launch_tiled<real, true, true>(p, v, step, tau, s, o);
+    if (is) return launch_tiled<real, true, false>(p, v, step, tau, s, o);
+    return launch_tiled<real, false, true>(p, v, step, tau, s, o);
   }
   const int bs = 128;
   dim3 grid(nblk(ncell(p), bs));
@@ -413,6 +441,35 @@ int clv_max_ed_read(const clv_params* pp, const void* key, double* out, void* st
   }
   return CLV_OK;
 }
+
+int clv_status(const clv_params* pp, const void* ev, const void* pi, int npi, const unsigned char* goodcell,
+               const long long* sf_total, long long sf_capacity, long long* counts_dev, long long* counts_host,
+               void* stream) {
+  clv::Params p;
+  int rc = to_params(pp, &p);
+  if (rc) return rc;
+  if (!ev || !counts_dev || (pi && (npi < 1 || npi > 11)) || sf_capacity < 0)
+    return fail(CLV_ERR_INVALID, "status: bad argument%s");
+  const long long n = ncell(p);
+  unsigned int g = nblk(n, 256);
+  if (g > 148u * 8u) g = 148u * 8u;
+  unsigned long long* out = reinterpret_cast<unsigned long long*>(counts_dev);
+  cudaMemsetAsync(out, 0, 3 * sizeof(unsigned long long), S(stream));
+  if (pp->precision == 4) {
+    clv::status_kernel<float><<<g, 256, 0, S(stream)>>>((const float*)ev, 4, p.ld, n, goodcell, sf_total, sf_capacity, out);
+    if (pi) clv::status_kernel<float><<<g, 256, 0, S(stream)>>>((const float*)pi, npi, p.ld, n, nullptr, nullptr, 0, out);
+  } else {
+    clv::status_kernel<double><<<g, 256, 0, S(stream)>>>((const double*)ev, 4, p.ld, n, goodcell, sf_total, sf_capacity, out);
+    if (pi) clv::status_kernel<double><<<g, 256, 0, S(stream)>>>((const double*)pi, npi, p.ld, n, nullptr, nullptr, 0, out);
+  }
+  rc = cuda_check("status_kernel");
+  if (rc || !counts_host) return rc;
+  cudaMemcpyAsync(counts_host, counts_dev, 3 * sizeof(long long), cudaMemcpyDeviceToHost, S(stream));
+  cudaStreamSynchronize(S(stream));
+  return cuda_check("status readback");
+}
+
+size_t clv_params_size(void) { return sizeof(clv_params); }
 
 size_t clv_hypersf_scratch_bytes(const clv_params* pp) {
   clv::Params p;

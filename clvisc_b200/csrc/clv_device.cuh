@@ -6,9 +6,27 @@
 // compiled with --fmad=false and IEEE division/square root, so each cell's
 // result is bit-identical to a straightforward evaluation of the reference
 // source in the same precision.
+//
+// Compiled with CLV_FAST=1 (the tolerance build, clv_fast.cu: FMA
+// contraction, approximate division and square root) the same headers give the
+// fast arithmetic: division by run constants through their reciprocals, the
+// EOS texel index straight from e / step, the limiters in sign-test form and
+// the KT speed max(lambda, 1) taken as 1 (lambda <= 1 for |v| < 1 and
+// c_s^2 <= 1). Functions and kernels live in an inline namespace named after
+// the arithmetic (clv::exact or clv::fast), so both builds link into one
+// library; plain structs are shared.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
+
+#ifndef CLV_FAST
+#define CLV_FAST 0
+#endif
+#if CLV_FAST
+#define CLV_ARITH fast
+#else
+#define CLV_ARITH exact
+#endif
 
 namespace clv {
 
@@ -36,10 +54,13 @@ struct Params {
   float ZETAOS_TMIN;  // Pi = 0 in cells colder than this
   Recips<float> rf;   // reciprocals for float kernels
   Recips<double> rd;  // reciprocals for double kernels
+  int opt[4];         // the run's own stage_kernel+1, chunk, tiled blocks, tile+1 (0: process-wide)
 };
+inline namespace CLV_ARITH {
 template <class real> __device__ __forceinline__ const Recips<real>& recips(const Params& p);
 template <> __device__ __forceinline__ const Recips<float>& recips<float>(const Params& p) { return p.rf; }
 template <> __device__ __forceinline__ const Recips<double>& recips<double>(const Params& p) { return p.rd; }
+}  // namespace CLV_ARITH
 
 // tau-dependent divisors of one stage launch and their reciprocals
 template <class real> struct TauConst {
@@ -53,6 +74,15 @@ enum : int {
   FLAG_PIMN_OMEGA = 4,
   FLAG_OMEGA_OMEGA = 8,
   FLAG_BULK = 16,
+  FLAG_FAST = 32,
+};
+
+// launch choices of the viscous stage (clv_set_option, or a run's own)
+struct StageOpts {
+  int stage_kernel;  // 0 automatic, 1 per-cell, 2 tiled (3+1)D, 3 tiled (2+1)D
+  int chunk;         // x planes per tiled (3+1)D CTA
+  int minb;          // resident tiled CTAs per SM (FP32)
+  int tile;          // 0 = 8 x 32, 1 = 16 x 16, 2 = 8 x 16 (y, eta)
 };
 
 template <class real> struct Acu;
@@ -61,6 +91,24 @@ template <> struct Acu<double> { static constexpr double v = 1.0E-14; };
 
 #define CLV_THETA 1.1f
 #define CLV_HBARC 0.19733f
+
+template <class real> struct DivRange;
+template <> struct DivRange<float> {
+  static constexpr float lo = 0x1p-80f, hi = 0x1p+80f;
+};
+template <> struct DivRange<double> {
+  static constexpr double lo = 0x1p-900, hi = 0x1p+900;
+};
+// the two texels (as texel indices) and the interpolation weight at eps
+template <class real> struct EosSpot {
+  long long t0, t1;
+  real r;
+};
+template <class real> struct KeyT;
+template <> struct KeyT<float> { typedef unsigned int type; };
+template <> struct KeyT<double> { typedef unsigned long long type; };
+
+inline namespace CLV_ARITH {
 
 // OpenCL min/max/sign semantics (helper.h uses the builtins)
 template <class real> __device__ __forceinline__ real cmin(real x, real y) { return (y < x) ? y : x; }
@@ -79,16 +127,13 @@ template <class real> __device__ __forceinline__ real csign(real x) {
 // holds (|a| below 2^-80 / 2^-900 or above 2^80 / 2^900, infinities, NaN) the
 // IEEE division is used; a = 0 gives a*y, the correctly signed zero. Only used
 // with divisors and reciprocals that are normal numbers well inside the range.
-template <class real> struct DivRange;
-template <> struct DivRange<float> {
-  static constexpr float lo = 0x1p-80f, hi = 0x1p+80f;
-};
-template <> struct DivRange<double> {
-  static constexpr double lo = 0x1p-900, hi = 0x1p+900;
-};
 static __device__ __noinline__ float ieee_div(float a, float b) { return a / b; }
 static __device__ __noinline__ double ieee_div(double a, double b) { return a / b; }
 template <class real> __device__ __forceinline__ real div_by(real a, real b, real y) {
+#if CLV_FAST
+  (void)b;
+  return a * y;  // tolerance build: the reciprocal's product
+#endif
   real q0 = a * y;
   real r = fma(-q0, b, a);
   real q = fma(r, y, q0);
@@ -119,13 +164,24 @@ template <class real> __device__ __forceinline__ real div_step(real x, int step)
 #else
 #define CLV_EOS_ATTR __noinline__
 #endif
-// the two texels (as texel indices) and the interpolation weight at eps
-template <class real> struct EosSpot {
-  long long t0, t1;
-  real r;
-};
 template <class real> __device__ __forceinline__ EosSpot<real> eos_spot(const Params& p, real eps) {
   const Recips<real>& rc = recips<real>(p);
+#if CLV_FAST
+  // tolerance build: texel t = floor((e - start) / step) of the row-major
+  // image, the next texel, and the fraction between them; outside the table
+  // both indices clamp to its edge as the image's clamp-to-edge does (the
+  // reference's row-boundary rounding quirk is not reproduced)
+  {
+    const real t = (eps - (real)p.eos_start) * rc.eos_step;
+    const int last = p.eos_nrow * p.eos_ncol - 1;
+    const int i0 = (int)t;
+    EosSpot<real> s;
+    s.t0 = min(max(i0, 0), last);
+    s.t1 = min(max(i0 + 1, 0), last);
+    s.r = t - (real)i0;
+    return s;
+  }
+#endif
   real ed_per_row = p.eos_step * p.eos_ncol;
   int row = (int)div_by<real>(eps, ed_per_row, rc.eos_epr);
   int col = (int)div_by<real>(eps - p.eos_start - row * ed_per_row, (real)p.eos_step, rc.eos_step);
@@ -181,12 +237,31 @@ template <class real> __device__ __forceinline__ real eosCS2(const Params& p, re
 
 // ---------------------------------------------------------------- helper.h
 template <class real> __device__ __forceinline__ real gamma3(real vx, real vy, real vz) {  // helper.h:46-48
+#if CLV_FAST
+  return rsqrt(cmax<real>(1.0f - vx * vx - vy * vy - vz * vz, Acu<real>::v));
+#else
   return 1.0f / sqrt(cmax<real>(1.0f - vx * vx - vy * vy - vz * vz, Acu<real>::v));
+#endif
 }
 template <class real> __device__ __forceinline__ real minmod(real x, real y) {  // helper.h:74-77
   real res = cmin<real>(fabs(x), fabs(y));
   return res * (csign(x) + csign(y)) * 0.5f;
 }
+#if CLV_FAST
+// tolerance build: the generalised minmod of the two one-sided differences
+// a = R - C, b = C - L: zero unless they have the same sign, else that sign
+// times min(TH |a|, TH |b|, |a + b| / 2) -- the value of the nested minmods
+// below, in a few instructions
+template <class real> __device__ __forceinline__ real gminmod(real a, real b) {
+  const real TH = CLV_THETA;
+  const real m = fmin(TH * fmin(fabs(a), fabs(b)), (real)0.5f * fabs(a + b));
+  return (a * b > (real)0) ? copysign(m, a) : (real)0;
+}
+template <class real> __device__ __forceinline__ real slope(real L, real C, real R) { return gminmod<real>(R - C, C - L); }
+template <class real> __device__ __forceinline__ real grad_limit(real L, real C, real R) {
+  return gminmod<real>(R - C, C - L);
+}
+#else
 // slope limiter of kt1d (helper.h:213-217): minmod(0.5(R-L), minmod(TH(R-C), TH(C-L)))
 template <class real> __device__ __forceinline__ real slope(real L, real C, real R) {
   const real TH = CLV_THETA;
@@ -197,10 +272,17 @@ template <class real> __device__ __forceinline__ real grad_limit(real L, real C,
   const real TH = CLV_THETA;
   return minmod<real>(0.5f * (R - L), minmod<real>(TH * (C - L), TH * (R - C)));
 }
+#endif
 
 // helper.h:94-105, with edv = 0.5*(ev_L + ev_R)
 template <class real>
 __device__ __forceinline__ real max_speed(const Params& p, real e, real vx, real vy, real vz, real vk) {
+#if CLV_FAST
+  // tolerance build: lambda, the larger characteristic speed of flow plus
+  // sound, is below 1 for |v| < 1 and c_s^2 <= 1, so max(lambda, 1) is 1
+  (void)p; (void)e; (void)vx; (void)vy; (void)vz; (void)vk;
+  return (real)1.0f;
+#endif
   real ut = gamma3<real>(vx, vy, vz);
   real uk = ut * vk;
   real ut2 = ut * ut;
@@ -384,8 +466,27 @@ __device__ __forceinline__ unsigned long long fkey(double f) {
   unsigned long long b = (unsigned long long)__double_as_longlong(f);
   return (b & 0x8000000000000000ull) ? ~b : (b | 0x8000000000000000ull);
 }
-template <class real> struct KeyT;
-template <> struct KeyT<float> { typedef unsigned int type; };
-template <> struct KeyT<double> { typedef unsigned long long type; };
-
+// atomicMax of the ordered key of f into *key; the tolerance build first takes
+// the maximum over the warp's active lanes (hardware warp reduction; 64-bit
+// keys as the high word, then the low word among the lanes holding the
+// largest high word) so that one lane issues the atomic
+__device__ __forceinline__ unsigned int warp_max_key(unsigned int m, unsigned int k) { return __reduce_max_sync(m, k); }
+__device__ __forceinline__ unsigned long long warp_max_key(unsigned int m, unsigned long long k) {
+  const unsigned int hi = __reduce_max_sync(m, (unsigned int)(k >> 32));
+  const unsigned int lo = __reduce_max_sync(m, (unsigned int)(k >> 32) == hi ? (unsigned int)k : 0u);
+  return ((unsigned long long)hi << 32) | lo;
+}
+template <class real> __device__ __forceinline__ void key_max(typename KeyT<real>::type* key, real f) {
+  typedef typename KeyT<real>::type K;
+  const bool ok = (f == f);
+  K k = ok ? fkey(f) : (K)0;
+#if CLV_FAST
+  const unsigned int m = __activemask();
+  k = warp_max_key(m, k);
+  if ((threadIdx.x & 31) == (unsigned int)(__ffs(m) - 1) && k != (K)0) atomicMax(key, k);
+#else
+  if (ok) atomicMax(key, k);
+#endif
+}
+}  // namespace CLV_ARITH
 }  // namespace clv

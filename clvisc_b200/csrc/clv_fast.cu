@@ -1,0 +1,83 @@
+// The fused viscous stage in tolerance arithmetic (CLV_FLAG_FAST).
+//
+// This translation unit compiles the same stage headers as the exact build
+// with CLV_FAST=1 and --fmad=true -prec-div=false -prec-sqrt=false, which
+// selects the fast branches of clv_device.cuh (division by run constants as a
+// product with the reciprocal, the EOS texel index straight from e / step,
+// sign-test minmod, the KT speed max(lambda, 1) as 1, one atomic per warp for
+// the max energy density). Its functions and kernels live in clv::fast, so
+// they link beside the exact ones in clv::exact.
+#define CLV_FAST 1
+#include <string>
+
+#include "../../include/clvisc_b200.h"
+#include "clv_fast.h"
+#include "clv_stage_tiled.cuh"
+
+namespace clv_host {
+int set_error(int code, const std::string& msg);
+int check_cuda(const char* where);
+}  // namespace clv_host
+
+namespace clv_fastpath {
+namespace {
+
+constexpr int kTiledMinNz = 24;  // fewer cells along eta: per-cell kernel
+
+// per-device "dynamic shared memory raised" flags of each tiled instantiation
+constexpr int kMaxDev = 64;
+
+template <class real, bool CPL, int MINB, int TJ, int TK>
+int launch_tiled(const clv::Params& p, const clv::ViscBuffers<real>& v, int step, const clv::TauConst<real>& tc,
+                 int chunk, cudaStream_t s) {
+  typedef clv::TileSmem<real, TJ, TK> SM;
+  auto kern = clv::visc_stage_tiled_kernel<real, true, true, CPL, TJ, TK, MINB>;
+  static bool configured[kMaxDev] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDev) return clv_host::check_cuda("cudaGetDevice");
+  if (!configured[dev]) {
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SM)) != cudaSuccess)
+      return clv_host::check_cuda("cudaFuncSetAttribute(fast visc_stage_tiled_kernel)");
+    configured[dev] = true;
+  }
+  dim3 grid((p.nz + TK - 1) / TK, (p.ny + TJ - 1) / TJ, (p.nx + chunk - 1) / chunk);
+  kern<<<grid, TJ * TK, sizeof(SM), s>>>(p, v, step, tc, chunk);
+  return clv_host::check_cuda("fast visc_stage_tiled_kernel");
+}
+
+}  // namespace
+
+template <class real>
+int visc_stage(const clv::Params& p, const clv::ViscBuffers<real>& v, int step, const clv::TauConst<real>& tc,
+               const clv::StageOpts& o, cudaStream_t s) {
+  const bool bulk = p.flags & clv::FLAG_BULK;
+  const bool cpl = p.flags & (clv::FLAG_GUBSER_VISC | clv::FLAG_PIMN_OMEGA | clv::FLAG_OMEGA_OMEGA);
+  if (o.chunk < 1) return clv_host::set_error(CLV_ERR_INVALID, "fast visc stage: chunk must be >= 1");
+  if (!bulk && (o.stage_kernel == 2 || (o.stage_kernel != 1 && p.nz >= kTiledMinNz))) {
+    if (cpl) return launch_tiled<real, true, 1, 8, 32>(p, v, step, tc, o.chunk, s);
+    if constexpr (sizeof(real) == 8) return launch_tiled<real, false, 1, 8, 32>(p, v, step, tc, o.chunk, s);
+    else {
+      if (o.minb == 1) return launch_tiled<real, false, 1, 8, 32>(p, v, step, tc, o.chunk, s);
+      return launch_tiled<real, false, 2, 8, 32>(p, v, step, tc, o.chunk, s);
+    }
+  }
+  // one thread per cell: (2+1)D grids, short eta axes, the bulk sector
+  const int bs = 128;
+  const long long n = (long long)p.nx * p.ny * p.nz;
+  dim3 grid((unsigned int)((n + bs - 1) / bs));
+  if (bulk) {
+    if (cpl) clv::visc_stage_kernel<real, true, true, true, true><<<grid, bs, 0, s>>>(p, v, step, tc);
+    else clv::visc_stage_kernel<real, true, true, false, true><<<grid, bs, 0, s>>>(p, v, step, tc);
+  } else {
+    if (cpl) clv::visc_stage_kernel<real, true, true, true, false><<<grid, bs, 0, s>>>(p, v, step, tc);
+    else clv::visc_stage_kernel<real, true, true, false, false><<<grid, bs, 0, s>>>(p, v, step, tc);
+  }
+  return clv_host::check_cuda("fast visc_stage_kernel");
+}
+
+template int visc_stage<float>(const clv::Params&, const clv::ViscBuffers<float>&, int, const clv::TauConst<float>&,
+                               const clv::StageOpts&, cudaStream_t);
+template int visc_stage<double>(const clv::Params&, const clv::ViscBuffers<double>&, int,
+                                const clv::TauConst<double>&, const clv::StageOpts&, cudaStream_t);
+
+}  // namespace clv_fastpath

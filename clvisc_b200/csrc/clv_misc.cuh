@@ -72,6 +72,32 @@ __global__ void max_key_kernel(const real* x, long long n, typename KeyT<real>::
   if ((threadIdx.x & 31) == 0 && best) atomicMax(key, best);
 }
 
+// Health of a state (clv_status): counts of non-finite values over w planes of
+// n cells, and of cells whose goodcell flag is 0 (the reference's bad-cell
+// reset, kernel_IS.cl:697-708), added into out[0] and out[1]; block 0 also
+// sets out[2] to the surface elements beyond the capacity (0 if none).
+template <class real>
+__global__ void status_kernel(const real* f, int w, long long ld, long long n, const uint8_t* goodcell,
+                              const long long* sf_total, long long capacity, unsigned long long* out) {
+  unsigned long long nonfinite = 0, bad = 0;
+  for (long long I = (long long)blockIdx.x * blockDim.x + threadIdx.x; I < n; I += (long long)gridDim.x * blockDim.x) {
+    if (f)
+      for (int c = 0; c < w; c++) nonfinite += isfinite(f[c * ld + I]) ? 0ull : 1ull;
+    if (goodcell) bad += goodcell[I] == 0 ? 1ull : 0ull;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    nonfinite += __shfl_xor_sync(0xffffffffu, nonfinite, o);
+    bad += __shfl_xor_sync(0xffffffffu, bad, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    if (nonfinite) atomicAdd(out, nonfinite);
+    if (bad) atomicAdd(out + 1, bad);
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0 && sf_total)
+    out[2] = *sf_total > capacity ? (unsigned long long)(*sf_total - capacity) : 0ull;
+}
+
 // (n, w) row-major  <->  w planes of stride ld
 template <class real>
 __global__ void aos_to_soa_kernel(const real* aos, real* soa, long long n, int w, long long ld) {

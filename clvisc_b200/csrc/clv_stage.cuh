@@ -50,6 +50,21 @@ template <class real> struct IdealBuffers {
 struct Stencil {
   long long off[5];
 };
+// Grid of one event: sizes and plane stride (the single-event kernels take
+// them from Params, the batch kernel from its event table).
+struct GridDims {
+  int nx, ny, nz;
+  long long ld;
+};
+// Values of one cell that the Christoffel terms, the pi update and update_ev
+// share, each evaluated once: the stage input ev (d_ev[step]) and d_ev[1] at
+// the cell, with their gamma and table pressure P(e) (no bulk part).
+template <class real> struct CellIn {
+  real e0[4], g0, p0;
+  real e1[4], g1, p1;
+};
+
+inline namespace CLV_ARITH {
 __device__ __forceinline__ Stencil make_stencil(int q, int L, long long stride) {
   Stencil s;
 #pragma unroll
@@ -60,13 +75,6 @@ __device__ __forceinline__ Stencil make_stencil(int q, int L, long long stride) 
   return s;
 }
 
-// Values of one cell that the Christoffel terms, the pi update and update_ev
-// share, each evaluated once: the stage input ev (d_ev[step]) and d_ev[1] at
-// the cell, with their gamma and table pressure P(e) (no bulk part).
-template <class real> struct CellIn {
-  real e0[4], g0, p0;
-  real e1[4], g1, p1;
-};
 // e0, g0 and p0 set: fills e1, g1, p1. At stage 1 the stencil input is d_ev[1]
 // itself (same buffer), so its values are e0's; otherwise they are read.
 template <class real>
@@ -299,16 +307,10 @@ __device__ __forceinline__ void ev_update(const Params& p, const ViscBuffers<rea
     b.udiff[2 * ld + I] = gn * en[2] - go * e1[2];
     b.udiff[3 * ld + I] = gn * en[3] - go * e1[3];
   }
-  if (b.edmax_key && en[0] == en[0]) atomicMax(b.edmax_key, fkey(en[0]));
+  if (b.edmax_key) key_max<real>(b.edmax_key, en[0]);
 }
 
 // --------------------------------------------------------------- viscous
-// Grid of one event: sizes and plane stride (the single-event kernels take
-// them from Params, the batch kernel from its event table).
-struct GridDims {
-  int nx, ny, nz;
-  long long ld;
-};
 
 // One cell of the fused viscous stage. With BULK the pi fields carry an
 // eleventh plane, the bulk pressure Pi, and the sources an eleventh IS term.
@@ -713,7 +715,8 @@ __global__ void __launch_bounds__(128) ideal_stage_kernel(Params p, IdealBuffers
   if (b.write_src)
 #pragma unroll
     for (int c = 0; c < 4; c++) b.src[c * ld + I] = S[c];
-  if (b.edmax_key && en[0] == en[0]) atomicMax(b.edmax_key, fkey(en[0]));
+  if (b.edmax_key) key_max<real>(b.edmax_key, en[0]);
 }
 
+}  // namespace CLV_ARITH
 }  // namespace clv

@@ -53,6 +53,8 @@ template <class real, int TJ, int TK> struct TileSmem {
   real SZ[NCOMP][G::NSZ];     // z slopes, then z face fluxes
 };
 
+inline namespace CLV_ARITH {
+
 // record of one (clamped) cell of the stage input
 template <class real>
 __device__ CLV_TILED_ATTR void make_record(const Params& p, const ViscBuffers<real>& b, real tau, int i, int j, int k,
@@ -398,4 +400,5 @@ __global__ void __launch_bounds__(TJ * TK, MINB)
   (void)acu;
 }
 
+}  // namespace CLV_ARITH
 }  // namespace clv

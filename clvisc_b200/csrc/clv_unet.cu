@@ -18,6 +18,13 @@ using namespace clv::unet;
 
 namespace {
 inline cudaStream_t S(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+// the current device (launch set-up is cached per device), or -1
+constexpr int kMaxDevices = 64;
+inline int current_device() {
+  int d = 0;
+  return (cudaGetDevice(&d) == cudaSuccess && d >= 0 && d < kMaxDevices) ? d : -1;
+}
 inline unsigned nb(long long n, int bs) { return (unsigned)((n + bs - 1) / bs); }
 inline bool al16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
 static_assert(sizeof(clv_unet_conv) == sizeof(ConvArgs), "clv_unet_conv layout");
@@ -89,7 +96,10 @@ template <int BN, bool SW> int launch_conv_tma(const ConvArgs& a, int bw, cudaSt
       return clv_host::set_error(CLV_ERR_INVALID, "unet_conv3x3: weight tensor map rejected");
   }
   auto kern = conv3x3_tma_kernel<BN, SW>;
-  static int grid = 0;
+  static int grids[kMaxDevices] = {};  // resident CTAs of this device
+  const int gdev = current_device();
+  if (gdev < 0) return clv_host::check_cuda("cudaGetDevice");
+  int& grid = grids[gdev];
   if (!grid) {
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TmaSmem<BN>)) !=
             cudaSuccess ||
@@ -140,18 +150,23 @@ int wgrad_tma(const WgradArgs& a, float* dw, int accumulate, int max_splits, cud
             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
       return clv_host::set_error(CLV_ERR_INVALID, "unet_wgrad3x3: activation tensor map rejected");
   }
-  static bool configured = false;
-  if (!configured) {
+  static bool configured[kMaxDevices] = {};  // launch attributes are per device
+  const int cdev = current_device();
+  if (cdev < 0) return clv_host::check_cuda("cudaGetDevice");
+  if (!configured[cdev]) {
     if (cudaFuncSetAttribute(wgrad3x3_tma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)sizeof(WgTmaSmem)) != cudaSuccess)
       return clv_host::check_cuda("cudaFuncSetAttribute(wgrad3x3_tma_kernel)");
-    configured = true;
+    configured[cdev] = true;
   }
   const long long nchunks = (long long)a.N * (a.H / bh) * (a.W / bw);
   const int blocks = ((9 * a.Cin + WGT_BM - 1) / WGT_BM) * ((a.Cout + WGT_BN - 1) / WGT_BN);
   // one wave of resident CTAs (two an SM: shared memory), within the scratch
   // the caller sized for max_splits
-  static int resident = 0;
+  static int residents[kMaxDevices] = {};  // per device: SM counts differ
+  const int rdev = current_device();
+  if (rdev < 0) return clv_host::check_cuda("cudaGetDevice");
+  int& resident = residents[rdev];
   if (!resident) {
     int dev = 0, sms = 0;
     cudaGetDevice(&dev);
@@ -172,12 +187,14 @@ int wgrad_tma(const WgradArgs& a, float* dw, int accumulate, int max_splits, cud
 
 template <int BN> int launch_conv_tc(const ConvArgs& a, long long P, cudaStream_t s) {
   auto kern = conv3x3_tc_kernel<BN>;
-  static bool configured = false;
-  if (!configured) {
+  static bool configured[kMaxDevices] = {};  // launch attributes are per device
+  const int cdev = current_device();
+  if (cdev < 0) return clv_host::check_cuda("cudaGetDevice");
+  if (!configured[cdev]) {
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TcSmem<BN>)) !=
         cudaSuccess)
       return clv_host::check_cuda("cudaFuncSetAttribute(conv3x3_tc_kernel)");
-    configured = true;
+    configured[cdev] = true;
   }
   dim3 grid(nb(P, TC_BM), a.Cout / BN);
   kern<<<grid, 128, sizeof(TcSmem<BN>), s>>>(a);

@@ -176,6 +176,19 @@ class CLVisc(object):
         if save_hypersf:
             self.save_pimn_sf()
 
+    def status(self, slot=1):
+        """Health of d_ev[slot], d_pi[slot] after a step (clv_status): a dict
+        with the non-finite values of the fields ('nan'), the cells whose pi
+        was reset by the bad-cell test ('bad_cells', kernel_IS.cl:697-708) and
+        the surface elements found beyond the capacity ('sf_overflow')."""
+        counts = torch.zeros(3, dtype=torch.int64, device=self.device)
+        host = (ctypes.c_longlong * 3)()
+        self._call('clv_status', _lib.ptr(self.ideal.d_ev[slot]), _lib.ptr(self.d_pi[slot]),
+                   int(self.d_pi[slot].shape[0]), _lib.ptr(self.d_goodcell), _lib.ptr(self.ideal.d_num_of_sf),
+                   int(self.ideal.hypersf_capacity), _lib.ptr(counts), ctypes.cast(host, ctypes.c_void_p),
+                   self.stream)
+        return {'nan': int(host[0]), 'bad_cells': int(host[1]), 'sf_overflow': int(host[2])}
+
     def pi_to_host(self, slot=1):
         """d_pi[slot] as (cells, 10)."""
         return self.ideal.field_to_host(self.d_pi[slot][:10])

@@ -49,6 +49,17 @@ extern "C" {
  * tau_Pi = zeta / (14.55 (1/3 - cs2)^2 (e+P)), is held within |Pi| <= P and
  * at zero in cells colder than zetaos_tmin, and P + Pi replaces P in T^{mu nu}. */
 #define CLV_FLAG_BULK 16
+/* Tolerance arithmetic for the fused viscous stage (both parts in one
+ * launch), an option with no counterpart in the reference: the kernels are
+ * compiled with fused multiply-add contraction and approximate division and
+ * square root, divide by run constants through their reciprocals, index the
+ * EOS image by e / step, evaluate the minmod limiters in sign-test form and
+ * take the KT speed max(lambda, 1) as 1 (lambda <= 1 for |v| < 1). Results
+ * differ from the reference's arithmetic by rounding: within 1e-5 of each
+ * field's largest magnitude in FP32 after the tested step counts. Without the
+ * flag every kernel reproduces the reference's arithmetic bit for bit. The
+ * split stages (one part per launch) always use the exact arithmetic. */
+#define CLV_FLAG_FAST 32
 
 /* parts of a viscous stage (visc.py:287 IS_stepUpdate, visc.py:232 visc_stepUpdate) */
 #define CLV_PART_IS 1
@@ -71,6 +82,11 @@ typedef struct clv_params {
   int flags;              /* CLV_FLAG_* */
   float zetaos_max, zetaos_t0, zetaos_width, zetaos_skew; /* bulk sector (CLV_FLAG_BULK) */
   float zetaos_tmin;      /* bulk sector: Pi = 0 in cells colder than this */
+  /* Kernel choices of this run (see clv_set_option); 0 = the process-wide
+   * setting. opt_stage_kernel = 1 + CLV_OPT_STAGE_KERNEL value, opt_chunk =
+   * x planes per tiled CTA, opt_tiled_blocks = 1 or 2, opt_tile = 1 +
+   * CLV_OPT_TILE value. */
+  int opt_stage_kernel, opt_chunk, opt_tiled_blocks, opt_tile;
 } clv_params;
 
 /* Buffers of one viscous Runge-Kutta stage. `step` is 1 or 2 as in
@@ -93,7 +109,8 @@ typedef struct clv_visc_buffers {
   int write_udiff;       /* step 2 only: udiff = u(ev_new) - u(ev1)            */
 } clv_visc_buffers;
 
-/* Tuning options (process-wide): the viscous-stage kernel variant
+/* Tuning options (process-wide defaults; a run's own opt_* fields in
+ * clv_params take precedence): the viscous-stage kernel variant
  * (0 = automatic, the default: on grids with at least 24 cells along eta and
  * no bulk sector the tiled (3+1)D kernel, else one thread per cell; 1 = one
  * thread per cell without shared memory; 2 = tiled (3+1)D wherever it
@@ -120,6 +137,22 @@ int clv_version(void);
 const char *clv_last_error(void);
 /* Required alignment (bytes) of every field pointer and of ld*elem_size. */
 int clv_alignment(void);
+
+/* Health of a state after a step (replaces reading d_goodcell and scanning
+ * the fields on the host; the reference reports neither, kernel_IS.cl:697-708
+ * only flags bad cells in d_goodcell). Into counts_dev (3 device int64, the
+ * caller's memory) it writes, on `stream`: [0] the non-finite values in the 4
+ * planes of ev and the npi planes of pi (pi nullable), [1] the cells whose
+ * goodcell flag is 0 (goodcell nullable: 0), [2] the surface elements beyond
+ * sf_capacity given the device count sf_total (nullable: 0). With counts_host
+ * non-null it also copies the three counts there and synchronizes the
+ * stream. */
+int clv_status(const clv_params *p, const void *ev, const void *pi, int npi, const unsigned char *goodcell,
+               const long long *sf_total, long long sf_capacity, long long *counts_dev, long long *counts_host,
+               void *stream);
+/* sizeof(clv_params) as compiled into the library, for bindings that mirror
+ * the struct (a ctypes or cgo binding checks its own size against it). */
+size_t clv_params_size(void);
 
 /* One ideal Runge-Kutta stage: kt_src_christoffel + kt_src_alongx/y/z +
  * update_ev (kernel_ideal.cl:3-231, driven by ideal.py:211-255).

@@ -23,6 +23,10 @@ def make_cfg(nx, ny, nz, use_float32=True, eos_type='lattice_pce165', dx=0.3, dz
     for k, v in extra.items():
         setattr(cfg, k, v)
     cfg.BSZ = 64
+    # the parity tests compare bit for bit: the reference's arithmetic unless
+    # a test asks for the tolerance build
+    if 'arithmetic' not in extra:
+        cfg.arithmetic = 'exact'
     from clvisc_b200.config import set_real
     return set_real(cfg)
 

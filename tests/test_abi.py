@@ -59,3 +59,23 @@ def test_read_config_overrides():
     assert cfg.real == np.float64 and cfg.sz_real == 8
     assert cfg.riemann_test
     assert read_config([]).real == np.float32
+
+
+def test_params_struct_size_matches_library():
+    """The ctypes mirror of clv_params has the library's layout size (a
+    binding that drops fields would make the library read past its struct)."""
+    lib = _lib.load()
+    assert lib.clv_params_size() == ctypes.sizeof(_lib.ClvParams)
+
+
+def test_arithmetic_flag():
+    from clvisc_b200.ideal import fast_arithmetic
+    cfg = read_config([])
+    assert cfg.arithmetic == 'auto' and fast_arithmetic(cfg)
+    cfg.use_float32 = False
+    assert not fast_arithmetic(cfg)
+    cfg.arithmetic = 'fast'
+    assert fast_arithmetic(cfg)
+    cfg.arithmetic = 'exact'
+    cfg.use_float32 = True
+    assert not fast_arithmetic(cfg)

@@ -1,0 +1,101 @@
+"""The tolerance-arithmetic fused stage (CLV_FLAG_FAST, cfg.arithmetic =
+'fast') against the oracle, which follows the reference's arithmetic.
+
+The fast build contracts multiply-adds, divides through reciprocals and
+evaluates the limiters in sign-test form, so its fields differ from the
+reference's by rounding. The stated tolerance, per field and per component:
+    max_cells |fast - oracle| <= tol * max_cells |oracle|
+with tol = 1e-5 in FP32 and 1e-11 in FP64, after the listed numbers of fused
+time steps. The largest error seen is printed with each case.
+"""
+import numpy as np
+import pytest
+
+from parity_util import make_cfg, seeded_ic
+
+pytestmark = pytest.mark.gpu
+
+TOL = {True: 1e-5, False: 1e-11}
+
+
+def scaled_err(got, want):
+    """Per-column max |got - want| / max |want| (0 for an all-zero column)."""
+    got = np.asarray(got, dtype=np.float64).reshape(want.shape[0], -1)
+    want = np.asarray(want, dtype=np.float64).reshape(want.shape[0], -1)
+    scale = np.abs(want).max(axis=0)
+    d = np.abs(got - want).max(axis=0)
+    return np.where(scale > 0, d / np.where(scale > 0, scale, 1.0), d)
+
+
+def compare_fields(v, o, use_float32, tag):
+    errs = {'ev': scaled_err(v.ideal.field_to_host(v.ideal.d_ev[1]), o.ideal.d_ev[1]),
+            'pi': scaled_err(v.ideal.field_to_host(v.d_pi[1])[:, :10], o.d_pi[1])}
+    if v.bulk:
+        errs['bulk'] = scaled_err(v.bulk_to_host(1)[:, None], o.d_bulk[1][:, None])
+    worst = max(float(e.max()) for e in errs.values())
+    print('%s: max scaled error %.3e (ev %s, pi %s)' % (tag, worst, np.array2string(errs['ev'], precision=2),
+                                                        np.array2string(errs['pi'], precision=2)))
+    assert np.isfinite(worst) and worst <= TOL[use_float32], (tag, errs)
+    return worst
+
+
+@pytest.mark.parametrize('use_float32', [True, False])
+@pytest.mark.parametrize('grid,steps', [((40, 37, 35), 12), ((25, 23, 13), 12), ((41, 39, 1), 20), ((9, 1, 30), 12)])
+def test_fast_stage_within_tolerance(cuda_lib, oracle_mod, use_float32, grid, steps):
+    """Tiled (3+1)D (40x37x35: eta >= 24 cells), per-cell (short eta, (2+1)D,
+    one-cell y) kernels of the fast build against the oracle."""
+    from clvisc_b200.visc import CLVisc
+    cfg = make_cfg(*grid, use_float32=use_float32, arithmetic='fast')
+    ic = seeded_ic(cfg, seed=11, flow=0.2)
+    v = CLVisc(cfg)
+    assert v.params.flags & 32
+    o = oracle_mod.OracleVisc(cfg)
+    v.load_ini(ic)
+    o.load_ini(ic)
+    v.IS_initialize()
+    o.IS_initialize()
+    for n in range(steps):
+        v.step(n, edmax=(n == steps - 1))
+        o.step(n)
+    compare_fields(v, o, use_float32, 'fast %s %s' % (grid, 'fp32' if use_float32 else 'fp64'))
+    want = o.ideal.max_energy_density()
+    assert abs(v.read_edmax_key() - want) <= TOL[use_float32] * abs(want)
+
+
+@pytest.mark.parametrize('use_float32', [True, False])
+def test_fast_bulk_and_gubser_flag(cuda_lib, oracle_mod, use_float32):
+    """The fast per-cell instantiations with the bulk sector and with the
+    GUBSER_VISC_TEST coupling terms."""
+    from clvisc_b200.visc import CLVisc
+    bulk = dict(ZETAOS_MAX=0.05, ZETAOS_T0=0.18, ZETAOS_WIDTH=0.02)
+    for extra, grid in ((bulk, (19, 17, 9)), (dict(gubser_visc_test=True, LAM1=-10.0), (17, 15, 1))):
+        kw = dict(eos_type='ideal_gas') if 'gubser_visc_test' in extra else {}
+        cfg = make_cfg(*grid, use_float32=use_float32, arithmetic='fast', **kw, **extra)
+        ic = seeded_ic(cfg, seed=4, flow=0.1)
+        v = CLVisc(cfg)
+        o = oracle_mod.OracleVisc(cfg)
+        v.load_ini(ic)
+        o.load_ini(ic)
+        v.IS_initialize()
+        o.IS_initialize()
+        for n in range(8):
+            v.step(n)
+            o.step(n)
+        compare_fields(v, o, use_float32, 'fast %s' % sorted(extra))
+
+
+def test_fast_is_not_exact(cuda_lib):
+    """The flag reaches the kernels: fast and exact runs of the same input
+    differ (by rounding), exact runs are reproducible bit for bit."""
+    from clvisc_b200.visc import CLVisc
+    out = {}
+    for mode in ('fast', 'exact', 'exact2'):
+        cfg = make_cfg(30, 28, 26, arithmetic=mode.rstrip('2'))
+        v = CLVisc(cfg)
+        v.load_ini(seeded_ic(cfg, seed=2))
+        for n in range(4):
+            v.step(n)
+        out[mode] = v.ideal.field_to_host(v.ideal.d_ev[1])
+    assert np.array_equal(out['exact'], out['exact2'])
+    assert not np.array_equal(out['fast'], out['exact'])
+    assert scaled_err(out['fast'], out['exact']).max() < 1e-5
