@@ -14,7 +14,8 @@ through the public API with host buffers: load_ini from pinned host memory,
 CLVisc.evolve for K steps, ev_to_host. With N > 1 every rank advances its own
 replica of the event (weak scaling; the path has no exchange step).
 --impl reference times the oracle (the C++/OpenMP restatement of the
-reference kernels, all host threads) on a bounded slab of the same workload.
+reference kernels, all host threads) on the same whole workload, the same
+warm-up and timed step counts.
 """
 import argparse
 import json
@@ -36,7 +37,6 @@ UNIT = 'cell-updates/s'
 # S = 14 state reals, U = 4 udiff reals; the stencil halo and EOS table
 # counted as cache hits)
 ALG_BYTES_PER_CELL_UPDATE = 312
-SLAB_NZ = 16  # CPU-baseline sample: a 385 x 385 x 16 eta slab of the event
 
 
 def make_cfg(nz=NZ, out='/tmp/clv_bench', nx=NX, ny=NY, fp64=False, arithmetic='auto'):
@@ -167,18 +167,18 @@ def issue_roofline(cell_updates_per_s, sm_mhz):
             'instructions_per_cell_update': inst, 'sm_mhz': sm_mhz}
 
 
-def cpu_baseline(steps=2, warmup=0, nx=NX, ny=NY, nz=NZ):
-    """The oracle on an nx x ny x SLAB_NZ eta slab of the event, all host threads."""
+def cpu_baseline(steps=5, warmup=0, nx=NX, ny=NY, nz=NZ, ic=None):
+    """The oracle (the C++/OpenMP restatement of the reference kernels and
+    its orchestration, all host threads) on the whole workload: the same grid,
+    initial condition and step as the GPU arm, `warmup` untimed steps, then
+    `steps` timed steps."""
     sys.path.insert(0, os.path.join(ROOT, 'oracle'))
-    import numpy as np
     import oracle as O
-    slab = min(SLAB_NZ, nz)
-    cfg = make_cfg(nz=slab, nx=nx, ny=ny)
-    ic = initial_condition(nx=nx, ny=ny, nz=nz).reshape(nx, ny, nz, 4)
-    k0 = nz // 2 - slab // 2
-    sub = np.ascontiguousarray(ic[:, :, k0:k0 + slab]).reshape(-1, 4)
+    cfg = make_cfg(nz=nz, nx=nx, ny=ny, arithmetic='exact')
+    if ic is None:
+        ic = initial_condition(nx=nx, ny=ny, nz=nz)
     o = O.OracleVisc(cfg)
-    o.load_ini(sub)
+    o.load_ini(ic)
     for n in range(warmup):
         o.step(n)
     t = time.perf_counter()
@@ -186,10 +186,19 @@ def cpu_baseline(steps=2, warmup=0, nx=NX, ny=NY, nz=NZ):
         o.step(n)
     dt = time.perf_counter() - t
     cores = int(os.environ.get('OMP_NUM_THREADS', os.cpu_count() or 1))
-    cells = nx * ny * slab
+    cells = nx * ny * nz
     return {'value': cells * steps / dt, 'unit': UNIT, 'cores': cores, 'kind': 'port',
-            'sample': '%d steps of a %dx%dx%d eta slab of the same event (oracle, OpenMP)' % (steps, nx, ny, slab),
+            'sample': '%d steps (after %d untimed) of the whole %dx%dx%d event (oracle, OpenMP, %d threads)'
+                      % (steps, warmup, nx, ny, nz, cores),
             'seconds': dt}
+
+
+def workload_config(nx, ny, nz, fp64, world):
+    """The `config` object of both arms' lines."""
+    return {'workload': 'viscous %dx%dx%d Pb+Pb b=8 fm seed 5, %s, lattice EOS, dtau=0.01'
+                        % (nx, ny, nz, 'FP64' if fp64 else 'FP32'),
+            'cells': nx * ny * nz, 'l2': 'inputs larger than L2 (state 0.95 GB per stage)',
+            'parallelism': 'replicas x%d' % world}
 
 
 def max_over_ranks(x, dist):
@@ -213,11 +222,12 @@ def run_reference(args, rank, world):
     if rank != 0:
         return
     nx, ny, nz = args.grid
-    cb = cpu_baseline(steps=max(1, args.steps), warmup=min(args.warmup, 1), nx=nx, ny=ny, nz=nz)
+    cb = cpu_baseline(steps=max(1, args.steps), warmup=args.warmup, nx=nx, ny=ny, nz=nz)
     line = {'impl': 'reference', 'metric': METRIC, 'value': cb['value'], 'unit': UNIT, 'n_gpus': world,
             'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': 1e3 * cb['seconds'] / max(1, args.steps),
             'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic',
-            'config': {'workload': 'viscous %dx%dx%d Pb+Pb b=8 fm, FP32, lattice EOS (slab sample)' % (nx, ny, nz)},
+            'config': workload_config(nx, ny, nz, False, world),
+            'arithmetic': 'the reference\'s (oracle)',
             'cpu_baseline': {k: cb[k] for k in ('value', 'unit', 'cores', 'kind', 'sample')},
             'e2e': {'value': cb['value'], 'unit': UNIT, 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}}
     print(json.dumps(line), flush=True)
@@ -436,17 +446,14 @@ def run_gpu(args, rank, world, dist):
     alg = ALG_BYTES_PER_CELL_UPDATE * (2 if args.fp64 else 1)
     achieved = value / world * alg / 1e9
     traffic = None if args.fp64 else read_traffic()
-    prec = 'FP64' if args.fp64 else 'FP32'
     real = 'double' if args.fp64 else 'float'
     if rank == 0:
         line = {
             'metric': METRIC, 'value': value, 'unit': UNIT, 'n_gpus': world, 'steps': args.steps,
             'warmup': args.warmup, 'ms_per_step': ms / args.steps, 'higher_is_better': True, 'scaling': 'weak',
             'vs_baseline': None, 'dtype': 'f64' if args.fp64 else 'f32', 'data': 'synthetic',
-            'config': {'workload': 'viscous %dx%dx%d Pb+Pb b=8 fm seed 5, %s, lattice EOS, dtau=0.01'
-                                   % (nx, ny, nz, prec),
-                       'cells': cells, 'l2': 'inputs larger than L2 (state 0.95 GB per stage)',
-                       'parallelism': 'replicas x%d' % world},
+            'config': workload_config(nx, ny, nz, args.fp64, world),
+            'arithmetic': 'fast' if v.params.flags & 32 else 'exact',
             'e2e': {'value': e2e, 'unit': UNIT, 'h2d_bytes_per_step': h2d, 'd2h_bytes_per_step': d2h,
                     'wall_s': e2e_wall},
             'gpu_launches': 2 * args.steps,
@@ -462,7 +469,7 @@ def run_gpu(args, rank, world, dist):
         if args.evolve and world == 1:
             line['evolve'] = evolve_to_freezeout(args, nx, ny, nz)
         if not args.no_cpu_baseline and not args.fp64:
-            cb = cpu_baseline(steps=2)
+            cb = cpu_baseline(steps=5, nx=nx, ny=ny, nz=nz, ic=ic)
             line['cpu_baseline'] = {k: cb[k] for k in ('value', 'unit', 'cores', 'kind', 'sample')}
         if args.batch_events > 0 and world == 1:
             line['batch'] = run_batch(args.batch_events, one_at_a_time=not args.no_one_at_a_time)

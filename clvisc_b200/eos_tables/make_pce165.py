@@ -101,7 +101,10 @@ def build(refroot):
 
 
 if __name__ == '__main__':
-    ref = sys.argv[1] if len(sys.argv) > 1 else '/root/reference'
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get('CLVISC_REFERENCE_ROOT')
+    if not ref:
+        sys.exit('usage: make_pce165.py REFERENCE_ROOT (or set CLVISC_REFERENCE_ROOT): '
+                 'the directory that holds the reference project (pyvisc/, eos tables)')
     (e, p, s, T), cs2 = build(ref)
     out = os.path.join(os.path.dirname(os.path.abspath(__file__)), 'lattice_pce165.npz')
     np.savez_compressed(out, src_e=e, src_p=p, src_s=s, src_T=T, cs2=cs2.astype(np.float32),

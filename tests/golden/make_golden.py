@@ -115,4 +115,8 @@ def main(refroot):
 
 
 if __name__ == '__main__':
-    main(sys.argv[1] if len(sys.argv) > 1 else '/root/reference')
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get('CLVISC_REFERENCE_ROOT')
+    if not root:
+        sys.exit('usage: make_golden.py REFERENCE_ROOT (or set CLVISC_REFERENCE_ROOT): '
+                 'the directory that holds the reference project (pyvisc/)')
+    main(root)
