@@ -3,9 +3,11 @@
 The tiled stage kernel takes its (y, eta) tile from a compile-time set
 (8 x 32, 16 x 16 or 8 x 16, CLV_OPT_TILE) and its x extent per block at run time
 (CLV_OPT_CHUNK); the per-cell kernel is the alternative on any grid. Every
-variant computes the same bits. tune_visc() times each candidate for a few
-fused steps on the run's own state, saved before and restored after each, and
-leaves the fastest selected (the options are process-wide).
+variant computes the same bits (in either arithmetic). tune_visc() times each
+candidate for a few fused steps on the run's own state, saved before and
+restored after each, and leaves the fastest selected for that run only: the
+choice goes into the run's own clv_params (opt_* fields), so other CLVisc
+objects in the process keep theirs.
 
     from clvisc_b200.autotune import tune_visc
     v = CLVisc(cfg); v.load_ini(ic)
@@ -18,11 +20,13 @@ from . import _lib
 DEFAULTS = {'kernel': 0, 'tile': 0, 'chunk': 32, 'blocks': 2}
 
 
-def _apply(c):
-    _lib.set_option(_lib.CLV_OPT_STAGE_KERNEL, c['kernel'])
-    _lib.set_option(_lib.CLV_OPT_TILE, c['tile'])
-    _lib.set_option(_lib.CLV_OPT_CHUNK, c['chunk'])
-    _lib.set_option(_lib.CLV_OPT_TILED_BLOCKS, c['blocks'])
+def _apply(v, c):
+    """Select candidate c for the run v (its clv_params opt_* fields)."""
+    p = v.params
+    p.opt_stage_kernel = c['kernel'] + 1
+    p.opt_tile = c['tile'] + 1
+    p.opt_chunk = c['chunk']
+    p.opt_tiled_blocks = c['blocks']
 
 
 def candidates(nz, use_float32=True):
@@ -53,7 +57,7 @@ def tune_visc(v, steps=3, cands=None):
     tau = v.ideal.tau
     table = {}
     for c in cands:
-        _apply(c)
+        _apply(v, c)
         v.step(0)  # warm-up (and one-time kernel set-up)
         torch.cuda.synchronize(v.device)
         e0 = torch.cuda.Event(enable_timing=True)
@@ -71,10 +75,17 @@ def tune_visc(v, steps=3, cands=None):
     best_key = min(table, key=table.get)
     best = next(c for c in cands if 'kernel%d_tile%d_chunk%d_blocks%d' % (c['kernel'], c['tile'], c['chunk'],
                                                                             c['blocks']) == best_key)
-    _apply(best)
+    _apply(v, best)
     return best, table
 
 
-def reset():
-    """Back to the library's default launch shape."""
-    _apply(DEFAULTS)
+def reset(v=None):
+    """The run v (if given) back to the process-wide launch choices, and
+    those back to the library's defaults."""
+    if v is not None:
+        p = v.params
+        p.opt_stage_kernel = p.opt_tile = p.opt_chunk = p.opt_tiled_blocks = 0
+    _lib.set_option(_lib.CLV_OPT_STAGE_KERNEL, DEFAULTS['kernel'])
+    _lib.set_option(_lib.CLV_OPT_TILE, DEFAULTS['tile'])
+    _lib.set_option(_lib.CLV_OPT_CHUNK, DEFAULTS['chunk'])
+    _lib.set_option(_lib.CLV_OPT_TILED_BLOCKS, DEFAULTS['blocks'])

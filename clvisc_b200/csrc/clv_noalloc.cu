@@ -25,9 +25,11 @@
 // Each call writes every block count and both counters it reads before reading
 // them, so nothing left from a previous call is used.
 //
-// The array's device address is looked up with cudaGetSymbolAddress the first
-// time the entry point runs on a device (with that device current); that first
-// call on each device should therefore come before any stream capture.
+// The array's device address is looked up with cudaGetSymbolAddress, with the
+// call's device current, on every call made outside stream capture (so it is
+// right again after a cudaDeviceReset); a call during capture reuses the
+// address of the last call outside capture on that device. The first call on
+// each device should therefore come before any stream capture.
 #include <mutex>
 #include <string>
 
@@ -100,13 +102,20 @@ __global__ void noalloc_scan_kernel(int* block_count, int n, long long* total) {
 
 __global__ void noalloc_advance_kernel(const long long* count, long long* total) { *total += *count; }
 
-// device address of the scratch array on the current device
-int noalloc_scratch(NoallocScratch** out) {
+// device address of the scratch array on the current device. Outside stream
+// capture the address is looked up again on every call, so a context that was
+// torn down and rebuilt (cudaDeviceReset) never leaves a stale pointer behind;
+// during capture, where that lookup is best avoided, the address cached by the
+// last call outside capture on this device is used.
+int noalloc_scratch(NoallocScratch** out, cudaStream_t s) {
   int dev = -1;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 256)
     return noalloc_fail(CLV_ERR_CUDA, "hypersf_noalloc: no current CUDA device");
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s, &cap) != cudaSuccess)
+    return noalloc_fail(CLV_ERR_CUDA, "hypersf_noalloc: cudaStreamIsCapturing failed");
   std::lock_guard<std::mutex> lock(g_noalloc_mu);
-  if (!g_noalloc_addr[dev]) {
+  if (cap == cudaStreamCaptureStatusNone || !g_noalloc_addr[dev]) {
     void* ptr = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
     if (e != cudaSuccess || !ptr)
@@ -243,7 +252,7 @@ int noalloc_run(const clv_params* pp, int visc, double tau_old, double tau_new, 
     return noalloc_fail(CLV_ERR_INVALID, "hypersf_noalloc: " + std::to_string(nc) + " coarse cubes exceed the limit of " +
                                              std::to_string(NOALLOC_MAX_CUBES) + "; use clv_hypersf_append");
   NoallocScratch* scr = nullptr;
-  int rc = noalloc_scratch(&scr);
+  int rc = noalloc_scratch(&scr, s);
   if (rc) return rc;
   const unsigned int nb = (unsigned int)((nc + NOALLOC_BLOCK - 1) / NOALLOC_BLOCK);
   noalloc_count_kernel<real><<<nb, NOALLOC_BLOCK, 0, s>>>(p, (const real*)ev_old, (const real*)ev_new, visc,

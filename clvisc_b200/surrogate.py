@@ -130,6 +130,16 @@ class UNet(object):
     def _chk(self, rc, what):
         _lib.check(rc, what)
 
+    def check_timeouts(self, what):
+        """Raise if a tensor-core kernel's bounded wait ran out since the last
+        check (clv_unet_timeouts; such a kernel skips its epilogue and leaves
+        output tiles unwritten, so its results cannot be used)."""
+        n = ctypes.c_int(0)
+        self._chk(self.lib.clv_unet_timeouts(ctypes.byref(n), 1), 'clv_unet_timeouts')
+        if n.value:
+            raise RuntimeError('%s: %d tensor-core waits timed out; results discarded' % (what, n.value))
+        return 0
+
     def pack(self):
         """BF16 copies of the 3x3 weights for the forward and input-gradient convolutions."""
         for name, cin, cout, _ in LAYERS:
@@ -383,6 +393,7 @@ class Surrogate(object):
                 net.adam(lr_s)
                 step += 1
             history.append(float(ep_loss) / steps_per_epoch)
+            self.net.check_timeouts('training epoch %d' % ep)
             if log:
                 log('epoch %d loss %.5f' % (ep, history[-1]))
         return history
@@ -398,6 +409,7 @@ class Surrogate(object):
             net.buf['x'][:m].copy_(xb * self.in_scale)
             o = net.forward()
             out[i0:i0 + m] = (o.view(B, n, n, K_OUT)[:m] * self.out_scale)
+        net.check_timeouts('inference')
         return out
 
 
@@ -519,6 +531,7 @@ def run_experiment(n_train=20000, n_test=1000, epochs=12, batch=32, n=128, steps
         err = err.clone()
         err[torch.from_numpy(idx).to(dev)] = rel_l2(yfb[..., 0], yte[torch.from_numpy(idx).to(dev)][..., 0])
     res['pred_not_finite'] = int((~torch.isfinite(pred)).reshape(pred.shape[0], -1).any(1).sum())
+    res['tensor_core_timeouts'] = sur.net.check_timeouts('evaluation')  # training and inference raised on any
     res.update({
         'inference_s': t_inf, 'fallback_events': n_rerun, 'fallback_s': t_fb,
         'surrogate_events_per_h': xte.shape[0] / (t_inf + t_fb) * 3600.0,

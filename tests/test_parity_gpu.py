@@ -268,3 +268,23 @@ def test_autotune_restores_state(cuda_lib, use_float32):
     reset()
     assert_same('ev after tuning', runs[1][0], runs[0][0])
     assert_same('pi after tuning', runs[1][1], runs[0][1])
+
+
+def test_tuned_choice_is_per_run(cuda_lib):
+    """A run's own kernel choice (clv_params opt_*) leaves other runs on the
+    process-wide setting: a per-cell run and a tiled run of the same input in
+    one process, exact arithmetic, give the same bits, and the process-wide
+    option is untouched."""
+    from clvisc_b200.visc import CLVisc
+    cfg = make_cfg(30, 28, 26)
+    ic = seeded_ic(cfg, seed=9)
+    a, b = CLVisc(cfg), CLVisc(cfg)
+    a.params.opt_stage_kernel = 1 + 1  # per-cell for a only
+    b.params.opt_stage_kernel = 1 + 2  # tiled for b only
+    for v in (a, b):
+        v.load_ini(ic)
+        for n in range(3):
+            v.step(n)
+    assert_same('per-run kernels', a.ideal.field_to_host(a.ideal.d_ev[1]), b.ideal.field_to_host(b.ideal.d_ev[1]))
+    c = CLVisc(cfg)
+    assert c.params.opt_stage_kernel == 0
