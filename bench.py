@@ -65,20 +65,47 @@ def initial_condition(seed=5, nx=NX, ny=NY, nz=NZ):
 
 
 class ClockSampler(object):
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clock and throttle reasons sampled during the timed region: NVML
+    (read-only queries) every 20 ms from a thread, so that a timed region of a
+    fraction of a second still holds several samples; nvidia-smi every 200 ms
+    where NVML cannot be loaded."""
 
     Q = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
          'clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,'
          'clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap')
+    REASONS = (('hw_slowdown', 0x8), ('hw_thermal_slowdown', 0x40), ('sw_thermal_slowdown', 0x20),
+               ('sw_power_cap', 0x4))
 
     def __init__(self, gpu_index):
-        self.gpu = str(gpu_index)
+        self.gpu = int(gpu_index)
         self.proc = None
         self.lines = []
+        self.samples = []  # (sm MHz, max sm MHz, reason bits)
+        self.stop = threading.Event()
+        self.nvml = None
 
     def __enter__(self):
         try:
-            self.proc = subprocess.Popen(['nvidia-smi', '-i', self.gpu, '--query-gpu=' + self.Q,
+            import pynvml
+            pynvml.nvmlInit()
+            self.nvml = pynvml
+            # the CUDA ordinal may differ from NVML's index when
+            # CUDA_VISIBLE_DEVICES is set: find the device by its UUID
+            h = None
+            try:
+                import torch
+                u = str(torch.cuda.get_device_properties(self.gpu).uuid)
+                h = pynvml.nvmlDeviceGetHandleByUUID(u if u.startswith('GPU-') else 'GPU-' + u)
+            except Exception:
+                h = None
+            self.h = h if h is not None else pynvml.nvmlDeviceGetHandleByIndex(self.gpu)
+            self.t = threading.Thread(target=self._poll, daemon=True)
+            self.t.start()
+            return self
+        except Exception:
+            self.nvml = None
+        try:
+            self.proc = subprocess.Popen(['nvidia-smi', '-i', str(self.gpu), '--query-gpu=' + self.Q,
                                           '--format=csv,noheader,nounits', '-lms', '200'],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
@@ -87,11 +114,30 @@ class ClockSampler(object):
             self.proc = None
         return self
 
+    def _poll(self):
+        n = self.nvml
+        while not self.stop.is_set():
+            try:
+                sm = n.nvmlDeviceGetClockInfo(self.h, n.NVML_CLOCK_SM)
+                smax = n.nvmlDeviceGetMaxClockInfo(self.h, n.NVML_CLOCK_SM)
+                r = n.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                self.samples.append((float(sm), float(smax), int(r)))
+            except Exception:
+                pass
+            self.stop.wait(0.02)
+
     def _read(self):
         for ln in self.proc.stdout:
             self.lines.append(ln.strip())
 
     def __exit__(self, *a):
+        self.stop.set()
+        if self.nvml is not None:
+            self.t.join(timeout=2)
+            try:
+                self.nvml.nvmlShutdown()
+            except Exception:
+                pass
         if self.proc is not None:
             self.proc.terminate()
             try:
@@ -102,7 +148,13 @@ class ClockSampler(object):
 
     def summary(self):
         sm, smax, reasons = [], [], set()
-        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
+        for f, fm, r in self.samples:
+            sm.append(f)
+            smax.append(fm)
+            for name, bit in self.REASONS:
+                if r & bit:
+                    reasons.add(name)
+        names = [n for n, _ in self.REASONS]
         for ln in self.lines:
             f = [x.strip() for x in ln.split(',')]
             if len(f) < 9:
@@ -118,7 +170,7 @@ class ClockSampler(object):
         if not sm:
             return {'sm_mhz': None, 'sm_max_mhz': None, 'reasons': [], 'samples': 0}
         return {'sm_mhz': statistics.median(sm), 'sm_max_mhz': max(smax), 'reasons': sorted(reasons),
-                'samples': len(sm)}
+                'samples': len(sm), 'source': 'nvml' if self.samples else 'nvidia-smi'}
 
 
 def read_peaks():
@@ -130,13 +182,15 @@ def read_peaks():
         return 6650.0, 'fallback'
 
 
-def read_profile_value(key):
+def read_profile_value(key, arithmetic='fast', precision='fp32'):
     """A per-cell-update figure of the stage kernel from the committed ncu
-    summary (profiles/visc_stage_*.txt, a line 'key: X'), or None."""
+    summary of that arithmetic and precision
+    (profiles/visc_stage_tiled_<arithmetic>_*_<precision>.txt, a line
+    'key: X'), or None."""
     d = os.path.join(ROOT, 'profiles')
     try:
         for fn in sorted(os.listdir(d)):
-            if fn.startswith('visc_stage') and fn.endswith('.txt'):
+            if fn.startswith('visc_stage_tiled_%s_' % arithmetic) and fn.endswith('_%s.txt' % precision):
                 for ln in open(os.path.join(d, fn)):
                     if ln.startswith(key + ':'):
                         return float(ln.split(':')[1])
@@ -145,19 +199,19 @@ def read_profile_value(key):
     return None
 
 
-def read_traffic():
+def read_traffic(arithmetic='fast', precision='fp32'):
     """DRAM bytes per cell-update of the stage kernel (committed ncu summary)."""
-    return read_profile_value('dram_bytes_per_cell_update')
+    return read_profile_value('dram_bytes_per_cell_update', arithmetic, precision)
 
 
-def issue_roofline(cell_updates_per_s, sm_mhz):
+def issue_roofline(cell_updates_per_s, sm_mhz, arithmetic='fast', precision='fp32'):
     """Warp instructions issued per second by the stage kernel (instructions
     per cell-update from the committed ncu summary, divided by 32, times
     cell-updates/s) against the SMs' issue peak: 4 schedulers x 1 warp
     instruction per cycle x the SM count x the SM clock sampled in the timed
     region."""
     import torch
-    inst = read_profile_value('instructions_per_cell_update')
+    inst = read_profile_value('instructions_per_cell_update', arithmetic, precision)
     if inst is None or not sm_mhz:
         return None
     sms = torch.cuda.get_device_properties(0).multi_processor_count
@@ -165,6 +219,47 @@ def issue_roofline(cell_updates_per_s, sm_mhz):
     peak = 4.0 * sms * sm_mhz * 1e6
     return {'achieved': achieved, 'peak': peak, 'unit': 'warp instructions/s', 'frac': achieved / peak,
             'instructions_per_cell_update': inst, 'sm_mhz': sm_mhz}
+
+
+def time_steps(v, warmup, steps, first=0):
+    """ms per fused step of the CLVisc v over `steps` steps after `warmup`
+    (CUDA events on the launch stream)."""
+    import torch
+    stream = torch.cuda.current_stream()
+    for n in range(first, first + warmup):
+        v.step(n)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for n in range(first + warmup, first + warmup + steps):
+        v.step(n)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def fp64_leg(nx, ny, nz, ic, peak, steps=5, warmup=2):
+    """The same workload in FP64, both arithmetics: ms per step, cell-updates/s
+    and the HBM fraction at 624 B per cell-update."""
+    import torch
+    from clvisc_b200.visc import CLVisc
+    out = {}
+    for arith in ('exact', 'fast'):
+        cfg = make_cfg(nz=nz, nx=nx, ny=ny, out='/tmp/clv_bench_fp64', fp64=True, arithmetic=arith)
+        v = CLVisc(cfg)
+        v.load_ini(ic)
+        ms = time_steps(v, warmup, steps)
+        rate = nx * ny * nz / (ms * 1e-3)
+        ach = rate * 2 * ALG_BYTES_PER_CELL_UPDATE / 1e9
+        t = read_traffic(arith, 'fp64')
+        out[arith] = {'ms_per_step': ms, 'cell_updates_per_s': rate, 'steps': steps, 'warmup': warmup,
+                      'roofline': {'achieved': ach, 'peak': peak, 'unit': 'GB/s', 'frac': ach / peak,
+                                   'alg_bytes_per_cell_update': 2 * ALG_BYTES_PER_CELL_UPDATE,
+                                   'traffic_bytes_per_cell_update': t}}
+        del v
+        torch.cuda.synchronize()
+    out['default'] = 'exact (cfg.arithmetic auto)'
+    return out
 
 
 def cpu_baseline(steps=5, warmup=0, nx=NX, ny=NY, nz=NZ, ic=None):
@@ -441,11 +536,12 @@ def run_gpu(args, rank, world, dist):
     d2h = out.nbytes / args.steps
 
     peak, peak_kind = read_peaks()
-    # FP64 moves twice the bytes; the committed traffic and instruction
-    # figures are the FP32 kernel's
+    # FP64 moves twice the bytes
     alg = ALG_BYTES_PER_CELL_UPDATE * (2 if args.fp64 else 1)
     achieved = value / world * alg / 1e9
-    traffic = None if args.fp64 else read_traffic()
+    arith = 'fast' if v.params.flags & 32 else 'exact'
+    precision = 'fp64' if args.fp64 else 'fp32'
+    traffic = read_traffic(arith, precision)
     real = 'double' if args.fp64 else 'float'
     if rank == 0:
         line = {
@@ -461,11 +557,12 @@ def run_gpu(args, rank, world, dist):
                          'frac': achieved / peak, 'peak_kind': peak_kind,
                          'traffic': None if traffic is None else traffic * cells / 2,
                          'alg_bytes_per_launch': alg * cells / 2,
-                         'kernel': 'visc_stage_tiled_kernel<%s,IS,KT> (2 launches per step)' % real},
+                         'kernel': 'clv::%s::visc_stage_tiled_kernel<%s,IS,KT> (2 launches per step)' % (arith, real)},
             'clocks': clocks.summary(),
         }
-        line['roofline']['issue'] = None if args.fp64 else issue_roofline(value / world,
-                                                                          line['clocks'].get('sm_mhz'))
+        line['roofline']['issue'] = issue_roofline(value / world, line['clocks'].get('sm_mhz'), arith, precision)
+        if not args.fp64 and not args.no_fp64 and world == 1:
+            line['fp64'] = fp64_leg(nx, ny, nz, ic, peak)
         if args.evolve and world == 1:
             line['evolve'] = evolve_to_freezeout(args, nx, ny, nz)
         if not args.no_cpu_baseline and not args.fp64:
@@ -499,6 +596,7 @@ def main():
     ap.add_argument('--surrogate-epochs', type=int, default=12)
     ap.add_argument('--surrogate-only', action='store_true', help='print only the surrogate experiment line')
     ap.add_argument('--fp64', action='store_true', help='the same workload in double precision')
+    ap.add_argument('--no-fp64', action='store_true', help='skip the FP64 object of the default line')
     ap.add_argument('--arithmetic', default='auto', choices=['auto', 'fast', 'exact'],
                     help='fused-stage arithmetic (auto: fast in FP32, exact in FP64)')
     ap.add_argument('--evolve', action='store_true',
