@@ -385,6 +385,7 @@ def run_batch(n_events=BATCH_EVENTS, one_at_a_time=True):
     cfg = batch_cfg()
     out = {'metric': 'events/h (%d seeded (2+1)D events, 121^2..301^2, to freeze-out)' % n_events,
            'unit': 'events/h', 'events': n_events, 'cells': int(sum(n * n for n, _, _ in specs)),
+           'arithmetic': 'fast' if cfg.use_float32 and cfg.arithmetic in ('auto', 'fast') else 'exact',
            'ic_host_s': ic_s}
     # autotuned launch shape (timed separately), then the timed batch from host arrays
     bt = CLViscBatch(cfg, grids)
@@ -443,11 +444,15 @@ def run_batch(n_events=BATCH_EVENTS, one_at_a_time=True):
             v.evolve(save_hypersf=False)
             singles.append(v.ideal.ev_to_host())
         t1 = time.perf_counter() - t
+        worst = 0.0
         for f, g in zip(singles, finals):  # bit patterns, so that NaN equals NaN
             differ += int(np.count_nonzero(f.view(np.uint32) != g.view(np.uint32)))
+            worst = max(worst, float(np.abs(f[:, 0].astype(np.float64) - g[:, 0]).max() / max(np.abs(g[:, 0]).max(),
+                                                                                                  1e-30)))
         out['one_at_a_time'] = {'value': n_events / t1 * 3600.0, 'unit': 'events/h', 'seconds': t1,
                                 'api': 'CLVisc(cfg); load_ini; evolve(save_hypersf=False); ev_to_host per event',
-                                'bitwise_equal_to_batch': differ == 0, 'values_differing': differ}
+                                'bitwise_equal_to_batch': differ == 0, 'values_differing': differ,
+                                'max_scaled_energy_density_difference': worst}
         out['speedup_e2e'] = out['e2e']['value'] / out['one_at_a_time']['value']
     return out
 

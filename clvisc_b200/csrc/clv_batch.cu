@@ -5,6 +5,8 @@
 
 #include "../../include/clvisc_b200.h"
 #include "clv_batch.cuh"
+#include "clv_batch_launch.cuh"
+#include "clv_fast.h"
 
 namespace clv_host {
 int params_from_abi(const clv_params* in, clv::Params* out);
@@ -16,12 +18,6 @@ namespace {
 
 inline cudaStream_t S(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 
-// the current device (launch set-up is cached per device), or -1
-constexpr int kMaxDevices = 64;
-inline int current_device() {
-  int d = 0;
-  return (cudaGetDevice(&d) == cudaSuccess && d >= 0 && d < kMaxDevices) ? d : -1;
-}
 
 static_assert(sizeof(clv_batch_event) == sizeof(clv::BatchEvent), "clv_batch_event layout");
 static_assert(sizeof(clv_batch_ctl) == sizeof(clv::BatchCtl), "clv_batch_ctl layout");
@@ -64,46 +60,6 @@ int make_args(const clv_params* pp, const clv_batch* b, clv::Params* p, clv::Bat
   return CLV_OK;
 }
 
-template <class real, bool BULK, int BS, int MINB>
-int launch_stage(const clv::Params& p, const clv::BatchArgs<real>& a, int step, int grid, cudaStream_t s) {
-  auto kern = clv::batch_stage_kernel<real, BULK, BS, MINB>;
-  if (grid <= 0) {
-    int dev = 0, sms = 0, per_sm = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, BS, 0);
-    grid = sms * (per_sm > 0 ? per_sm : 1);
-  }
-  kern<<<grid, BS, 0, s>>>(p, a, step);
-  return clv_host::check_cuda("batch_stage_kernel");
-}
-
-// the register caps are offered in FP32 only (FP64 spills heavily under
-// them): 128 registers a thread (512 threads per SM) or, for 64- and
-// 128-thread blocks, 168 (384 threads per SM)
-template <class real> constexpr int capped_minb(int bs) { return sizeof(real) == 4 ? 512 / bs : 1; }
-template <class real> constexpr int capped168_minb(int bs) { return sizeof(real) == 4 ? 384 / bs : 1; }
-
-template <class real, bool BULK>
-int stage_bs(const clv::Params& p, const clv::BatchArgs<real>& a, int step, int bs, int grid, int cap,
-             cudaStream_t s) {
-  if (cap && sizeof(real) == 8) return clv_host::set_error(CLV_ERR_INVALID, "batch: max_registers is FP32 only");
-  if (cap == 168 && bs == 256)
-    return clv_host::set_error(CLV_ERR_INVALID, "batch: max_registers 168 needs 64- or 128-thread blocks");
-  if (bs == 64 && cap == 168) return launch_stage<real, BULK, 64, capped168_minb<real>(64)>(p, a, step, grid, s);
-  if (bs == 128 && cap == 168) return launch_stage<real, BULK, 128, capped168_minb<real>(128)>(p, a, step, grid, s);
-  if (bs == 64)
-    return cap ? launch_stage<real, BULK, 64, capped_minb<real>(64)>(p, a, step, grid, s)
-               : launch_stage<real, BULK, 64, 1>(p, a, step, grid, s);
-  if (bs == 128)
-    return cap ? launch_stage<real, BULK, 128, capped_minb<real>(128)>(p, a, step, grid, s)
-               : launch_stage<real, BULK, 128, 1>(p, a, step, grid, s);
-  if (bs == 256)
-    return cap ? launch_stage<real, BULK, 256, capped_minb<real>(256)>(p, a, step, grid, s)
-               : launch_stage<real, BULK, 256, 1>(p, a, step, grid, s);
-  return clv_host::set_error(CLV_ERR_INVALID, "batch: block_size must be 64, 128 or 256");
-}
-
 template <class real>
 int batch_stage_t(const clv_params* pp, int step, const clv_batch* b, int bs, int grid, int max_regs,
                   cudaStream_t s) {
@@ -117,31 +73,9 @@ int batch_stage_t(const clv_params* pp, int step, const clv_batch* b, int bs, in
   if (max_regs != 0 && max_regs != 128 && max_regs != 168)
     return clv_host::set_error(CLV_ERR_INVALID, "batch: max_registers must be 0, 128 or 168");
   const int cap = max_regs;
-  if (p.flags & clv::FLAG_BULK) return stage_bs<real, true>(p, a, step, bs, grid, cap, s);
-  return stage_bs<real, false>(p, a, step, bs, grid, cap, s);
-}
-
-template <class real, bool BULK, int TB>
-int launch_tiled(const clv::Params& p, const clv::BatchArgs<real>& a, int step, int chunk, int grid, cudaStream_t s) {
-  typedef clv::Tile2Smem<real, BULK, TB> SM;
-  auto kern = clv::batch_tiled2d_kernel<real, BULK, TB, clv::tiled2d_minb<real, TB>()>;
-  static bool configured[kMaxDevices] = {};  // launch attributes are per device
-  const int cdev = current_device();
-  if (cdev < 0) return clv_host::check_cuda("cudaGetDevice");
-  if (!configured[cdev]) {
-    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SM)) != cudaSuccess)
-      return clv_host::check_cuda("cudaFuncSetAttribute(batch_tiled2d_kernel)");
-    configured[cdev] = true;
-  }
-  if (grid <= 0) {
-    int dev = 0, sms = 0, per_sm = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, TB, sizeof(SM));
-    grid = sms * (per_sm > 0 ? per_sm : 1);
-  }
-  kern<<<grid, TB, sizeof(SM), s>>>(p, a, step, chunk);
-  return clv_host::check_cuda("batch_tiled2d_kernel");
+  if (p.flags & clv::FLAG_FAST) return clv_fastpath::batch_stage<real>(p, a, step, bs, grid, cap, s);
+  if (p.flags & clv::FLAG_BULK) return clv::batch_launch::stage_bs<real, true>(p, a, step, bs, grid, cap, s);
+  return clv::batch_launch::stage_bs<real, false>(p, a, step, bs, grid, cap, s);
 }
 
 template <class real>
@@ -155,14 +89,9 @@ int batch_stage_tiled_t(const clv_params* pp, int step, const clv_batch* b, int 
   if (p.flags & (clv::FLAG_GUBSER_VISC | clv::FLAG_PIMN_OMEGA | clv::FLAG_OMEGA_OMEGA | clv::FLAG_RIEMANN))
     return clv_host::set_error(CLV_ERR_INVALID, "batch: test flags (Gubser, couplings, Riemann) are not batched");
   if (chunk < 1 || chunk > 4096) return clv_host::set_error(CLV_ERR_INVALID, "batch: chunk must be in 1..4096");
-  const bool bulk = p.flags & clv::FLAG_BULK;
-  if (rows == 64)
-    return bulk ? launch_tiled<real, true, 64>(p, a, step, chunk, grid, s)
-                : launch_tiled<real, false, 64>(p, a, step, chunk, grid, s);
-  if (rows == 128)
-    return bulk ? launch_tiled<real, true, 128>(p, a, step, chunk, grid, s)
-                : launch_tiled<real, false, 128>(p, a, step, chunk, grid, s);
-  return clv_host::set_error(CLV_ERR_INVALID, "batch: rows must be 64 or 128");
+  if (rows != 64 && rows != 128) return clv_host::set_error(CLV_ERR_INVALID, "batch: rows must be 64 or 128");
+  if (p.flags & clv::FLAG_FAST) return clv_fastpath::batch_stage_tiled<real>(p, a, step, rows, chunk, grid, s);
+  return clv::batch_launch::stage_tiled<real>(p, a, step, rows, chunk, grid, s);
 }
 
 template <class real, bool BULK, int TB> int occupancy_tiled(int* n) {
@@ -243,9 +172,9 @@ int clv_batch_occupancy(const clv_params* p, int block_size, int max_registers, 
 #define CLV_K(real, B, BS, M) f = reinterpret_cast<const void*>(clv::batch_stage_kernel<real, B, BS, M>)
 #define CLV_PICK(real, B)                                                  \
   do {                                                                     \
-    if (block_size == 64) { if (cap168) CLV_K(real, B, 64, capped168_minb<real>(64)); else if (cap) CLV_K(real, B, 64, capped_minb<real>(64)); else CLV_K(real, B, 64, 1); }     \
-    else if (block_size == 128) { if (cap168) CLV_K(real, B, 128, capped168_minb<real>(128)); else if (cap) CLV_K(real, B, 128, capped_minb<real>(128)); else CLV_K(real, B, 128, 1); } \
-    else { if (cap) CLV_K(real, B, 256, capped_minb<real>(256)); else CLV_K(real, B, 256, 1); } \
+    if (block_size == 64) { if (cap168) CLV_K(real, B, 64, clv::batch_launch::capped168_minb<real>(64)); else if (cap) CLV_K(real, B, 64, clv::batch_launch::capped_minb<real>(64)); else CLV_K(real, B, 64, 1); }     \
+    else if (block_size == 128) { if (cap168) CLV_K(real, B, 128, clv::batch_launch::capped168_minb<real>(128)); else if (cap) CLV_K(real, B, 128, clv::batch_launch::capped_minb<real>(128)); else CLV_K(real, B, 128, 1); } \
+    else { if (cap) CLV_K(real, B, 256, clv::batch_launch::capped_minb<real>(256)); else CLV_K(real, B, 256, 1); } \
   } while (0)
   if (p->precision == 4) {
     if (bulk) CLV_PICK(float, true);

@@ -61,6 +61,8 @@ template <class real> struct BatchArgs {
   int ntskip, max_loops;
 };
 
+inline namespace CLV_ARITH {
+
 // tau in the run precision after `n` steps: real(TAU0 + n*DT) as the host
 // forms it (ideal.py:317-320; n = 0 gives real(TAU0))
 template <class real> __device__ __forceinline__ real batch_tau(double tau0, double dt, int n) {
@@ -262,4 +264,5 @@ template <class real> __global__ void __launch_bounds__(1024) batch_advance_kern
   }
 }
 
+}  // namespace CLV_ARITH
 }  // namespace clv

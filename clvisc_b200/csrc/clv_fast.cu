@@ -6,18 +6,15 @@
 // product with the reciprocal, the EOS texel index straight from e / step,
 // sign-test minmod, the KT speed max(lambda, 1) as 1, one atomic per warp for
 // the max energy density). Its functions and kernels live in clv::fast, so
-// they link beside the exact ones in clv::exact.
+// they link beside the exact ones in clv::exact. The batched stage kernels
+// (clv_batch.cuh) come in this arithmetic too.
 #define CLV_FAST 1
 #include <string>
 
 #include "../../include/clvisc_b200.h"
 #include "clv_fast.h"
+#include "clv_batch_launch.cuh"
 #include "clv_stage_tiled.cuh"
-
-namespace clv_host {
-int set_error(int code, const std::string& msg);
-int check_cuda(const char* where);
-}  // namespace clv_host
 
 namespace clv_fastpath {
 namespace {
@@ -74,6 +71,26 @@ int visc_stage(const clv::Params& p, const clv::ViscBuffers<real>& v, int step, 
   }
   return clv_host::check_cuda("fast visc_stage_kernel");
 }
+
+template <class real>
+int batch_stage(const clv::Params& p, const clv::BatchArgs<real>& a, int step, int bs, int grid, int cap,
+                cudaStream_t s) {
+  if (p.flags & clv::FLAG_BULK) return clv::batch_launch::stage_bs<real, true>(p, a, step, bs, grid, cap, s);
+  return clv::batch_launch::stage_bs<real, false>(p, a, step, bs, grid, cap, s);
+}
+
+template <class real>
+int batch_stage_tiled(const clv::Params& p, const clv::BatchArgs<real>& a, int step, int rows, int chunk, int grid,
+                      cudaStream_t s) {
+  return clv::batch_launch::stage_tiled<real>(p, a, step, rows, chunk, grid, s);
+}
+
+template int batch_stage<float>(const clv::Params&, const clv::BatchArgs<float>&, int, int, int, int, cudaStream_t);
+template int batch_stage<double>(const clv::Params&, const clv::BatchArgs<double>&, int, int, int, int, cudaStream_t);
+template int batch_stage_tiled<float>(const clv::Params&, const clv::BatchArgs<float>&, int, int, int, int,
+                                      cudaStream_t);
+template int batch_stage_tiled<double>(const clv::Params&, const clv::BatchArgs<double>&, int, int, int, int,
+                                       cudaStream_t);
 
 template int visc_stage<float>(const clv::Params&, const clv::ViscBuffers<float>&, int, const clv::TauConst<float>&,
                                const clv::StageOpts&, cudaStream_t);

@@ -9,6 +9,7 @@
 
 namespace clv {
 template <class real> struct ViscBuffers;
+template <class real> struct BatchArgs;
 }
 
 namespace clv_fastpath {
@@ -16,4 +17,12 @@ namespace clv_fastpath {
 template <class real>
 int visc_stage(const clv::Params& p, const clv::ViscBuffers<real>& v, int step, const clv::TauConst<real>& tc,
                const clv::StageOpts& o, cudaStream_t s);
+// one stage of a batch of events, one thread per cell (block size bs, grid
+// blocks, register cap 0 / 128 / 168) or (2+1)D tiles of rows - 4 rows
+template <class real>
+int batch_stage(const clv::Params& p, const clv::BatchArgs<real>& a, int step, int bs, int grid, int cap,
+                cudaStream_t s);
+template <class real>
+int batch_stage_tiled(const clv::Params& p, const clv::BatchArgs<real>& a, int step, int rows, int chunk, int grid,
+                      cudaStream_t s);
 }  // namespace clv_fastpath

@@ -50,6 +50,8 @@ template <class real, bool BULK, int TB> struct Tile2Smem {
   real FY[R::NCOMP][TB];  // flux through the y face between rows t and t+1
 };
 
+inline namespace CLV_ARITH {
+
 // record of the (clamped) cell (i, j) of the stage input, NZ = 1
 template <class real, bool BULK>
 __device__ __forceinline__ void rec2_make(const Params& p, const GridDims& gd, const ViscBuffers<real>& b, real tau,
@@ -362,4 +364,5 @@ __global__ void __launch_bounds__(TB, MINB)
   tile2d<real, BULK, TB>(p, gd, b, step, tc, blockIdx.x * (TB - 4), i0, min(i0 + chunk, p.nx), s);
 }
 
+}  // namespace CLV_ARITH
 }  // namespace clv

@@ -130,3 +130,37 @@ def test_batch_tiled_equals_per_cell(cuda_lib, use_float32, bulk):
         for e in range(len(GRIDS_2D)):
             for name, got, want in zip(('ev', 'pi', 'Pi', 'ev[2]'), run[e], runs[0][e]):
                 assert_same('%s event %d %s' % (name, e, shape), got, want)
+
+
+@pytest.mark.parametrize('bulk', [False, True])
+def test_fast_batch_matches_fast_single_runs(cuda_lib, bulk):
+    """The batched stage in tolerance arithmetic (CLV_FLAG_FAST): every event
+    stops at the same step as a CLVisc run of it alone in the same arithmetic,
+    and its fields agree within the fast build's tolerance (the two evaluate
+    the same per-cell function; the check does not rely on the compiler
+    contracting it identically in both kernels)."""
+    from clvisc_b200.batch import CLViscBatch
+    from clvisc_b200.eos import Eos
+    from clvisc_b200.visc import CLVisc
+    from test_fast_gpu import field_errors
+    ics = _ics(True, bulk)
+    cfg0 = _cfg(GRIDS[0], True, bulk, arithmetic='fast')
+    b = CLViscBatch(cfg0, GRIDS)
+    assert b.params.flags & 32
+    for e, ic in enumerate(ics):
+        b.load_ini(e, ic)
+    b.evolve()
+    loops = b.loops()
+    eos = Eos(cfg0.eos_type)
+    bitwise = 0
+    for e, (g, ic) in enumerate(zip(GRIDS, ics)):
+        v = CLVisc(_cfg(g, True, bulk, arithmetic='fast'))
+        v.load_ini(ic)
+        v.evolve(save_hypersf=False)
+        assert loops[e] == (len(v.ideal.history) - 1) * 4
+        got_ev, got_pi = b.ev_to_host(e), b.pi_to_host(e)
+        want_ev, want_pi = v.ideal.field_to_host(v.ideal.d_ev[1]), v.pi_to_host(1)
+        errs = field_errors(got_ev, want_ev, got_pi, want_pi, eos, float(v.ideal.tau))
+        assert max(errs['e'], errs['T'], errs['pi']) <= 1e-5, (e, errs)
+        bitwise += int(np.array_equal(got_ev, want_ev) and np.array_equal(got_pi, want_pi))
+    print('fast batch: %d of %d events bit for bit equal to their single runs' % (bitwise, len(GRIDS)))
