@@ -9,8 +9,9 @@
 //
 // Compiled with CLV_FAST=1 (the tolerance build, clv_fast.cu: FMA
 // contraction, approximate division and square root) the same headers give the
-// fast arithmetic: division by run constants through their reciprocals, the
-// EOS texel index straight from e / step, the limiters in sign-test form and
+// fast arithmetic: division by run constants through their reciprocals (the
+// EOS lookup included: the reference's row and column arithmetic, with its
+// float-rounded row width, is kept), the limiters in sign-test form and
 // the KT speed max(lambda, 1) taken as 1 (lambda <= 1 for |v| < 1 and
 // c_s^2 <= 1). Functions and kernels live in an inline namespace named after
 // the arithmetic (clv::exact or clv::fast), so both builds link into one
@@ -166,22 +167,6 @@ template <class real> __device__ __forceinline__ real div_step(real x, int step)
 #endif
 template <class real> __device__ __forceinline__ EosSpot<real> eos_spot(const Params& p, real eps) {
   const Recips<real>& rc = recips<real>(p);
-#if CLV_FAST
-  // tolerance build: texel t = floor((e - start) / step) of the row-major
-  // image, the next texel, and the fraction between them; outside the table
-  // both indices clamp to its edge as the image's clamp-to-edge does (the
-  // reference's row-boundary rounding quirk is not reproduced)
-  {
-    const real t = (eps - (real)p.eos_start) * rc.eos_step;
-    const int last = p.eos_nrow * p.eos_ncol - 1;
-    const int i0 = (int)t;
-    EosSpot<real> s;
-    s.t0 = min(max(i0, 0), last);
-    s.t1 = min(max(i0 + 1, 0), last);
-    s.r = t - (real)i0;
-    return s;
-  }
-#endif
   real ed_per_row = p.eos_step * p.eos_ncol;
   int row = (int)div_by<real>(eps, ed_per_row, rc.eos_epr);
   int col = (int)div_by<real>(eps - p.eos_start - row * ed_per_row, (real)p.eos_step, rc.eos_step);
@@ -467,9 +452,11 @@ __device__ __forceinline__ unsigned long long fkey(double f) {
   return (b & 0x8000000000000000ull) ? ~b : (b | 0x8000000000000000ull);
 }
 // atomicMax of the ordered key of f into *key; the tolerance build first takes
-// the maximum over the warp's active lanes (hardware warp reduction; 64-bit
-// keys as the high word, then the low word among the lanes holding the
-// largest high word) so that one lane issues the atomic
+// the maximum over the active lanes of the warp that update the same key (a
+// warp of the batched kernel can span several events), by hardware warp
+// reductions over the lanes __match_any_sync groups (64-bit keys as the high
+// word, then the low word among the lanes holding the largest high word), so
+// that one lane of each group issues the atomic
 __device__ __forceinline__ unsigned int warp_max_key(unsigned int m, unsigned int k) { return __reduce_max_sync(m, k); }
 __device__ __forceinline__ unsigned long long warp_max_key(unsigned int m, unsigned long long k) {
   const unsigned int hi = __reduce_max_sync(m, (unsigned int)(k >> 32));
@@ -481,7 +468,7 @@ template <class real> __device__ __forceinline__ void key_max(typename KeyT<real
   const bool ok = (f == f);
   K k = ok ? fkey(f) : (K)0;
 #if CLV_FAST
-  const unsigned int m = __activemask();
+  const unsigned int m = __match_any_sync(__activemask(), (unsigned long long)key);
   k = warp_max_key(m, k);
   if ((threadIdx.x & 31) == (unsigned int)(__ffs(m) - 1) && k != (K)0) atomicMax(key, k);
 #else

@@ -3,9 +3,8 @@
 // This translation unit compiles the same stage headers as the exact build
 // with CLV_FAST=1 and --fmad=true -prec-div=false -prec-sqrt=false, which
 // selects the fast branches of clv_device.cuh (division by run constants as a
-// product with the reciprocal, the EOS texel index straight from e / step,
-// sign-test minmod, the KT speed max(lambda, 1) as 1, one atomic per warp for
-// the max energy density). Its functions and kernels live in clv::fast, so
+// product with the reciprocal, sign-test minmod, the KT speed max(lambda, 1)
+// as 1, one atomic per warp and event for the max energy density). Its functions and kernels live in clv::fast, so
 // they link beside the exact ones in clv::exact. The batched stage kernels
 // (clv_batch.cuh) come in this arithmetic too.
 #define CLV_FAST 1

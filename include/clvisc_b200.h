@@ -52,8 +52,8 @@ extern "C" {
 /* Tolerance arithmetic for the fused viscous stage (both parts in one
  * launch), an option with no counterpart in the reference: the kernels are
  * compiled with fused multiply-add contraction and approximate division and
- * square root, divide by run constants through their reciprocals, index the
- * EOS image by e / step, evaluate the minmod limiters in sign-test form and
+ * square root, divide by run constants through their reciprocals, evaluate
+ * the minmod limiters in sign-test form and
  * take the KT speed max(lambda, 1) as 1 (lambda <= 1 for |v| < 1). Results
  * differ from the reference's arithmetic by rounding: within 1e-5 of each
  * field's largest magnitude in FP32 after the tested step counts. Without the
