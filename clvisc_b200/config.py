@@ -92,10 +92,10 @@ def read_config(argv=None, info_path=None):
         'BSZ': (gi('opencl', 'local_workgroup_size'), 'work-group size (accepted, unused)'),
         # arithmetic of the fused viscous stage (no counterpart in the
         # reference): 'exact' reproduces the reference's arithmetic bit for
-        # bit; 'fast' contracts multiply-adds and divides through reciprocals
-        # (within 1e-5 of each field's scale in FP32); 'auto' is fast in FP32
-        # and exact in FP64
-        'arithmetic': ('auto', 'fused-stage arithmetic: auto, fast or exact'),
+        # bit; 'fast' (the default; 'auto' is the same) contracts
+        # multiply-adds and divides through reciprocals, within 1e-5 (FP32) /
+        # 1e-11 (FP64) of each field's scale
+        'arithmetic': ('fast', 'fused-stage arithmetic: fast or exact'),
     }
     parser = argparse.ArgumentParser(description='CLVisc B200 hydro configuration')
     for key, (val, hlp) in config.items():

@@ -76,7 +76,7 @@ int to_params(const clv_params* in, clv::Params* out) {
   p.ZETAOS_WIDTH = in->zetaos_width; p.ZETAOS_SKEW = in->zetaos_skew; p.ZETAOS_TMIN = in->zetaos_tmin;
   p.opt[0] = in->opt_stage_kernel; p.opt[1] = in->opt_chunk; p.opt[2] = in->opt_tiled_blocks; p.opt[3] = in->opt_tile;
   if (in->opt_stage_kernel < 0 || in->opt_stage_kernel > 4 || in->opt_chunk < 0 || in->opt_chunk > 4096 ||
-      in->opt_tiled_blocks < 0 || in->opt_tiled_blocks > 2 || in->opt_tile < 0 || in->opt_tile > 3)
+      in->opt_tiled_blocks < 0 || in->opt_tiled_blocks > 2 || in->opt_tile < 0 || in->opt_tile > 4)
     return fail(CLV_ERR_INVALID, "opt_* fields out of range%s");
   if ((in->flags & CLV_FLAG_BULK) && (!(in->zetaos_width > 0.0f) || !(in->zetaos_max >= 0.0f)))
     return fail(CLV_ERR_INVALID, "bulk sector: zetaos_width must be > 0 and zetaos_max >= 0%s");
@@ -333,7 +333,7 @@ int clv_set_option(int option, int value) {
     g_minb = value;
     return CLV_OK;
   }
-  if (option == CLV_OPT_TILE && value >= 0 && value <= 2) {
+  if (option == CLV_OPT_TILE && value >= 0 && value <= 3) {
     g_tile = value;
     return CLV_OK;
   }

@@ -53,6 +53,8 @@ int visc_stage(const clv::Params& p, const clv::ViscBuffers<real>& v, int step, 
     if (cpl) return launch_tiled<real, true, 1, 8, 32>(p, v, step, tc, o.chunk, s);
     if constexpr (sizeof(real) == 8) return launch_tiled<real, false, 1, 8, 32>(p, v, step, tc, o.chunk, s);
     else {
+      // 16 x 32 (y, eta) tiles, one 512-thread CTA an SM: less halo than two 8 x 32 CTAs
+      if (o.tile == 3) return launch_tiled<real, false, 1, 16, 32>(p, v, step, tc, o.chunk, s);
       if (o.minb == 1) return launch_tiled<real, false, 1, 8, 32>(p, v, step, tc, o.chunk, s);
       return launch_tiled<real, false, 2, 8, 32>(p, v, step, tc, o.chunk, s);
     }

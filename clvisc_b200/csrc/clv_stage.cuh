@@ -167,6 +167,16 @@ __device__ __forceinline__ void pi_update(const Params& p, const ViscBuffers<rea
   const real den = u_new[0] + p.DT * one_over_taupi;
   const real rden = (real)1.0f / den;
   real max_pimn_abs = 0.0f;
+#if CLV_FAST
+  // tolerance build: the transversality terms of every component,
+  // (u^mu pi^{nu lam} + u^nu pi^{mu lam}) Du_lam, from the lowered vector
+  // W^mu = pi^{mu lam} g_{lam lam} Du^lam, formed once
+  real Wv[4];
+#pragma unroll
+  for (int q = 0; q < 4; q++)
+    Wv[q] = pc[pidx(q, 0)] * DU[0] - pc[pidx(q, 1)] * DU[1] - pc[pidx(q, 2)] * DU[2] - pc[pidx(q, 3)] * DU[3];
+  const real r3 = (real)1.0f / 3.0f;
+#endif
 #pragma unroll
   for (int mu = 0; mu < 4; mu++)
 #pragma unroll
@@ -179,11 +189,15 @@ __device__ __forceinline__ void pi_update(const Params& p, const ViscBuffers<rea
       if (u[0] > 10000.0f) sigma = 0.0f;
       real piNS = etav * sigma;
       real pi_old = b.pi1[mn * ld + I] * u_old[0];
+#if CLV_FAST
+      real src = -pc[mn] * (theta * r3 + u[0] * tc.rtau) - (u[mu] * Wv[nu] + u[nu] * Wv[mu]);
+#else
       real src = div_by<real>(-pc[mn] * theta, (real)3.0f, rc.three) - div_by<real>(pc[mn] * u[0], tau, tc.rtau);
       src -= (u[mu] * pc[pidx(nu, 0)] + u[nu] * pc[pidx(mu, 0)]) * DU[0] * gmn<real>(0, 0);
       src -= (u[mu] * pc[pidx(nu, 1)] + u[nu] * pc[pidx(mu, 1)]) * DU[1] * gmn<real>(1, 1);
       src -= (u[mu] * pc[pidx(nu, 2)] + u[nu] * pc[pidx(mu, 2)]) * DU[2] * gmn<real>(2, 2);
       src -= (u[mu] * pc[pidx(nu, 3)] + u[nu] * pc[pidx(mu, 3)]) * DU[3] * gmn<real>(3, 3);
+#endif
       if (COUPLED && (p.flags & FLAG_GUBSER_VISC))
         src -= one_over_taupi * coef_pipi *
                (pipi<real>(0, mu, nu, pc, u) - pipi<real>(1, mu, nu, pc, u) - pipi<real>(2, mu, nu, pc, u) -

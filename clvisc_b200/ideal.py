@@ -81,11 +81,12 @@ def add_visc_params(c, p):
 
 def fast_arithmetic(c):
     """Whether the fused viscous stage runs in the tolerance arithmetic
-    (CLV_FLAG_FAST): cfg.arithmetic 'fast', or 'auto' (the default) in FP32."""
-    mode = str(getattr(c, 'arithmetic', 'auto')).lower()
+    (CLV_FLAG_FAST): cfg.arithmetic 'fast' (the default) or 'auto'; 'exact'
+    keeps the reference's arithmetic bit for bit."""
+    mode = str(getattr(c, 'arithmetic', 'fast')).lower()
     if mode not in ('auto', 'fast', 'exact'):
-        raise ValueError("cfg.arithmetic must be 'auto', 'fast' or 'exact', not %r" % mode)
-    return mode == 'fast' or (mode == 'auto' and bool(c.use_float32))
+        raise ValueError("cfg.arithmetic must be 'fast' or 'exact' ('auto' = 'fast'), not %r" % mode)
+    return mode != 'exact'
 
 
 def load_eos(cfg, handcrafted_eos, device):

@@ -12,9 +12,11 @@ concatenation, a 1x1 head to 6 channels.
 
 The solver is the judge and the fallback: training and test events come from
 the batched solver (CLViscBatch) on seeded initial conditions, the error of the
-network is measured against solver results, and events whose predicted
-transverse energy strays from the value the training events relate to their
-initial transverse energy are run by the solver instead.
+network is measured against solver results, and an event is run by the solver
+instead when its prediction fails the energy balance (its transverse energy
+strays from the value the training events relate to their initial profile) or
+when the predictions for the event and its mirror images disagree by more than
+a threshold calibrated on held-out training events.
 """
 import ctypes
 import math
@@ -413,6 +415,47 @@ class Surrogate(object):
         return out
 
 
+# The evolution commutes with the reflections of the grid's x and y axes
+# (the stencil, the limiters and the initial-condition construction, whose
+# impact parameter lies along x, are all mirror symmetric): the fields of a
+# mirrored initial condition are the mirrored fields, with u^x (x mirror),
+# u^y (y mirror) and pi^xy (either) changing sign.
+_FLIPS = ((), (1,), (2,), (1, 2))  # axes of (E, n, n) inputs to reverse
+_SIGN = {(): (1, 1, 1, 1, 1, 1), (1,): (1, -1, 1, 1, -1, 1), (2,): (1, 1, -1, 1, -1, 1),
+         (1, 2): (1, -1, -1, 1, 1, 1)}
+
+
+def predict_mirrored(sur, x):
+    """The network on x and its three mirror images, each prediction mapped
+    back: returns (mean over the four (E, n, n, 6), per-event spread of the
+    energy density: the largest relative L2 distance of one of the four from
+    their mean)."""
+    preds = []
+    for ax in _FLIPS:
+        xin = torch.flip(x, dims=ax) if ax else x
+        out = sur.predict(xin.contiguous())
+        if ax:
+            out = torch.flip(out, dims=ax)
+        sign = torch.tensor(_SIGN[ax], dtype=out.dtype, device=out.device)
+        preds.append(out * sign)
+    stack = torch.stack(preds)
+    mean = stack.mean(0)
+    spread = torch.stack([rel_l2(q[..., 0], mean[..., 0]) for q in preds]).amax(0)
+    return mean, spread
+
+
+def calibrate_threshold(score, err, bad=0.02, keep_frac=0.01):
+    """The largest threshold on `score` for which, on calibration events,
+    at most keep_frac of the events would be kept (score <= threshold) with an
+    error above `bad`; events above the threshold go to the solver."""
+    order = torch.argsort(score)
+    s_sorted, bad_sorted = score[order], (err[order] > bad).double()
+    kept_bad = torch.cumsum(bad_sorted, 0)  # bad events among those at or below each score
+    ok = kept_bad <= keep_frac * score.numel()
+    idx = int(torch.nonzero(ok)[-1]) if bool(ok.any()) else -1
+    return float(s_sorted[idx]) if idx >= 0 else float('-inf')
+
+
 def transverse_energy(fields, eos_p, tau, dx):
     """tau * sum over the slice of T^{tau tau} = (e + P) u0^2 - P, u0^2 = 1 + ux^2 + uy^2."""
     e = fields[..., 0]
@@ -480,6 +523,12 @@ def run_experiment(n_train=20000, n_test=1000, epochs=12, batch=32, n=128, steps
     res['solver_s'] = t_solver
     res['solver_events_per_h'] = n_test / t_solver * 3600.0
     log('solver: %d test events in %.2f s' % (n_test, t_solver))
+    # the last 5 % of the training events calibrate the fallback threshold
+    # and are not trained on
+    n_cal = max(32, xtr.shape[0] // 20)
+    xcal, ycal = xtr[-n_cal:], ytr[-n_cal:]
+    xtr, ytr = xtr[:-n_cal], ytr[:-n_cal]
+    res['calibration_events'] = int(n_cal)
     sur = Surrogate(batch, n)
     t = time.perf_counter()
     hist = sur.train(xtr, ytr, epochs=epochs, lr=lr, log=log)
@@ -487,12 +536,14 @@ def run_experiment(n_train=20000, n_test=1000, epochs=12, batch=32, n=128, steps
     res['train_s'] = time.perf_counter() - t
     log('trained %d epochs in %.1f s' % (epochs, res['train_s']))
     res['loss_history'] = [round(h, 6) for h in hist]
-    # inference, timed
+    # inference, timed: the network on each event and its three mirror
+    # images, averaged; their spread is the network's own error estimate
     torch.cuda.synchronize()
     t = time.perf_counter()
-    pred = sur.predict(xte)
+    pred, spread = predict_mirrored(sur, xte)
     torch.cuda.synchronize()
     t_inf = time.perf_counter() - t
+    pred_single = sur.predict(xte)
     err = rel_l2(pred[..., 0], yte[..., 0])
     # the method without the network: Bjorken cooling of the initial profile
     tau0, tau1 = 0.6, 0.6 + steps * 0.02
@@ -515,7 +566,24 @@ def run_experiment(n_train=20000, n_test=1000, epochs=12, batch=32, n=128, steps
     e1 = ((ic_features(xte, tau0, 0.16, Pf)[:, [0, 5]] / scale[[0, 5]]) @ c1).float()
     res['fallback_events_one_feature'] = int(((transverse_energy(pred, Pf, tau1, 0.16) - e1).abs() / e1.abs()
                                               > residual_max).sum())
-    rerun = resid > residual_max
+    # the fallback: an event goes to the solver when the energy-balance
+    # residual of its prediction exceeds residual_max, or the spread of its
+    # mirrored predictions exceeds a threshold calibrated on held-out training
+    # events (at most 1 % of them kept with an error above 2 %, the balance
+    # test applied first)
+    pcal, scal = predict_mirrored(sur, xcal)
+    ecal = rel_l2(pcal[..., 0], ycal[..., 0])
+    et_cal = ((ic_features(xcal, tau0, 0.16, Pf) / scale) @ coef).float()
+    rcal = (transverse_energy(pcal, Pf, tau1, 0.16) - et_cal).abs() / et_cal.abs()
+    keep_cal = rcal <= residual_max
+    spread_max = calibrate_threshold(torch.where(keep_cal, scal, torch.full_like(scal, float('inf'))), ecal)
+    res['spread_threshold'] = spread_max
+    res['calibration'] = {'events': int(n_cal), 'err_mean': float(ecal.mean()),
+                          'rerun_frac': float(((~keep_cal) | (scal > spread_max)).float().mean())}
+    res['fallback_balance_only'] = int((resid > residual_max).sum())
+    res['kept_events_above_2pct_balance_only'] = int(((rel_l2(pred[..., 0], yte[..., 0]) > 0.02) &
+                                                      (resid <= residual_max)).sum())
+    rerun = (resid > residual_max) | (spread > spread_max)
     net_err = rel_l2(pred[..., 0], yte[..., 0])
     res['kept_events_above_2pct'] = int(((net_err > 0.02) & ~rerun).sum())
     n_rerun = int(rerun.sum())
@@ -538,7 +606,9 @@ def run_experiment(n_train=20000, n_test=1000, epochs=12, batch=32, n=128, steps
         'speedup_vs_solver': t_solver / (t_inf + t_fb),
         'rel_l2_e': {'mean': float(err.mean()), 'median': float(err.median()), 'p90': float(err.quantile(0.9)),
                      'max': float(err.max()), 'frac_le_2pct': float((err <= 0.02).float().mean())},
-        'rel_l2_e_network_only': {'mean': float(rel_l2(pred[..., 0], yte[..., 0]).mean())},
+        'rel_l2_e_network_only': {'mean': float(rel_l2(pred[..., 0], yte[..., 0]).mean()),
+                                  'single_pass_mean': float(rel_l2(pred_single[..., 0], yte[..., 0]).mean())},
+        'spread_vs_error_corr': float(torch.corrcoef(torch.stack([spread, net_err]))[0, 1]),
         'rel_l2_e_without_network': {'mean': float(base.mean()), 'median': float(base.median())},
         'rel_l2_other_fields_mean': {f: float(rel_l2(pred[..., k], yte[..., k]).mean())
                                      for k, f in enumerate(FIELDS) if k > 0},

@@ -123,7 +123,8 @@ typedef struct clv_visc_buffers {
 #define CLV_OPT_CHUNK 2
 #define CLV_OPT_TILED_BLOCKS 3
 /* (y, eta) tile of the fused tiled stage: 0 = 8 x 32 (default), 1 = 16 x 16,
- * 2 = 8 x 16 (128-thread CTAs, four an SM in FP32) */
+ * 2 = 8 x 16 (128-thread CTAs, four an SM in FP32), 3 = 16 x 32 (one
+ * 512-thread CTA an SM; FP32 tolerance arithmetic only, else as 0) */
 #define CLV_OPT_TILE 4
 /* (2+1)D tiles: threads of a block (64, the default, or 128; a tile is that
  * many rows minus 4) and x planes per tile (default 8) */

@@ -71,11 +71,10 @@ def test_params_struct_size_matches_library():
 def test_arithmetic_flag():
     from clvisc_b200.ideal import fast_arithmetic
     cfg = read_config([])
-    assert cfg.arithmetic == 'auto' and fast_arithmetic(cfg)
+    assert cfg.arithmetic == 'fast' and fast_arithmetic(cfg)
     cfg.use_float32 = False
-    assert not fast_arithmetic(cfg)
-    cfg.arithmetic = 'fast'
+    assert fast_arithmetic(cfg)
+    cfg.arithmetic = 'auto'
     assert fast_arithmetic(cfg)
     cfg.arithmetic = 'exact'
-    cfg.use_float32 = True
     assert not fast_arithmetic(cfg)
