@@ -117,6 +117,10 @@ class CLIdeal(object):
         self.tau = self.cfg.real(self.cfg.TAU0)
 
         self.eos, self.eos_table, meta, self.efrz = load_eos(self.cfg, handcrafted_eos, self.device)
+        # effective chemical potentials on the freeze-out surface (ideal.py:65)
+        from .chempot import write_chemical_potential
+        self.chemical_potential = write_chemical_potential(self.eos.f_ed(self.cfg.TFRZ), self.cfg.fPathOut,
+                                                           eos_type=self.cfg.eos_type)
         self.params = self._make_params(meta)
         from .bulkinfo import BulkInfo
         self.bulkinfo = BulkInfo(self.cfg, self.lib, self.params, self.eos, self.device)

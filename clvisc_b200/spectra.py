@@ -73,7 +73,7 @@ class SmoothSpec(object):
     """Direct Cooper-Frye spectra on a freeze-out surface (Spec, cl_spec.h)."""
 
     def __init__(self, sf, tfrz, pisf=None, one_o_2TsqrEplusP=0.0, use_float32=True, device=None,
-                 ny=41, ylo=-8.0, yhi=8.0, npt=15, nphi=48):
+                 ny=41, ylo=-8.0, yhi=8.0, npt=15, nphi=48, mu=None):
         if not torch.cuda.is_available():
             raise RuntimeError('SmoothSpec needs a CUDA device; there is no CPU path')
         self.lib = _lib.load()
@@ -84,6 +84,9 @@ class SmoothSpec(object):
         self.pisf = None if pisf is None else torch.as_tensor(pisf).to(self.device, self.dtype).reshape(-1, 10)
         self.tfrz = float(tfrz)
         self.tcoeff = float(one_o_2TsqrEplusP)
+        # effective chemical potential of each hadron by PDG id (the
+        # chemical_potential.dat of the run; cl_spec.cpp:56-58, 183-200)
+        self.mu = dict(mu or {})
         self.y, self.pt, self.phi = momentum_grid(ny, ylo, yhi, npt, nphi)
         self.ylo, self.yhi = ylo, yhi
         as_dev = lambda a: torch.from_numpy(np.ascontiguousarray(a, dtype=self.real)).to(self.device)
@@ -93,17 +96,25 @@ class SmoothSpec(object):
 
     @classmethod
     def from_files(cls, path, viscous_on=False, **kw):
+        """hypersf.dat (and pimnsf.dat) of a run, with the effective chemical
+        potentials of its chemical_potential.dat (cl_spec.cpp:56-58)."""
+        from .chempot import read_chemical_potential
         sf, tfrz = read_hypersf(os.path.join(path, 'hypersf.dat'))
         pisf, coeff = (None, 0.0)
         if viscous_on:
             pisf, coeff = read_pimnsf(os.path.join(path, 'pimnsf.dat'))
+        kw.setdefault('mu', read_chemical_potential(path))
         return cls(sf, tfrz, pisf, coeff, **kw)
 
-    def calc(self, pid, mass=None, gspin=None, fermi_boson=None, mu=0.0):
+    def calc(self, pid, mass=None, gspin=None, fermi_boson=None, mu=None):
         """dN/(dY pt dpt dphi) of one species as (ny, npt, nphi); the hadron
-        is one of HADRONS by its PDG id, or given explicitly."""
+        is one of HADRONS by its PDG id, or given explicitly. mu defaults to
+        the hadron's effective chemical potential (0 without one), which the
+        kernel subtracts from u.p as kernel_spec.cl:28,52 does."""
         if mass is None:
             mass, gspin, fermi_boson = HADRONS[pid]
+        if mu is None:
+            mu = self.mu.get(int(pid), 0.0)
         ny, npt, nphi = len(self.y), len(self.pt), len(self.phi)
         out = torch.empty(ny * npt * nphi, dtype=self.dtype, device=self.device)
         n = self.sf.shape[0]

@@ -444,7 +444,7 @@ def predict_mirrored(sur, x):
     return mean, spread
 
 
-def calibrate_threshold(score, err, bad=0.02, keep_frac=0.01):
+def calibrate_threshold(score, err, bad=0.02, keep_frac=0.005):
     """The largest threshold on `score` for which, on calibration events,
     at most keep_frac of the events would be kept (score <= threshold) with an
     error above `bad`; events above the threshold go to the solver."""
@@ -569,7 +569,7 @@ def run_experiment(n_train=20000, n_test=1000, epochs=12, batch=32, n=128, steps
     # the fallback: an event goes to the solver when the energy-balance
     # residual of its prediction exceeds residual_max, or the spread of its
     # mirrored predictions exceeds a threshold calibrated on held-out training
-    # events (at most 1 % of them kept with an error above 2 %, the balance
+    # events (at most 0.5 % of them kept with an error above 2 %, the balance
     # test applied first)
     pcal, scal = predict_mirrored(sur, xcal)
     ecal = rel_l2(pcal[..., 0], ycal[..., 0])

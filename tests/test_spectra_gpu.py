@@ -81,3 +81,23 @@ def test_spectra_from_files_and_write(surface, tmp_path):
     vals = open(str(tmp_path / 'dNdYPtdPtdPhi_211.dat')).read().split()
     assert len(vals) == 41 * 15 * 48
     assert os.path.exists(str(tmp_path / 'dNdEtaPtdPtdPhi_211.dat'))
+
+
+@pytest.mark.parametrize('pid', [211, 2212])
+def test_spectra_with_chemical_potential(oracle_mod, surface, pid):
+    """The run wrote chemical_potential.dat at construction (ideal.py:65);
+    from_files reads it and calc() subtracts each hadron's mu from u.p
+    (kernel_spec.cl:28,52), against the oracle at the same nonzero mu."""
+    from clvisc_b200.spectra import HADRONS, SmoothSpec
+    use_float32, out, sf, pisf, cfg, pr, ed = surface
+    a = SmoothSpec.from_files(out, viscous_on=False, use_float32=use_float32)
+    mu = a.mu[pid]
+    assert mu > 0.03
+    b = SmoothSpec(sf, cfg.TFRZ, use_float32=use_float32)
+    got = b.calc(pid, mu=mu)
+    m, g, fb = HADRONS[pid]
+    want = oracle_mod.spectra(sf.cpu().numpy(), None, m, g, fb, mu, cfg.TFRZ, 0.0, b.y, b.pt, b.phi, use_float32)
+    _close(got, want, use_float32)
+    zero = b.calc(pid, mu=0.0)
+    ratio = got[20, 0, 0] / zero[20, 0, 0]
+    assert 1.2 < ratio < np.exp(mu / cfg.TFRZ) * 1.01, ratio

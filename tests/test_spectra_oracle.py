@@ -5,7 +5,8 @@ dSigma_mu = (tau A d eta, 0, 0, 0) at eta_s on a fine grid, has for
 Boltzmann statistics (fermi_boson = 0)
     dN/(dY pt dpt dphi) = g/(2 pi)^3 tau A * 2 mt K1(mt / T),
 independent of Y and phi; for Bose statistics the sum over n of
-K1(n mt / T) (Juttner series). The grid helpers reproduce Spec::InitGrid.
+K1(n mt / T) (Juttner series). A chemical potential mu multiplies the n-th
+term by exp(n mu / T) (kernel_spec.cl:52 subtracts mu from u.p). The grid helpers reproduce Spec::InitGrid.
 """
 import numpy as np
 import pytest
@@ -34,14 +35,15 @@ def test_momentum_grid_matches_reference_construction():
 
 @pytest.mark.parametrize('use_float32', [False, True])
 @pytest.mark.parametrize('fb', [0.0, -1.0])
-def test_static_bjorken_source(oracle_mod, use_float32, fb):
+@pytest.mark.parametrize('mu', [0.0, 0.0456])
+def test_static_bjorken_source(oracle_mod, use_float32, fb, mu):
     sf, ta = _bjorken_surface()
     y, pt, phi = momentum_grid(ny=5, ylo=-2.0, yhi=2.0, npt=15, nphi=8)
     T, m, g = 0.15, 0.13957, 1.0
-    spec = oracle_mod.spectra(sf, None, m, g, fb, 0.0, T, 0.0, y, pt, phi, use_float32)
+    spec = oracle_mod.spectra(sf, None, m, g, fb, mu, T, 0.0, y, pt, phi, use_float32)
     mt = np.sqrt(m * m + pt * pt)
     nmax = 1 if fb == 0.0 else 40
-    series = sum(k1(n * mt / T) for n in range(1, nmax + 1))
+    series = sum(np.exp(n * mu / T) * k1(n * mt / T) for n in range(1, nmax + 1))
     want = g / (2 * np.pi) ** 3 * ta * 2.0 * mt * series
     rtol = 2e-4 if use_float32 else 1e-7
     for k in range(5):
