@@ -51,6 +51,15 @@ int visc_stage(const clv::Params& p, const clv::ViscBuffers<real>& v, int step, 
   if (o.chunk < 1) return clv_host::set_error(CLV_ERR_INVALID, "fast visc stage: chunk must be >= 1");
   if (!bulk && (o.stage_kernel == 2 || (o.stage_kernel != 1 && p.nz >= kTiledMinNz))) {
     if (cpl) return launch_tiled<real, true, 1, 8, 32>(p, v, step, tc, o.chunk, s);
+    // 16 x 16 and 8 x 16 (y, eta) tiles as in the exact build (CLV_OPT_TILE 1, 2)
+    if (o.tile == 1) {
+      if (sizeof(real) == 8 || o.minb == 1) return launch_tiled<real, false, 1, 16, 16>(p, v, step, tc, o.chunk, s);
+      if constexpr (sizeof(real) == 4) return launch_tiled<real, false, 2, 16, 16>(p, v, step, tc, o.chunk, s);
+    }
+    if (o.tile == 2) {
+      if (sizeof(real) == 8 || o.minb == 1) return launch_tiled<real, false, 2, 8, 16>(p, v, step, tc, o.chunk, s);
+      if constexpr (sizeof(real) == 4) return launch_tiled<real, false, 4, 8, 16>(p, v, step, tc, o.chunk, s);
+    }
     if constexpr (sizeof(real) == 8) return launch_tiled<real, false, 1, 8, 32>(p, v, step, tc, o.chunk, s);
     else {
       // 16 x 32 (y, eta) tiles, one 512-thread CTA an SM: less halo than two 8 x 32 CTAs
