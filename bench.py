@@ -594,10 +594,10 @@ def main():
                     help='events of the batched workload reported under "batch" (0: skip)')
     ap.add_argument('--no-one-at-a-time', action='store_true', help='skip the one-event-at-a-time comparison')
     ap.add_argument('--batch-only', action='store_true', help='print only the batched workload line')
-    ap.add_argument('--surrogate-train', type=int, default=8000,
-                    help='training events of the learned-surrogate experiment reported under "surrogate" (0: skip); '
-                         'the full configuration is 20000 (--surrogate-only)')
-    ap.add_argument('--surrogate-test', type=int, default=500)
+    ap.add_argument('--surrogate-train', type=int, default=20000,
+                    help='training events of the learned-surrogate experiment reported under "surrogate" '
+                         '(the 20000 / 1000 configuration by default; 0: skip)')
+    ap.add_argument('--surrogate-test', type=int, default=1000)
     ap.add_argument('--surrogate-epochs', type=int, default=12)
     ap.add_argument('--surrogate-only', action='store_true', help='print only the surrogate experiment line')
     ap.add_argument('--fp64', action='store_true', help='the same workload in double precision')

@@ -52,6 +52,7 @@ class ClvParams(ctypes.Structure):
         ('zetaos_skew', ctypes.c_float), ('zetaos_tmin', ctypes.c_float),
         ('opt_stage_kernel', ctypes.c_int), ('opt_chunk', ctypes.c_int), ('opt_tiled_blocks', ctypes.c_int),
         ('opt_tile', ctypes.c_int),
+        ('eos_p2', ctypes.c_void_p),
     ]
 
 

@@ -71,6 +71,9 @@ int to_params(const clv_params* in, clv::Params* out) {
   p.eos_start = in->eos_ed_start; p.eos_step = in->eos_ed_step;
   p.eos_num = in->eos_num_ed; p.eos_nrow = in->eos_nrow; p.eos_ncol = in->eos_ncol;
   p.eos = in->eos_table;
+  p.eos_p2 = reinterpret_cast<const float2*>(in->eos_p2);
+  if (in->eos_p2 && (reinterpret_cast<uintptr_t>(in->eos_p2) % 8))
+    return fail(CLV_ERR_INVALID, "eos_p2 must be 8-byte aligned%s");
   p.flags = in->flags;
   p.ZETAOS_MAX = in->zetaos_max; p.ZETAOS_T0 = in->zetaos_t0;
   p.ZETAOS_WIDTH = in->zetaos_width; p.ZETAOS_SKEW = in->zetaos_skew; p.ZETAOS_TMIN = in->zetaos_tmin;

@@ -49,6 +49,7 @@ struct Params {
   float eos_start, eos_step;
   int eos_num, eos_nrow, eos_ncol;
   const float* eos;  // nrow*ncol texels of (cs2, p, T, s)
+  const float2* eos_p2;  // optional: pairs (p[t], p[t+1]) of the pressure column (tolerance build)
   int flags;
   // bulk sector (FLAG_BULK): zeta/s(T) peak, position, width, skewness
   float ZETAOS_MAX, ZETAOS_T0, ZETAOS_WIDTH, ZETAOS_SKEW;
@@ -190,6 +191,14 @@ template <class real> __device__ __forceinline__ real eos_lerp(real r, float lo,
 template <class real>
 __device__ CLV_EOS_ATTR real eos_comp(const Params& p, real eps, int c) {
   const EosSpot<real> s = eos_spot<real>(p, eps);
+#if CLV_FAST
+  // tolerance build: the pressure from one 8-byte read of the pair table
+  // when the two texels are neighbours (everywhere inside the table)
+  if (c == 1 && p.eos_p2 && s.t1 == s.t0 + 1) {
+    const float2 q = __ldg(p.eos_p2 + s.t0);
+    return eos_lerp<real>(s.r, q.x, q.y);
+  }
+#endif
   float lo = __ldg(p.eos + 4 * s.t0 + c);
   float hi = __ldg(p.eos + 4 * s.t1 + c);
   return eos_lerp<real>(s.r, lo, hi);

@@ -245,6 +245,8 @@ int noalloc_run(const clv_params* pp, int visc, double tau_old, double tau_new, 
   p.eos_start = pp->eos_ed_start; p.eos_step = pp->eos_ed_step;
   p.eos_num = pp->eos_num_ed; p.eos_nrow = pp->eos_nrow; p.eos_ncol = pp->eos_ncol;
   p.eos = pp->eos_table;
+  p.eos_p2 = nullptr;  // the surface kernels use the exact lookup
+  for (int q = 0; q < 4; q++) p.opt[q] = 0;
   p.flags = pp->flags;
   const clv::CubeGrid g = clv::cube_grid(p);
   const long long nc = (long long)g.nx * g.ny * g.nz;

@@ -48,6 +48,11 @@ def make_params(c, meta, eos_table, efrz, nx, ny, nz, ld):
     p.eos_num_ed = int(meta['num_of_ed'])
     p.eos_nrow, p.eos_ncol = int(meta['nrow']), int(meta['ncol'])
     p.eos_table = eos_table.data_ptr()
+    # pressure pairs (p[t], p[t+1]) for the tolerance build's one-read lookup,
+    # kept alive with the struct
+    pr = eos_table.view(-1, 4)[:, 1]
+    p._eos_p2 = torch.stack([pr, torch.cat([pr[1:], pr[-1:]])], dim=1).contiguous()
+    p.eos_p2 = p._eos_p2.data_ptr()
     flags = 0
     if getattr(c, 'riemann_test', False):
         flags |= _lib.CLV_FLAG_RIEMANN_TEST

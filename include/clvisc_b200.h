@@ -87,6 +87,11 @@ typedef struct clv_params {
    * x planes per tiled CTA, opt_tiled_blocks = 1 or 2, opt_tile = 1 +
    * CLV_OPT_TILE value. */
   int opt_stage_kernel, opt_chunk, opt_tiled_blocks, opt_tile;
+  /* Optional (nullable), read by the tolerance build (CLV_FLAG_FAST) only:
+   * device, 8-byte aligned, eos_nrow*eos_ncol pairs (p[t], p[t+1]) of the
+   * table's pressure column (the last pair repeats p[last]), so that a
+   * pressure lookup is one 8-byte read. */
+  const float *eos_p2;
 } clv_params;
 
 /* Buffers of one viscous Runge-Kutta stage. `step` is 1 or 2 as in
