@@ -74,7 +74,7 @@ def test_spectra_from_files_and_write(surface, tmp_path):
     from clvisc_b200.spectra import SmoothSpec
     use_float32, out, sf, pisf, cfg, pr, ed = surface
     a = SmoothSpec.from_files(out, viscous_on=True, use_float32=use_float32)
-    b = SmoothSpec(sf, a.tfrz, pisf, a.tcoeff, use_float32=use_float32)
+    b = SmoothSpec(sf, a.tfrz, pisf, a.tcoeff, use_float32=use_float32, mu=a.mu)
     sa, sb = a.calc(211), b.calc(211)
     np.testing.assert_allclose(sa, sb, rtol=1e-3, atol=1e-4 * np.abs(sb).max())
     a.write(str(tmp_path))
@@ -100,4 +100,6 @@ def test_spectra_with_chemical_potential(oracle_mod, surface, pid):
     _close(got, want, use_float32)
     zero = b.calc(pid, mu=0.0)
     ratio = got[20, 0, 0] / zero[20, 0, 0]
-    assert 1.2 < ratio < np.exp(mu / cfg.TFRZ) * 1.01, ratio
+    # at least the Boltzmann factor exp(mu/T) at the lowest p_T (Bose-Einstein
+    # enhances it further for pions)
+    assert ratio > 0.99 * np.exp(mu / cfg.TFRZ), ratio
