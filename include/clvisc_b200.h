@@ -217,9 +217,11 @@ int clv_hypersf_append(const clv_params *p, int visc, double tau_old, double tau
  * ((NY-1)/nyskip+1) * ((NZ-1)/nzskip+1); larger grids return
  * CLV_ERR_INVALID. It appends the same elements, in the same order, as
  * clv_hypersf_append. All calls share that array: calls whose launches overlap
- * on the GPU race, so serialise them. The first call on each device looks up
- * the array's device address (with that device current); make that first call
- * before any stream capture. Nothing is allocated or freed. */
+ * on the GPU race, so serialise them. A call made outside stream capture looks
+ * up the array's device address on the current device (so it stays right
+ * after a device reset); a call during capture reuses the address of the last
+ * call outside capture on that device, so make one call on each device before
+ * any stream capture. Nothing is allocated or freed. */
 int clv_hypersf_append_noalloc(const clv_params *p, int visc, double tau_old, double tau_new, const void *ev_old,
                                const void *ev_new, const void *pi_old, const void *pi_new, void *sf, void *txyz,
                                void *pisf, long long capacity, long long *total, void *stream);
