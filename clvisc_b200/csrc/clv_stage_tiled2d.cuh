@@ -108,6 +108,39 @@ __device__ __forceinline__ void rec2_face(const Params& p, real tau, int a, cons
                                           int ssl, const real* R_, int sr, const real* sR, int ssr,
                                           real F[Rec2<BULK>::NCOMP]) {
   typedef Rec2<BULK> R;
+#if CLV_FAST
+  // tolerance build, KT speed 1: the weighted form of the (3+1)D kernel's
+  // face_flux (cp = (v+1)/2 on the left state, cm = (v-1)/2 on the right)
+  {
+    const int va = R::VX + a;
+    const real vh = 0.5f * (L[va * sl] + R_[va * sr]);
+    const real cp = 0.5f * (vh + (real)1.0f), cm = 0.5f * (vh - (real)1.0f);
+    const real hp = 0.5f * cp, hm = 0.5f * cm;
+    const real pt = 0.5f * (L[R::PR * sl] + R_[R::PR * sr]) * tau;
+    const real th = 0.5f * tau;
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+      const int mi = a == 0 ? pidx(1, c) : pidx(2, c);
+      const real p0s = L[(R::PI + c) * sl] + R_[(R::PI + c) * sr];
+      const real pis = L[(R::PI + mi) * sl] + R_[(R::PI + mi) * sr];
+      real k = (c == 0 ? pt - th * p0s : -th * p0s) * vh + th * pis;
+      if (c == a + 1) k += pt;
+      real f = cm * R_[(R::Q0 + c) * sr] + k;
+      f = f - hm * sR[c * ssr];
+      f = f + cp * L[(R::Q0 + c) * sl];
+      F[c] = f + hp * sL[c * ssl];
+    }
+    const real cmR = cm * R_[R::U0 * sr], cpL = cp * L[R::U0 * sl];
+#pragma unroll
+    for (int m = 0; m < R::NPI; m++) {
+      real f = cmR * R_[(R::PI + m) * sr] - hm * sR[(4 + m) * ssr];
+      f = f + cpL * L[(R::PI + m) * sl];
+      F[4 + m] = f + hp * sL[(4 + m) * ssl];
+    }
+    (void)p;
+    return;
+  }
+#endif
   real h[4];
 #pragma unroll
   for (int c = 0; c < 4; c++) h[c] = 0.5f * (L[(R::E + c) * sl] + R_[(R::E + c) * sr]);
