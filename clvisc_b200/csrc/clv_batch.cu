@@ -94,17 +94,6 @@ int batch_stage_tiled_t(const clv_params* pp, int step, const clv_batch* b, int 
   return clv::batch_launch::stage_tiled<real>(p, a, step, rows, chunk, grid, s);
 }
 
-template <class real, bool BULK, int TB> int occupancy_tiled(int* n) {
-  typedef clv::Tile2Smem<real, BULK, TB> SM;
-  auto kern = clv::batch_tiled2d_kernel<real, BULK, TB, clv::tiled2d_minb<real, TB>()>;
-  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SM)) != cudaSuccess)
-    return clv_host::check_cuda("cudaFuncSetAttribute(batch_tiled2d_kernel)");
-  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(n, kern, TB, sizeof(SM));
-  if (e != cudaSuccess)
-    return clv_host::set_error(CLV_ERR_CUDA, std::string("batch_occupancy_tiled: ") + cudaGetErrorString(e));
-  return CLV_OK;
-}
-
 template <class real> int batch_advance_t(const clv_params* pp, const clv_batch* b, int first, cudaStream_t s) {
   clv::Params p;
   clv::BatchArgs<real> a;
@@ -144,12 +133,19 @@ int clv_batch_occupancy_tiled(const clv_params* p, int rows, int* blocks_per_sm)
   if (rows != 64 && rows != 128) return clv_host::set_error(CLV_ERR_INVALID, "batch_occupancy_tiled: rows must be 64 or 128");
   const bool bulk = p->flags & CLV_FLAG_BULK;
   int n = 0, rc;
-  if (p->precision == 4)
-    rc = rows == 64 ? (bulk ? occupancy_tiled<float, true, 64>(&n) : occupancy_tiled<float, false, 64>(&n))
-                    : (bulk ? occupancy_tiled<float, true, 128>(&n) : occupancy_tiled<float, false, 128>(&n));
+  if (p->flags & CLV_FLAG_FAST)
+    rc = p->precision == 4 ? clv_fastpath::batch_occupancy_tiled<float>(bulk, rows, &n)
+                           : clv_fastpath::batch_occupancy_tiled<double>(bulk, rows, &n);
+  else if (p->precision == 4)
+    rc = rows == 64 ? (bulk ? clv::batch_launch::occupancy_tiled<float, true, 64>(&n)
+                            : clv::batch_launch::occupancy_tiled<float, false, 64>(&n))
+                    : (bulk ? clv::batch_launch::occupancy_tiled<float, true, 128>(&n)
+                            : clv::batch_launch::occupancy_tiled<float, false, 128>(&n));
   else
-    rc = rows == 64 ? (bulk ? occupancy_tiled<double, true, 64>(&n) : occupancy_tiled<double, false, 64>(&n))
-                    : (bulk ? occupancy_tiled<double, true, 128>(&n) : occupancy_tiled<double, false, 128>(&n));
+    rc = rows == 64 ? (bulk ? clv::batch_launch::occupancy_tiled<double, true, 64>(&n)
+                            : clv::batch_launch::occupancy_tiled<double, false, 64>(&n))
+                    : (bulk ? clv::batch_launch::occupancy_tiled<double, true, 128>(&n)
+                            : clv::batch_launch::occupancy_tiled<double, false, 128>(&n));
   if (rc) return rc;
   *blocks_per_sm = n;
   return CLV_OK;
@@ -165,28 +161,17 @@ int clv_batch_occupancy(const clv_params* p, int block_size, int max_registers, 
     return clv_host::set_error(CLV_ERR_INVALID,
                                "batch_occupancy: max_registers must be 0 (or 128, or 168 below 256 threads, in FP32)");
   const bool bulk = p->flags & CLV_FLAG_BULK;
-  const bool cap = max_registers == 128, cap168 = max_registers == 168;
-  int n = 0;
-  cudaError_t e = cudaSuccess;
-  const void* f = nullptr;
-#define CLV_K(real, B, BS, M) f = reinterpret_cast<const void*>(clv::batch_stage_kernel<real, B, BS, M>)
-#define CLV_PICK(real, B)                                                  \
-  do {                                                                     \
-    if (block_size == 64) { if (cap168) CLV_K(real, B, 64, clv::batch_launch::capped168_minb<real>(64)); else if (cap) CLV_K(real, B, 64, clv::batch_launch::capped_minb<real>(64)); else CLV_K(real, B, 64, 1); }     \
-    else if (block_size == 128) { if (cap168) CLV_K(real, B, 128, clv::batch_launch::capped168_minb<real>(128)); else if (cap) CLV_K(real, B, 128, clv::batch_launch::capped_minb<real>(128)); else CLV_K(real, B, 128, 1); } \
-    else { if (cap) CLV_K(real, B, 256, clv::batch_launch::capped_minb<real>(256)); else CLV_K(real, B, 256, 1); } \
-  } while (0)
-  if (p->precision == 4) {
-    if (bulk) CLV_PICK(float, true);
-    else CLV_PICK(float, false);
-  } else {
-    if (bulk) CLV_PICK(double, true);
-    else CLV_PICK(double, false);
-  }
-#undef CLV_PICK
-#undef CLV_K
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, f, block_size, 0);
-  if (e != cudaSuccess) return clv_host::set_error(CLV_ERR_CUDA, std::string("batch_occupancy: ") + cudaGetErrorString(e));
+  int n = 0, rc;
+  if (p->flags & CLV_FLAG_FAST)
+    rc = p->precision == 4 ? clv_fastpath::batch_occupancy<float>(bulk, block_size, max_registers, &n)
+                           : clv_fastpath::batch_occupancy<double>(bulk, block_size, max_registers, &n);
+  else if (p->precision == 4)
+    rc = bulk ? clv::batch_launch::occupancy<float, true>(block_size, max_registers, &n)
+              : clv::batch_launch::occupancy<float, false>(block_size, max_registers, &n);
+  else
+    rc = bulk ? clv::batch_launch::occupancy<double, true>(block_size, max_registers, &n)
+              : clv::batch_launch::occupancy<double, false>(block_size, max_registers, &n);
+  if (rc) return rc;
   *blocks_per_sm = n;
   return CLV_OK;
 }

@@ -85,6 +85,34 @@ int launch_tiled(const Params& p, const BatchArgs<real>& a, int step, int chunk,
   return clv_host::check_cuda("batch_tiled2d_kernel");
 }
 
+// resident blocks per SM of the stage kernel of one launch shape (this also
+// loads the kernel and, for the tiled one, raises its shared-memory limit, so
+// that a later stream capture needs neither)
+template <class real, bool BULK>
+int occupancy(int bs, int cap, int* n) {
+  const void* f = nullptr;
+  if (bs == 64) f = cap == 168 ? (const void*)batch_stage_kernel<real, BULK, 64, capped168_minb<real>(64)>
+                 : cap ? (const void*)batch_stage_kernel<real, BULK, 64, capped_minb<real>(64)>
+                       : (const void*)batch_stage_kernel<real, BULK, 64, 1>;
+  else if (bs == 128) f = cap == 168 ? (const void*)batch_stage_kernel<real, BULK, 128, capped168_minb<real>(128)>
+                     : cap ? (const void*)batch_stage_kernel<real, BULK, 128, capped_minb<real>(128)>
+                           : (const void*)batch_stage_kernel<real, BULK, 128, 1>;
+  else f = cap ? (const void*)batch_stage_kernel<real, BULK, 256, capped_minb<real>(256)>
+               : (const void*)batch_stage_kernel<real, BULK, 256, 1>;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(n, f, bs, 0) != cudaSuccess)
+    return clv_host::check_cuda("batch_occupancy");
+  return 0;
+}
+template <class real, bool BULK, int TB> int occupancy_tiled(int* n) {
+  typedef Tile2Smem<real, BULK, TB> SM;
+  auto kern = batch_tiled2d_kernel<real, BULK, TB, tiled2d_minb<real, TB>()>;
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SM)) != cudaSuccess)
+    return clv_host::check_cuda("cudaFuncSetAttribute(batch_tiled2d_kernel)");
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(n, kern, TB, sizeof(SM)) != cudaSuccess)
+    return clv_host::check_cuda("batch_occupancy_tiled");
+  return 0;
+}
+
 template <class real>
 int stage_tiled(const Params& p, const BatchArgs<real>& a, int step, int rows, int chunk, int grid, cudaStream_t s) {
   const bool bulk = p.flags & FLAG_BULK;

@@ -95,6 +95,22 @@ int batch_stage_tiled(const clv::Params& p, const clv::BatchArgs<real>& a, int s
   return clv::batch_launch::stage_tiled<real>(p, a, step, rows, chunk, grid, s);
 }
 
+template <class real> int batch_occupancy(bool bulk, int bs, int cap, int* n) {
+  return bulk ? clv::batch_launch::occupancy<real, true>(bs, cap, n)
+              : clv::batch_launch::occupancy<real, false>(bs, cap, n);
+}
+template <class real> int batch_occupancy_tiled(bool bulk, int rows, int* n) {
+  if (rows == 64)
+    return bulk ? clv::batch_launch::occupancy_tiled<real, true, 64>(n)
+                : clv::batch_launch::occupancy_tiled<real, false, 64>(n);
+  return bulk ? clv::batch_launch::occupancy_tiled<real, true, 128>(n)
+              : clv::batch_launch::occupancy_tiled<real, false, 128>(n);
+}
+template int batch_occupancy<float>(bool, int, int, int*);
+template int batch_occupancy<double>(bool, int, int, int*);
+template int batch_occupancy_tiled<float>(bool, int, int*);
+template int batch_occupancy_tiled<double>(bool, int, int*);
+
 template int batch_stage<float>(const clv::Params&, const clv::BatchArgs<float>&, int, int, int, int, cudaStream_t);
 template int batch_stage<double>(const clv::Params&, const clv::BatchArgs<double>&, int, int, int, int, cudaStream_t);
 template int batch_stage_tiled<float>(const clv::Params&, const clv::BatchArgs<float>&, int, int, int, int,

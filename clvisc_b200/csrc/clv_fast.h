@@ -25,4 +25,7 @@ int batch_stage(const clv::Params& p, const clv::BatchArgs<real>& a, int step, i
 template <class real>
 int batch_stage_tiled(const clv::Params& p, const clv::BatchArgs<real>& a, int step, int rows, int chunk, int grid,
                       cudaStream_t s);
+// resident blocks per SM of the fast batched stage kernels (loads them)
+template <class real> int batch_occupancy(bool bulk, int bs, int cap, int* n);
+template <class real> int batch_occupancy_tiled(bool bulk, int rows, int* n);
 }  // namespace clv_fastpath

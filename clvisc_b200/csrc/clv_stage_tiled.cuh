@@ -142,9 +142,8 @@ __device__ CLV_TILED_ATTR void face_flux(const Params& p, real tau, int a, const
       }
     }
     (void)p;
-    return;
   }
-#endif
+#else
   real h[4];
 #pragma unroll
   for (int c = 0; c < 4; c++) h[c] = 0.5f * (L[(RF_E + c) * sl] + R[(RF_E + c) * sr]);
@@ -178,6 +177,7 @@ __device__ CLV_TILED_ATTR void face_flux(const Params& p, real tau, int a, const
       F[4 + m] = 0.5f * (Jp + Jm) - 0.5f * lam * (AR - AL);
     }
   }
+#endif
 }
 
 template <class real, bool DO_IS, bool DO_KT, bool COUPLED, int TJ, int TK, int MINB>

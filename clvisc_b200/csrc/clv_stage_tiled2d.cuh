@@ -138,9 +138,8 @@ __device__ __forceinline__ void rec2_face(const Params& p, real tau, int a, cons
       F[4 + m] = f + hp * sL[(4 + m) * ssl];
     }
     (void)p;
-    return;
   }
-#endif
+#else
   real h[4];
 #pragma unroll
   for (int c = 0; c < 4; c++) h[c] = 0.5f * (L[(R::E + c) * sl] + R_[(R::E + c) * sr]);
@@ -170,6 +169,7 @@ __device__ __forceinline__ void rec2_face(const Params& p, real tau, int a, cons
     real Jm = AL * vh;
     F[4 + m] = 0.5f * (Jp + Jm) - 0.5f * lam * (AR - AL);
   }
+#endif
 }
 
 // One tile: rows j0 .. j0+TB-5 of planes i0 .. i1-1 of the event (gd, b).
