@@ -522,7 +522,8 @@ def run_gpu(args, rank, world, dist):
                               'config': {'grid': [nx, ny, nz]}, 'gpu_launches': 2 * args.steps}), flush=True)
         return
     # end to end through the public API with host buffers
-    host_ic = torch.from_numpy(np.ascontiguousarray(ic)).pin_memory()
+    host_ic = torch.from_numpy(np.ascontiguousarray(ic, dtype=cfg.real)).pin_memory()
+    host_out = torch.empty((cells, 4), dtype=v.dtype, pin_memory=True)  # the result's pinned destination
     v2 = CLVisc(cfg, gpu_id=dev)
     torch.cuda.synchronize()
     barrier()
@@ -531,7 +532,7 @@ def run_gpu(args, rank, world, dist):
     f0.record(stream)
     v2.load_ini(host_ic)
     v2.evolve(max_loops=args.steps, force_run_to_maxloop=True, save_hypersf=False, save_pi=False)
-    out = v2.ideal.ev_to_host()
+    out = v2.ideal.ev_to_host(out=host_out)
     f1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = max_over_ranks(f0.elapsed_time(f1), dist)

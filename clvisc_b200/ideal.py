@@ -210,16 +210,25 @@ class CLIdeal(object):
         dev_aos = dev_aos.to(self.device, self.dtype).contiguous()
         self._call('clv_aos_to_soa', _lib.ptr(dev_aos), _lib.ptr(self.d_ev[1]), self.size, 4, self.stream)
 
-    def ev_to_host(self):
-        """d_ev[1] -> h_ev1 as (cells, 4) (ideal.py:265-267)."""
-        self.h_ev1 = self.field_to_host(self.d_ev[1])
+    def ev_to_host(self, out=None):
+        """d_ev[1] -> h_ev1 as (cells, 4) (ideal.py:265-267). `out`: an
+        optional pinned host tensor of that shape and the run's dtype, filled
+        by one direct copy (no pageable staging)."""
+        self.h_ev1 = self.field_to_host(self.d_ev[1], out=out)
         return self.h_ev1
 
-    def field_to_host(self, t, w=None):
-        """Any SoA field -> numpy (cells, w)."""
+    def field_to_host(self, t, w=None, out=None):
+        """Any SoA field -> numpy (cells, w); into the pinned host tensor
+        `out` when one is given."""
         w = t.shape[0] if w is None else w
         aos = torch.empty((self.size, w), dtype=self.dtype, device=self.device)
         self._call('clv_soa_to_aos', _lib.ptr(t), _lib.ptr(aos), self.size, w, self.stream)
+        if out is not None:
+            if tuple(out.shape) != (self.size, w) or out.dtype != self.dtype or not out.is_pinned():
+                raise ValueError('out must be a pinned (%d, %d) %s tensor' % (self.size, w, self.dtype))
+            out.copy_(aos, non_blocking=True)
+            torch.cuda.current_stream(self.device).synchronize()
+            return out.numpy()
         return aos.cpu().numpy()
 
     def field_from_host(self, t, arr):
