@@ -251,6 +251,7 @@ class OracleIdeal(object):
         else:
             self.table, meta = self.eos.create_table()
         self.efrz = self.eos.f_ed(cfg.TFRZ)
+        self.meta = meta
         self.consts = make_consts(cfg, meta, self.table, self.efrz)
         self.k = Kernels(self.consts, real)
         self.size = cfg.NX * cfg.NY * cfg.NZ
