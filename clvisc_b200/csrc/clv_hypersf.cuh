@@ -71,15 +71,18 @@ template <class real> __device__ R4<real> mass_center(const R4<real>* ints, int 
   return div4(c, (real)n);
 }
 
-// :135-159
+// :135-159. The reference builds the piece (i, j, k, l) inside the m loop;
+// it depends only on the intersections and their centre, which change only
+// at a hit, after which the m loop ends, so it is built once per (i, j, k, l)
+// here: the same values, n - l - 1 times fewer constructions.
 template <class real> __device__ void tiny_move_if_coplanar(R4<real>* ints, int n, R4<real>* mc, int gid) {
   int seed = (int)(32117u * (unsigned int)(gid + 1));
   for (int i = 0; i < n - 4; i++)
     for (int j = i + 1; j < n - 3; j++)
       for (int k = j + 1; k < n - 2; k++)
-        for (int l = k + 1; l < n - 1; l++)
+        for (int l = k + 1; l < n - 1; l++) {
+          const SurfPiece<real> sf = construct_hypersf(i, j, k, l, ints, *mc);
           for (int m = l + 1; m < n; m++) {
-            SurfPiece<real> sf = construct_hypersf(i, j, k, l, ints, *mc);
             if (dotr4(sf.norm, sub4(ints[m], sf.center)) == 0.0f) {
               for (int q = 0; q < n; q++) {
                 real r0 = sf_rand<real>(&seed), r1 = sf_rand<real>(&seed), r2 = sf_rand<real>(&seed),
@@ -91,6 +94,7 @@ template <class real> __device__ void tiny_move_if_coplanar(R4<real>* ints, int 
               break;
             }
           }
+        }
 }
 
 template <class real> __device__ bool on_convex_hull(const SurfPiece<real>& sf, const R4<real>* ints, int n) {  // :163-176
@@ -146,7 +150,9 @@ template <class real> __device__ R4<real> calc_area(R4<real>* ints, R4<real> flo
         for (int k = j + 1; k < n - 1; k++)
           for (int l = k + 1; l < n; l++) {
             SurfPiece<real> sf = construct_hypersf(i, j, k, l, ints, mc);
-            if (on_convex_hull(sf, ints, n) && dotr4(sf.norm, flow) > 0.0f) area = add4(area, sf.norm);
+            // both tests are pure: the cheap one first (the reference
+            // evaluates the hull test first; the sum is the same)
+            if (dotr4(sf.norm, flow) > 0.0f && on_convex_hull(sf, ints, n)) area = add4(area, sf.norm);
           }
   }
   return div4(area, (real)6.0f);

@@ -8,6 +8,10 @@
 //   * Per cell, a record (ev, P(e), u0, Q = tau*(T0m + pi^{tau mu}), pi) is
 //     computed once, into shared memory: the centre plane with a 2-cell halo
 //     in j and k, and the two planes ahead (i+1, i+2) for the x stencil.
+//     A record's 20 values are five groups of four, each group of a plane
+//     stored cell by cell, so a group moves in one 16-byte (FP32) or two
+//     16-byte (FP64) shared-memory accesses; slopes and face fluxes (14
+//     components) likewise as three groups of four and one pair.
 //   * The limited slope of every cell is computed once per direction, and the
 //     flux through every face once; a cell's flux difference subtracts the
 //     flux of its minus face from that of its plus face, exactly the two
@@ -30,10 +34,12 @@ namespace clv {
 #define CLV_TILED_ATTR __noinline__
 #endif
 
-// record fields (planes of the shared-memory region)
+// record fields: groups of four, field f in group f / 4, lane f % 4
 enum { RF_E = 0, RF_VX, RF_VY, RF_VZ, RF_PR, RF_U0, RF_Q0, RF_Q1, RF_Q2, RF_Q3, RF_PI, RF_N = RF_PI + 10 };
-// slope / face-flux components: 0..3 KT (Q), 4..13 IS (u0*pi)
-enum { NCOMP = 14 };
+enum { RG = RF_N / 4 };  // record groups
+// slope / face-flux components: 0..3 KT (Q), 4..13 IS (u0*pi); groups 0..2 of
+// four and the pair 12, 13
+enum { NCOMP = 14, SG4 = 3 };
 
 template <int TJ, int TK> struct TileGeom {
   static constexpr int CY = TJ + 4, CZ = TK + 4;     // centre region with halo
@@ -46,19 +52,78 @@ template <int TJ, int TK> struct TileGeom {
 
 template <class real, int TJ, int TK> struct TileSmem {
   typedef TileGeom<TJ, TK> G;
-  real C[RF_N][G::NC];        // centre plane i
-  real A[RF_N][G::NI];        // plane i+1 (interior)
-  real B[RF_N][G::NI];        // plane i+2 (interior)
-  real SY[NCOMP][G::NSY];     // y slopes, then y face fluxes
-  real SZ[NCOMP][G::NSZ];     // z slopes, then z face fluxes
+  __align__(16) real C[RG][G::NC][4];     // centre plane i
+  __align__(16) real A[RG][G::NI][4];     // plane i+1 (interior)
+  __align__(16) real B[RG][G::NI][4];     // plane i+2 (interior)
+  __align__(16) real SY4[SG4][G::NSY][4];  // y slopes, then y face fluxes: components 0..11
+  __align__(16) real SY2[G::NSY][2];       //   components 12, 13
+  __align__(16) real SZ4[SG4][G::NSZ][4];  // z slopes, then z face fluxes
+  __align__(16) real SZ2[G::NSZ][2];
 };
+
+// 16-byte shared-memory moves of four or two reals (two 16-byte moves for
+// four doubles)
+template <class real> __device__ __forceinline__ void lds4(const real* p, real* o) {
+  if constexpr (sizeof(real) == 4) {
+    const float4 t = *reinterpret_cast<const float4*>(p);
+    o[0] = t.x; o[1] = t.y; o[2] = t.z; o[3] = t.w;
+  } else {
+    const double2 a = reinterpret_cast<const double2*>(p)[0], b = reinterpret_cast<const double2*>(p)[1];
+    o[0] = a.x; o[1] = a.y; o[2] = b.x; o[3] = b.y;
+  }
+}
+template <class real> __device__ __forceinline__ void sts4(real* p, const real* v) {
+  if constexpr (sizeof(real) == 4) {
+    *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+  } else {
+    reinterpret_cast<double2*>(p)[0] = make_double2(v[0], v[1]);
+    reinterpret_cast<double2*>(p)[1] = make_double2(v[2], v[3]);
+  }
+}
+template <class real> __device__ __forceinline__ void lds2(const real* p, real* o) {
+  if constexpr (sizeof(real) == 4) {
+    const float2 t = *reinterpret_cast<const float2*>(p);
+    o[0] = t.x; o[1] = t.y;
+  } else {
+    const double2 t = *reinterpret_cast<const double2*>(p);
+    o[0] = t.x; o[1] = t.y;
+  }
+}
+template <class real> __device__ __forceinline__ void sts2(real* p, const real* v) {
+  if constexpr (sizeof(real) == 4) *reinterpret_cast<float2*>(p) = make_float2(v[0], v[1]);
+  else *reinterpret_cast<double2*>(p) = make_double2(v[0], v[1]);
+}
+
+// a record of cell c of a plane of n cells (plane = &X[0][0][0]); groups
+// whose values go unused are dropped by the compiler
+template <class real> __device__ __forceinline__ void rec_load(const real* plane, int n, int c, real r[RF_N]) {
+#pragma unroll
+  for (int g = 0; g < RG; g++) lds4<real>(plane + ((size_t)g * n + c) * 4, r + 4 * g);
+}
+template <class real> __device__ __forceinline__ void rec_store(real* plane, int n, int c, const real r[RF_N]) {
+#pragma unroll
+  for (int g = 0; g < RG; g++) sts4<real>(plane + ((size_t)g * n + c) * 4, r + 4 * g);
+}
+// the 14 slope (or face) components of slot c of an array of n slots
+template <class real>
+__device__ __forceinline__ void cmp_load(const real* s4, const real* s2, int n, int c, real v[NCOMP]) {
+#pragma unroll
+  for (int g = 0; g < SG4; g++) lds4<real>(s4 + ((size_t)g * n + c) * 4, v + 4 * g);
+  lds2<real>(s2 + (size_t)c * 2, v + 12);
+}
+template <class real>
+__device__ __forceinline__ void cmp_store(real* s4, real* s2, int n, int c, const real v[NCOMP]) {
+#pragma unroll
+  for (int g = 0; g < SG4; g++) sts4<real>(s4 + ((size_t)g * n + c) * 4, v + 4 * g);
+  sts2<real>(s2 + (size_t)c * 2, v + 12);
+}
 
 inline namespace CLV_ARITH {
 
-// record of one (clamped) cell of the stage input
+// record of one (clamped) cell of the stage input, into r
 template <class real>
 __device__ CLV_TILED_ATTR void make_record(const Params& p, const ViscBuffers<real>& b, real tau, int i, int j, int k,
-                                            real* dst, int stride) {
+                                            real r[RF_N]) {
   i = min(max(i, 0), p.nx - 1);
   j = min(max(j, 0), p.ny - 1);
   k = min(max(k, 0), p.nz - 1);
@@ -72,40 +137,76 @@ __device__ CLV_TILED_ATTR void make_record(const Params& p, const ViscBuffers<re
   real u0 = gamma3<real>(vx, vy, vz);
   real A = (e + pr) * u0;
   real u4[4] = {(real)1.0f * u0, vx * u0, vy * u0, vz * u0};
-  dst[RF_E * stride] = e;
-  dst[RF_VX * stride] = vx;
-  dst[RF_VY * stride] = vy;
-  dst[RF_VZ * stride] = vz;
-  dst[RF_PR * stride] = pr;
-  dst[RF_U0 * stride] = u0;
+  r[RF_E] = e;
+  r[RF_VX] = vx;
+  r[RF_VY] = vy;
+  r[RF_VZ] = vz;
+  r[RF_PR] = pr;
+  r[RF_U0] = u0;
 #pragma unroll
   for (int c = 0; c < 4; c++) {
     real g0 = c == 0 ? (real)1.0f : (real)0.0f;
     real T0m = A * u4[c] - g0 * pr;
-    dst[(RF_Q0 + c) * stride] = tau * (T0m + pi[c]);
+    r[RF_Q0 + c] = tau * (T0m + pi[c]);
   }
 #pragma unroll
-  for (int m = 0; m < 10; m++) dst[(RF_PI + m) * stride] = pi[m];
+  for (int m = 0; m < 10; m++) r[RF_PI + m] = pi[m];
+}
+template <class real>
+__device__ CLV_TILED_ATTR void store_record(const Params& p, const ViscBuffers<real>& b, real tau, int i, int j, int k,
+                                             real* plane, int n, int c) {
+  real r[RF_N];
+  make_record<real>(p, b, tau, i, j, k, r);
+  rec_store<real>(plane, n, c, r);
+}
+
+// records of the centre plane's halo: two rows above and below the tile
+// (interior columns) and two columns left and right (interior rows). The
+// corners of the (TJ+4) x (TK+4) region are never read (the y stencil stays
+// in the interior columns, the z stencil in the interior rows) and are not
+// computed.
+template <class real, int TJ, int TK>
+__device__ CLV_TILED_ATTR void halo_records(const Params& p, const ViscBuffers<real>& b, real tau, int i, int j0,
+                                             int k0, int tid, real* C) {
+  typedef TileGeom<TJ, TK> G;
+  constexpr int NHY = 4 * TK, NHZ = 4 * TJ;
+  for (int q = tid; q < NHY + NHZ; q += TJ * TK) {
+    int r, c;
+    if (q < NHY) {  // rows 0, 1, TJ+2, TJ+3; consecutive q along k
+      const int rr = q / TK;
+      r = rr < 2 ? rr : TJ + rr;
+      c = 2 + q % TK;
+    } else {  // columns 0, 1, TK+2, TK+3
+      const int qq = q - NHY, cc = qq / TJ;
+      c = cc < 2 ? cc : TK + cc;
+      r = 2 + qq % TJ;
+    }
+    store_record<real>(p, b, tau, i, j0 - 2 + r, k0 - 2 + c, C, G::NC, r * G::CZ + c);
+  }
 }
 
 // limited slopes of the 14 components at the middle of three records
 template <class real>
-__device__ CLV_TILED_ATTR void slopes3(const real* L, int sl, const real* M, int sm, const real* R, int sr,
-                                        real* out, int so) {
+__device__ CLV_TILED_ATTR void slopes3(const real L[RF_N], const real M[RF_N], const real R[RF_N], real out[NCOMP]) {
 #pragma unroll
-  for (int c = 0; c < 4; c++)
-    out[c * so] = slope<real>(L[(RF_Q0 + c) * sl], M[(RF_Q0 + c) * sm], R[(RF_Q0 + c) * sr]);
-  real uL = L[RF_U0 * sl], uM = M[RF_U0 * sm], uR = R[RF_U0 * sr];
+  for (int c = 0; c < 4; c++) out[c] = slope<real>(L[RF_Q0 + c], M[RF_Q0 + c], R[RF_Q0 + c]);
+  real uL = L[RF_U0], uM = M[RF_U0], uR = R[RF_U0];
 #pragma unroll
-  for (int m = 0; m < 10; m++)
-    out[(4 + m) * so] = slope<real>(uL * L[(RF_PI + m) * sl], uM * M[(RF_PI + m) * sm], uR * R[(RF_PI + m) * sr]);
+  for (int m = 0; m < 10; m++) out[4 + m] = slope<real>(uL * L[RF_PI + m], uM * M[RF_PI + m], uR * R[RF_PI + m]);
 }
 
 // flux through the face between records L and R along axis a, given their
 // slopes (kt1d_visc face part and kt1d_real face part)
 template <class real, bool DO_IS, bool DO_KT>
-__device__ CLV_TILED_ATTR void face_flux(const Params& p, real tau, int a, const real* L, int sl, const real* sL,
-                                          int ssl, const real* R, int sr, const real* sR, int ssr, real F[NCOMP]) {
+__device__ CLV_TILED_ATTR void face_flux(const Params& p, real tau, int a, const real L[RF_N], const real sL[NCOMP],
+                                          const real R[RF_N], const real sR[NCOMP], real F[NCOMP]) {
+  // components of a part this variant does not run: zero, stored and never used
+  if (!DO_KT)
+#pragma unroll
+    for (int c = 0; c < 4; c++) F[c] = 0.0f;
+  if (!DO_IS)
+#pragma unroll
+    for (int m = 0; m < 10; m++) F[4 + m] = 0.0f;
 #if CLV_FAST
   // tolerance build, with the KT speed 1: F = 0.5 (J(A_R) + J(A_L)) -
   // 0.5 (A_R - A_L) is, for J linear in A with slope v, the weighted sum
@@ -113,32 +214,32 @@ __device__ CLV_TILED_ATTR void face_flux(const Params& p, real tau, int a, const
   // A_L = Q_L + s_L/2, A_R = Q_R - s_R/2 expanded into fused multiply-adds
   {
     const int va = RF_VX + a;
-    const real vh = 0.5f * (L[va * sl] + R[va * sr]);
+    const real vh = 0.5f * (L[va] + R[va]);
     const real cp = 0.5f * (vh + (real)1.0f), cm = 0.5f * (vh - (real)1.0f);
     const real hp = 0.5f * cp, hm = 0.5f * cm;
     if (DO_KT) {
-      const real pt = 0.5f * (L[RF_PR * sl] + R[RF_PR * sr]) * tau;
+      const real pt = 0.5f * (L[RF_PR] + R[RF_PR]) * tau;
       const real th = 0.5f * tau;
 #pragma unroll
       for (int c = 0; c < 4; c++) {
         const int mi = a == 0 ? pidx(1, c) : (a == 1 ? pidx(2, c) : pidx(3, c));
-        const real p0s = L[(RF_PI + c) * sl] + R[(RF_PI + c) * sr];
-        const real pis = L[(RF_PI + mi) * sl] + R[(RF_PI + mi) * sr];
+        const real p0s = L[RF_PI + c] + R[RF_PI + c];
+        const real pis = L[RF_PI + mi] + R[RF_PI + mi];
         real k = (c == 0 ? pt - th * p0s : -th * p0s) * vh + th * pis;
         if (c == a + 1) k += pt;
-        real f = cm * R[(RF_Q0 + c) * sr] + k;
-        f = f - hm * sR[c * ssr];
-        f = f + cp * L[(RF_Q0 + c) * sl];
-        F[c] = f + hp * sL[c * ssl];
+        real f = cm * R[RF_Q0 + c] + k;
+        f = f - hm * sR[c];
+        f = f + cp * L[RF_Q0 + c];
+        F[c] = f + hp * sL[c];
       }
     }
     if (DO_IS) {
-      const real cmR = cm * R[RF_U0 * sr], cpL = cp * L[RF_U0 * sl];
+      const real cmR = cm * R[RF_U0], cpL = cp * L[RF_U0];
 #pragma unroll
       for (int m = 0; m < 10; m++) {
-        real f = cmR * R[(RF_PI + m) * sr] - hm * sR[(4 + m) * ssr];
-        f = f + cpL * L[(RF_PI + m) * sl];
-        F[4 + m] = f + hp * sL[(4 + m) * ssl];
+        real f = cmR * R[RF_PI + m] - hm * sR[4 + m];
+        f = f + cpL * L[RF_PI + m];
+        F[4 + m] = f + hp * sL[4 + m];
       }
     }
     (void)p;
@@ -146,19 +247,19 @@ __device__ CLV_TILED_ATTR void face_flux(const Params& p, real tau, int a, const
 #else
   real h[4];
 #pragma unroll
-  for (int c = 0; c < 4; c++) h[c] = 0.5f * (L[(RF_E + c) * sl] + R[(RF_E + c) * sr]);
+  for (int c = 0; c < 4; c++) h[c] = 0.5f * (L[RF_E + c] + R[RF_E + c]);
   const real vh = a == 0 ? h[1] : (a == 1 ? h[2] : h[3]);
   const real lam = max_speed<real>(p, h[0], h[1], h[2], h[3], vh);
   if (DO_KT) {
-    real pr_half = 0.5f * (L[RF_PR * sl] + R[RF_PR * sr]);
+    real pr_half = 0.5f * (L[RF_PR] + R[RF_PR]);
     real pt = pr_half * tau;
 #pragma unroll
     for (int c = 0; c < 4; c++) {
-      real AL = L[(RF_Q0 + c) * sl] + 0.5f * sL[c * ssl];
-      real AR = R[(RF_Q0 + c) * sr] - 0.5f * sR[c * ssr];
+      real AL = L[RF_Q0 + c] + 0.5f * sL[c];
+      real AR = R[RF_Q0 + c] - 0.5f * sR[c];
       const int mi = a == 0 ? pidx(1, c) : (a == 1 ? pidx(2, c) : pidx(3, c));
-      real pim0_half = 0.5f * (L[(RF_PI + c) * sl] + R[(RF_PI + c) * sr]);
-      real pimi_half = 0.5f * (L[(RF_PI + mi) * sl] + R[(RF_PI + mi) * sr]);
+      real pim0_half = 0.5f * (L[RF_PI + c] + R[RF_PI + c]);
+      real pimi_half = 0.5f * (L[RF_PI + mi] + R[RF_PI + mi]);
       real g0 = c == 0 ? (real)1.0f : (real)0.0f;
       real ga = c == a + 1 ? (real)-1.0f : (real)0.0f;
       real Jp = (AR + pt * g0 - tau * pim0_half) * vh - pt * ga + tau * pimi_half;
@@ -167,17 +268,26 @@ __device__ CLV_TILED_ATTR void face_flux(const Params& p, real tau, int a, const
     }
   }
   if (DO_IS) {
-    real uL = L[RF_U0 * sl], uR = R[RF_U0 * sr];
+    real uL = L[RF_U0], uR = R[RF_U0];
 #pragma unroll
     for (int m = 0; m < 10; m++) {
-      real AL = uL * L[(RF_PI + m) * sl] + 0.5f * sL[(4 + m) * ssl];
-      real AR = uR * R[(RF_PI + m) * sr] - 0.5f * sR[(4 + m) * ssr];
+      real AL = uL * L[RF_PI + m] + 0.5f * sL[4 + m];
+      real AR = uR * R[RF_PI + m] - 0.5f * sR[4 + m];
       real Jp = AR * vh;
       real Jm = AL * vh;
       F[4 + m] = 0.5f * (Jp + Jm) - 0.5f * lam * (AR - AL);
     }
   }
 #endif
+}
+
+// u^mu of a record
+template <class real> __device__ __forceinline__ void umu_of(const real r[RF_N], real u[4]) {
+  const real u0 = r[RF_U0];
+  u[0] = u0 * 1.0f;
+  u[1] = u0 * r[RF_VX];
+  u[2] = u0 * r[RF_VY];
+  u[3] = u0 * r[RF_VZ];
 }
 
 template <class real, bool DO_IS, bool DO_KT, bool COUPLED, int TJ, int TK, int MINB>
@@ -189,8 +299,13 @@ __global__ void __launch_bounds__(TJ * TK, MINB)
   typedef TileSmem<real, TJ, TK> SM;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   SM& s = *reinterpret_cast<SM*>(smem_raw);
-  real(*A)[G::NI] = s.A;
-  real(*B)[G::NI] = s.B;
+  real* const C = &s.C[0][0][0];
+  real* A = &s.A[0][0][0];
+  real* B = &s.B[0][0][0];
+  real* const SY4 = &s.SY4[0][0][0];
+  real* const SY2 = &s.SY2[0][0];
+  real* const SZ4 = &s.SZ4[0][0][0];
+  real* const SZ2 = &s.SZ2[0][0];
 
   const int tid = threadIdx.x;
   const int tj = tid / TK, tk = tid % TK;
@@ -204,47 +319,58 @@ __global__ void __launch_bounds__(TJ * TK, MINB)
   const real acu = Acu<real>::v;
 
   // ------------------------------------------------------------ prologue
-  // x window: records of planes i0-2 (A), i0-1 (B), i0 (own cell of C)
-  make_record<real>(p, b, tau, i0 - 2, jj, kk, &A[0][tid], G::NI);
-  make_record<real>(p, b, tau, i0 - 1, jj, kk, &B[0][tid], G::NI);
-  make_record<real>(p, b, tau, i0, jj, kk, &s.C[0][cself], G::NC);
-  real s_prev[NCOMP], s_cur[NCOMP], F_prev[NCOMP], s_next[NCOMP], umu_prev[4];
-  slopes3<real>(&A[0][tid], G::NI, &B[0][tid], G::NI, &s.C[0][cself], G::NC, s_prev, 1);  // slope at i0-1
-  make_record<real>(p, b, tau, i0 + 1, jj, kk, &A[0][tid], G::NI);
-  slopes3<real>(&B[0][tid], G::NI, &s.C[0][cself], G::NC, &A[0][tid], G::NI, s_cur, 1);   // slope at i0
-  face_flux<real, DO_IS, DO_KT>(p, tau, 0, &B[0][tid], G::NI, s_prev, 1, &s.C[0][cself], G::NC, s_cur, 1, F_prev);
+  // x window: records of planes i0-2 and i0-1 (registers only), i0 (own cell
+  // of C), i0+1 (A), i0+2 (B)
+  real s_cur[NCOMP], F_prev[NCOMP], s_next[NCOMP], umu_prev[4];
   {
-    real u0 = B[RF_U0][tid];
-    umu_prev[0] = u0 * 1.0f;
-    umu_prev[1] = u0 * B[RF_VX][tid];
-    umu_prev[2] = u0 * B[RF_VY][tid];
-    umu_prev[3] = u0 * B[RF_VZ][tid];
+    real r0[RF_N], r1[RF_N], r2[RF_N], s_prev[NCOMP];
+    make_record<real>(p, b, tau, i0 - 2, jj, kk, r0);
+    make_record<real>(p, b, tau, i0 - 1, jj, kk, r1);
+    make_record<real>(p, b, tau, i0, jj, kk, r2);
+    rec_store<real>(C, G::NC, cself, r2);
+    slopes3<real>(r0, r1, r2, s_prev);  // slope at i0-1
+    make_record<real>(p, b, tau, i0 + 1, jj, kk, r0);
+    rec_store<real>(A, G::NI, tid, r0);
+    slopes3<real>(r1, r2, r0, s_cur);  // slope at i0
+    face_flux<real, DO_IS, DO_KT>(p, tau, 0, r1, s_prev, r2, s_cur, F_prev);
+    umu_of<real>(r1, umu_prev);
   }
-  make_record<real>(p, b, tau, i0 + 2, jj, kk, &B[0][tid], G::NI);
+  store_record<real>(p, b, tau, i0 + 2, jj, kk, B, G::NI, tid);
   // halo of the centre plane i0
-  for (int h = tid; h < G::NC; h += TJ * TK) {
-    int r = h / G::CZ, c = h % G::CZ;
-    if (r >= 2 && r < TJ + 2 && c >= 2 && c < TK + 2) continue;
-    make_record<real>(p, b, tau, i0, j0 - 2 + r, k0 - 2 + c, &s.C[0][h], G::NC);
-  }
+  halo_records<real, TJ, TK>(p, b, tau, i0, j0, k0, tid, C);
   __syncthreads();
 
   for (int i = i0; i < i1; i++) {
     // ------------------------------------------------ slopes of plane i
     for (int q = tid; q < G::NSY + G::NSZ; q += TJ * TK) {
+      real rl[RF_N], rm[RF_N], rr[RF_N], sl[NCOMP];
       if (q < G::NSY) {  // y slope at row yr-1, column zc
         int yr = q / TK, zc = q % TK;
         int cm = (yr + 1) * G::CZ + (zc + 2);
-        slopes3<real>(&s.C[0][cm - G::CZ], G::NC, &s.C[0][cm], G::NC, &s.C[0][cm + G::CZ], G::NC, &s.SY[0][q], G::NSY);
+        rec_load<real>(C, G::NC, cm - G::CZ, rl);
+        rec_load<real>(C, G::NC, cm, rm);
+        rec_load<real>(C, G::NC, cm + G::CZ, rr);
+        slopes3<real>(rl, rm, rr, sl);
+        cmp_store<real>(SY4, SY2, G::NSY, q, sl);
       } else {  // z slope at row yr, column zc-1
         int qq = q - G::NSY;
         int yr = qq / (TK + 2), zc = qq % (TK + 2);
         int cm = (yr + 2) * G::CZ + (zc + 1);
-        slopes3<real>(&s.C[0][cm - 1], G::NC, &s.C[0][cm], G::NC, &s.C[0][cm + 1], G::NC, &s.SZ[0][qq], G::NSZ);
+        rec_load<real>(C, G::NC, cm - 1, rl);
+        rec_load<real>(C, G::NC, cm, rm);
+        rec_load<real>(C, G::NC, cm + 1, rr);
+        slopes3<real>(rl, rm, rr, sl);
+        cmp_store<real>(SZ4, SZ2, G::NSZ, qq, sl);
       }
     }
     // x slope at i+1 (own column)
-    slopes3<real>(&s.C[0][cself], G::NC, &A[0][tid], G::NI, &B[0][tid], G::NI, s_next, 1);
+    {
+      real rl[RF_N], rm[RF_N], rr[RF_N];
+      rec_load<real>(C, G::NC, cself, rl);
+      rec_load<real>(A, G::NI, tid, rm);
+      rec_load<real>(B, G::NI, tid, rr);
+      slopes3<real>(rl, rm, rr, s_next);
+    }
     __syncthreads();
 
     // ---------------------------------------------------- face fluxes
@@ -252,50 +378,63 @@ __global__ void __launch_bounds__(TJ * TK, MINB)
     {
       const int sy = (tj + 1) * TK + tk;        // slope slot of own cell (y)
       const int sz = tj * (TK + 2) + (tk + 1);  // slope slot of own cell (z)
-      face_flux<real, DO_IS, DO_KT>(p, tau, 1, &s.C[0][cself], G::NC, &s.SY[0][sy], G::NSY, &s.C[0][cself + G::CZ],
-                                    G::NC, &s.SY[0][sy + TK], G::NSY, Fy);
-      face_flux<real, DO_IS, DO_KT>(p, tau, 2, &s.C[0][cself], G::NC, &s.SZ[0][sz], G::NSZ, &s.C[0][cself + 1], G::NC,
-                                    &s.SZ[0][sz + 1], G::NSZ, Fz);
-      face_flux<real, DO_IS, DO_KT>(p, tau, 0, &s.C[0][cself], G::NC, s_cur, 1, &A[0][tid], G::NI, s_next, 1, Fx);
+      // the own record is read again for each face: holding its 20 values
+      // across the three faces costs more registers than the reads
+      real rs[RF_N], rn[RF_N], sa[NCOMP], sb[NCOMP];
+      rec_load<real>(C, G::NC, cself, rs);
+      rec_load<real>(A, G::NI, tid, rn);
+      face_flux<real, DO_IS, DO_KT>(p, tau, 0, rs, s_cur, rn, s_next, Fx);
+      rec_load<real>(C, G::NC, cself, rs);
+      rec_load<real>(C, G::NC, cself + G::CZ, rn);
+      cmp_load<real>(SY4, SY2, G::NSY, sy, sa);
+      cmp_load<real>(SY4, SY2, G::NSY, sy + TK, sb);
+      face_flux<real, DO_IS, DO_KT>(p, tau, 1, rs, sa, rn, sb, Fy);
+      rec_load<real>(C, G::NC, cself, rs);
+      rec_load<real>(C, G::NC, cself + 1, rn);
+      cmp_load<real>(SZ4, SZ2, G::NSZ, sz, sa);
+      cmp_load<real>(SZ4, SZ2, G::NSZ, sz + 1, sb);
+      face_flux<real, DO_IS, DO_KT>(p, tau, 2, rs, sa, rn, sb, Fz);
       if (tid < TK) {  // y face below row 0, column tid
         const int c0 = 1 * G::CZ + (tid + 2);
-        face_flux<real, DO_IS, DO_KT>(p, tau, 1, &s.C[0][c0], G::NC, &s.SY[0][tid], G::NSY, &s.C[0][c0 + G::CZ], G::NC,
-                                      &s.SY[0][TK + tid], G::NSY, Fh);
+        rec_load<real>(C, G::NC, c0, rs);
+        rec_load<real>(C, G::NC, c0 + G::CZ, rn);
+        cmp_load<real>(SY4, SY2, G::NSY, tid, sa);
+        cmp_load<real>(SY4, SY2, G::NSY, TK + tid, sb);
+        face_flux<real, DO_IS, DO_KT>(p, tau, 1, rs, sa, rn, sb, Fh);
       } else if (tid < TK + TJ) {  // z face left of column 0, row tid-TK
         const int r = tid - TK;
         const int c0 = (r + 2) * G::CZ + 1;
-        face_flux<real, DO_IS, DO_KT>(p, tau, 2, &s.C[0][c0], G::NC, &s.SZ[0][r * (TK + 2)], G::NSZ, &s.C[0][c0 + 1],
-                                      G::NC, &s.SZ[0][r * (TK + 2) + 1], G::NSZ, Fh);
+        rec_load<real>(C, G::NC, c0, rs);
+        rec_load<real>(C, G::NC, c0 + 1, rn);
+        cmp_load<real>(SZ4, SZ2, G::NSZ, r * (TK + 2), sa);
+        cmp_load<real>(SZ4, SZ2, G::NSZ, r * (TK + 2) + 1, sb);
+        face_flux<real, DO_IS, DO_KT>(p, tau, 2, rs, sa, rn, sb, Fh);
       }
     }
     __syncthreads();
     // faces replace slopes: y face j+1/2 in slot (j+1), z face k+1/2 in slot (k+1)
-#pragma unroll
-    for (int c = 0; c < NCOMP; c++) {
-      if (c < 4 && !DO_KT) continue;
-      if (c >= 4 && !DO_IS) continue;
-      s.SY[c][(tj + 1) * TK + tk] = Fy[c];
-      s.SZ[c][tj * (TK + 2) + (tk + 1)] = Fz[c];
-      if (tid < TK) s.SY[c][tid] = Fh[c];
-      else if (tid < TK + TJ) s.SZ[c][(tid - TK) * (TK + 2)] = Fh[c];
-    }
+    cmp_store<real>(SY4, SY2, G::NSY, (tj + 1) * TK + tk, Fy);
+    cmp_store<real>(SZ4, SZ2, G::NSZ, tj * (TK + 2) + (tk + 1), Fz);
+    if (tid < TK) cmp_store<real>(SY4, SY2, G::NSY, tid, Fh);
+    else if (tid < TK + TJ) cmp_store<real>(SZ4, SZ2, G::NSZ, (tid - TK) * (TK + 2), Fh);
     __syncthreads();
 
     // ------------------------------------------------------ cell update
     if (inside && i < p.nx) {
       const long long I = ((long long)i * p.ny + jj) * p.nz + kk;
-      const real* Cc = &s.C[0][cself];
+      real Cc[RF_N];
+      rec_load<real>(C, G::NC, cself, Cc);
       CellIn<real> cin;  // the record holds gamma and P(e) of the stage input
       real* e0 = cin.e0;
-      e0[0] = Cc[RF_E * G::NC];
-      e0[1] = Cc[RF_VX * G::NC];
-      e0[2] = Cc[RF_VY * G::NC];
-      e0[3] = Cc[RF_VZ * G::NC];
-      cin.g0 = Cc[RF_U0 * G::NC];
-      cin.p0 = Cc[RF_PR * G::NC];
+      e0[0] = Cc[RF_E];
+      e0[1] = Cc[RF_VX];
+      e0[2] = Cc[RF_VY];
+      e0[3] = Cc[RF_VZ];
+      cin.g0 = Cc[RF_U0];
+      cin.p0 = Cc[RF_PR];
       real pc[11];  // component 10 (bulk) unused: this kernel has no bulk sector
 #pragma unroll
-      for (int m = 0; m < 10; m++) pc[m] = Cc[(RF_PI + m) * G::NC];
+      for (int m = 0; m < 10; m++) pc[m] = Cc[RF_PI + m];
       real pin[5];
 #pragma unroll
       for (int c = 0; c < 4; c++) pin[c] = DO_KT ? b.pin[c * ld + I] : (real)0.0f;
@@ -345,17 +484,26 @@ __global__ void __launch_bounds__(TJ * TK, MINB)
           S4[3] = S4[3] + 3.0f * Ttz_tilde;
         }
       }
-      // flux differences in the reference's order x, y, z
+      // flux differences in the reference's order x, y, z; the y and z faces
+      // (plus and minus) from shared memory, the x faces from registers
 #pragma unroll
       for (int a = 0; a < 3; a++) {
         const real D = a == 0 ? (real)p.DX : (a == 1 ? (real)p.DY : tc.dzt);
         const real rD = a == 0 ? rc.DX : (a == 1 ? rc.DY : tc.rdzt);
+        real Fp[NCOMP], Fm[NCOMP];
+        if (a == 1) {
+          cmp_load<real>(SY4, SY2, G::NSY, (tj + 1) * TK + tk, Fp);
+          cmp_load<real>(SY4, SY2, G::NSY, tj * TK + tk, Fm);
+        } else if (a == 2) {
+          cmp_load<real>(SZ4, SZ2, G::NSZ, tj * (TK + 2) + (tk + 1), Fp);
+          cmp_load<real>(SZ4, SZ2, G::NSZ, tj * (TK + 2) + tk, Fm);
+        }
 #pragma unroll
         for (int c = 0; c < NCOMP; c++) {
           if (c < 4 && !DO_KT) continue;
           if (c >= 4 && !DO_IS) continue;
-          real fp = a == 0 ? Fx[c] : (a == 1 ? Fy[c] : Fz[c]);
-          real fm = a == 0 ? F_prev[c] : (a == 1 ? s.SY[c][tj * TK + tk] : s.SZ[c][tj * (TK + 2) + tk]);
+          real fp = a == 0 ? Fx[c] : Fp[c];
+          real fm = a == 0 ? F_prev[c] : Fm[c];
           real src = fp;
           src -= fm;
           if (c < 4) S4[c] = S4[c] - div_by<real>(src, D, rD);
@@ -369,19 +517,20 @@ __global__ void __launch_bounds__(TJ * TK, MINB)
         // velocity gradients, kernel_IS.cl:134-137 / 217-220 / 299-304
         real grad[3][4];
         {
-          const real* Cy0 = Cc - G::CZ;
-          const real* Cy1 = Cc + G::CZ;
-          const real* Cz0 = Cc - 1;
-          const real* Cz1 = Cc + 1;
-          real u0c = Cc[RF_U0 * G::NC];
-          real umc[4] = {u0c * 1.0f, u0c * e0[1], u0c * e0[2], u0c * e0[3]};
-          real ua = A[RF_U0][tid];
-          real umx1[4] = {ua * 1.0f, ua * A[RF_VX][tid], ua * A[RF_VY][tid], ua * A[RF_VZ][tid]};
-          real uy0 = Cy0[RF_U0 * G::NC], uy1 = Cy1[RF_U0 * G::NC], uz0 = Cz0[RF_U0 * G::NC], uz1 = Cz1[RF_U0 * G::NC];
-          real umy0[4] = {uy0 * 1.0f, uy0 * Cy0[RF_VX * G::NC], uy0 * Cy0[RF_VY * G::NC], uy0 * Cy0[RF_VZ * G::NC]};
-          real umy1[4] = {uy1 * 1.0f, uy1 * Cy1[RF_VX * G::NC], uy1 * Cy1[RF_VY * G::NC], uy1 * Cy1[RF_VZ * G::NC]};
-          real umz0[4] = {uz0 * 1.0f, uz0 * Cz0[RF_VX * G::NC], uz0 * Cz0[RF_VY * G::NC], uz0 * Cz0[RF_VZ * G::NC]};
-          real umz1[4] = {uz1 * 1.0f, uz1 * Cz1[RF_VX * G::NC], uz1 * Cz1[RF_VY * G::NC], uz1 * Cz1[RF_VZ * G::NC]};
+          real rn[RF_N];
+          real umc[4], umx1[4], umy0[4], umy1[4], umz0[4], umz1[4];
+          umu_of<real>(Cc, umc);
+          rec_load<real>(A, G::NI, tid, rn);
+          umu_of<real>(rn, umx1);
+          rec_load<real>(C, G::NC, cself - G::CZ, rn);
+          umu_of<real>(rn, umy0);
+          rec_load<real>(C, G::NC, cself + G::CZ, rn);
+          umu_of<real>(rn, umy1);
+          rec_load<real>(C, G::NC, cself - 1, rn);
+          umu_of<real>(rn, umz0);
+          rec_load<real>(C, G::NC, cself + 1, rn);
+          umu_of<real>(rn, umz1);
+          const real u0c = Cc[RF_U0];
 #pragma unroll
           for (int c = 0; c < 4; c++) {
             grad[0][c] = div_by<real>(grad_limit<real>(umu_prev[c], umc[c], umx1[c]), (real)p.DX, rc.DX);
@@ -397,11 +546,7 @@ __global__ void __launch_bounds__(TJ * TK, MINB)
         }
         pi_update<real, COUPLED, false>(p, b, step, tc, I, ld, cin, pc, grad, S10, pinew);
       } else {
-        real u0c = Cc[RF_U0 * G::NC];
-        umu_prev[0] = u0c * 1.0f;
-        umu_prev[1] = u0c * e0[1];
-        umu_prev[2] = u0c * e0[2];
-        umu_prev[3] = u0c * e0[3];
+        umu_of<real>(Cc, umu_prev);
       }
       if (DO_KT) ev_update<real, DO_IS, false>(p, b, step, tc, I, ld, cin, pin, S4, pinew);
       if (b.write_src) {
@@ -422,17 +567,16 @@ __global__ void __launch_bounds__(TJ * TK, MINB)
 
     // --------------------------------------------------------- advance
     if (i + 1 < i1) {
-#pragma unroll
-      for (int f = 0; f < RF_N; f++) s.C[f][cself] = A[f][tid];
-      real(*t)[G::NI] = A;
+      {
+        real r[RF_N];
+        rec_load<real>(A, G::NI, tid, r);
+        rec_store<real>(C, G::NC, cself, r);
+      }
+      real* t = A;
       A = B;
       B = t;
-      make_record<real>(p, b, tau, i + 3, jj, kk, &B[0][tid], G::NI);
-      for (int h = tid; h < G::NC; h += TJ * TK) {
-        int r = h / G::CZ, c = h % G::CZ;
-        if (r >= 2 && r < TJ + 2 && c >= 2 && c < TK + 2) continue;
-        make_record<real>(p, b, tau, i + 1, j0 - 2 + r, k0 - 2 + c, &s.C[0][h], G::NC);
-      }
+      store_record<real>(p, b, tau, i + 3, jj, kk, B, G::NI, tid);
+      halo_records<real, TJ, TK>(p, b, tau, i + 1, j0, k0, tid, C);
       __syncthreads();
     }
   }
