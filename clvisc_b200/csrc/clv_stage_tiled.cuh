@@ -8,10 +8,10 @@
 //   * Per cell, a record (ev, P(e), u0, Q = tau*(T0m + pi^{tau mu}), pi) is
 //     computed once, into shared memory: the centre plane with a 2-cell halo
 //     in j and k, and the two planes ahead (i+1, i+2) for the x stencil.
-//     A record's 20 values are five groups of four, each group of a plane
-//     stored cell by cell, so a group moves in one 16-byte (FP32) or two
-//     16-byte (FP64) shared-memory accesses; slopes and face fluxes (14
-//     components) likewise as three groups of four and one pair.
+//     A record's 20 values are groups of 16 bytes (four floats or two
+//     doubles), each group of a plane stored cell by cell, so a group moves
+//     in one shared-memory access and a warp's accesses are contiguous;
+//     slopes and face fluxes (14 components) likewise.
 //   * The limited slope of every cell is computed once per direction, and the
 //     flux through every face once; a cell's flux difference subtracts the
 //     flux of its minus face from that of its plus face, exactly the two
@@ -34,12 +34,21 @@ namespace clv {
 #define CLV_TILED_ATTR __noinline__
 #endif
 
-// record fields: groups of four, field f in group f / 4, lane f % 4
+// record fields; in shared memory a plane's records are stored as groups of
+// U = 16 / sizeof(real) fields (four floats or two doubles), each group cell
+// by cell: field f of cell c at [f / U][c][f % U], so a group moves in one
+// 16-byte access and a warp's accesses to one group are contiguous
 enum { RF_E = 0, RF_VX, RF_VY, RF_VZ, RF_PR, RF_U0, RF_Q0, RF_Q1, RF_Q2, RF_Q3, RF_PI, RF_N = RF_PI + 10 };
-enum { RG = RF_N / 4 };  // record groups
-// slope / face-flux components: 0..3 KT (Q), 4..13 IS (u0*pi); groups 0..2 of
-// four and the pair 12, 13
-enum { NCOMP = 14, SG4 = 3 };
+// slope / face-flux components: 0..3 KT (Q), 4..13 IS (u0*pi); as groups of U
+// and, for floats, a tail pair (12, 13)
+enum { NCOMP = 14 };
+
+template <class real> struct Lanes {
+  static constexpr int U = 16 / (int)sizeof(real);  // reals in 16 bytes
+  static constexpr int RG = RF_N / U;              // record groups: 5 (FP32), 10 (FP64)
+  static constexpr int SG = NCOMP / U;             // slope groups: 3, 7
+  static constexpr int ST = NCOMP % U;             // slope tail: 2, 0
+};
 
 template <int TJ, int TK> struct TileGeom {
   static constexpr int CY = TJ + 4, CZ = TK + 4;     // centre region with halo
@@ -50,72 +59,74 @@ template <int TJ, int TK> struct TileGeom {
   static constexpr int NHALO = NC - NI;               // halo cells of the centre plane
 };
 
-template <class real, int TJ, int TK> struct TileSmem {
-  typedef TileGeom<TJ, TK> G;
-  __align__(16) real C[RG][G::NC][4];     // centre plane i
-  __align__(16) real A[RG][G::NI][4];     // plane i+1 (interior)
-  __align__(16) real B[RG][G::NI][4];     // plane i+2 (interior)
-  __align__(16) real SY4[SG4][G::NSY][4];  // y slopes, then y face fluxes: components 0..11
-  __align__(16) real SY2[G::NSY][2];       //   components 12, 13
-  __align__(16) real SZ4[SG4][G::NSZ][4];  // z slopes, then z face fluxes
-  __align__(16) real SZ2[G::NSZ][2];
+// slope tail of n slots (none for doubles: one unused element)
+template <class real, int N, int ST> struct SlopeTail {
+  __align__(16) real v[N][ST];
+};
+template <class real, int N> struct SlopeTail<real, N, 0> {
+  real v[1][1];
 };
 
-// 16-byte shared-memory moves of four or two reals (two 16-byte moves for
-// four doubles)
-template <class real> __device__ __forceinline__ void lds4(const real* p, real* o) {
+template <class real, int TJ, int TK> struct TileSmem {
+  typedef TileGeom<TJ, TK> G;
+  typedef Lanes<real> L;
+  __align__(16) real C[L::RG][G::NC][L::U];     // centre plane i
+  __align__(16) real A[L::RG][G::NI][L::U];     // plane i+1 (interior)
+  __align__(16) real B[L::RG][G::NI][L::U];     // plane i+2 (interior)
+  __align__(16) real SY[L::SG][G::NSY][L::U];   // y slopes, then y face fluxes
+  __align__(16) real SZ[L::SG][G::NSZ][L::U];   // z slopes, then z face fluxes
+  SlopeTail<real, G::NSY, L::ST> SYT;
+  SlopeTail<real, G::NSZ, L::ST> SZT;
+};
+
+// 16-byte shared-memory moves: four floats or two doubles
+template <class real> __device__ __forceinline__ void ld16(const real* p, real* o) {
   if constexpr (sizeof(real) == 4) {
     const float4 t = *reinterpret_cast<const float4*>(p);
     o[0] = t.x; o[1] = t.y; o[2] = t.z; o[3] = t.w;
-  } else {
-    const double2 a = reinterpret_cast<const double2*>(p)[0], b = reinterpret_cast<const double2*>(p)[1];
-    o[0] = a.x; o[1] = a.y; o[2] = b.x; o[3] = b.y;
-  }
-}
-template <class real> __device__ __forceinline__ void sts4(real* p, const real* v) {
-  if constexpr (sizeof(real) == 4) {
-    *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
-  } else {
-    reinterpret_cast<double2*>(p)[0] = make_double2(v[0], v[1]);
-    reinterpret_cast<double2*>(p)[1] = make_double2(v[2], v[3]);
-  }
-}
-template <class real> __device__ __forceinline__ void lds2(const real* p, real* o) {
-  if constexpr (sizeof(real) == 4) {
-    const float2 t = *reinterpret_cast<const float2*>(p);
-    o[0] = t.x; o[1] = t.y;
   } else {
     const double2 t = *reinterpret_cast<const double2*>(p);
     o[0] = t.x; o[1] = t.y;
   }
 }
-template <class real> __device__ __forceinline__ void sts2(real* p, const real* v) {
-  if constexpr (sizeof(real) == 4) *reinterpret_cast<float2*>(p) = make_float2(v[0], v[1]);
+template <class real> __device__ __forceinline__ void st16(real* p, const real* v) {
+  if constexpr (sizeof(real) == 4) *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
   else *reinterpret_cast<double2*>(p) = make_double2(v[0], v[1]);
 }
 
 // a record of cell c of a plane of n cells (plane = &X[0][0][0]); groups
 // whose values go unused are dropped by the compiler
 template <class real> __device__ __forceinline__ void rec_load(const real* plane, int n, int c, real r[RF_N]) {
+  typedef Lanes<real> L;
 #pragma unroll
-  for (int g = 0; g < RG; g++) lds4<real>(plane + ((size_t)g * n + c) * 4, r + 4 * g);
+  for (int g = 0; g < L::RG; g++) ld16<real>(plane + ((size_t)g * n + c) * L::U, r + L::U * g);
 }
 template <class real> __device__ __forceinline__ void rec_store(real* plane, int n, int c, const real r[RF_N]) {
+  typedef Lanes<real> L;
 #pragma unroll
-  for (int g = 0; g < RG; g++) sts4<real>(plane + ((size_t)g * n + c) * 4, r + 4 * g);
+  for (int g = 0; g < L::RG; g++) st16<real>(plane + ((size_t)g * n + c) * L::U, r + L::U * g);
 }
-// the 14 slope (or face) components of slot c of an array of n slots
+// the 14 slope (or face) components of slot c of an array of n slots (sg:
+// the groups, st: the tail)
 template <class real>
-__device__ __forceinline__ void cmp_load(const real* s4, const real* s2, int n, int c, real v[NCOMP]) {
+__device__ __forceinline__ void cmp_load(const real* sg, const real* st, int n, int c, real v[NCOMP]) {
+  typedef Lanes<real> L;
 #pragma unroll
-  for (int g = 0; g < SG4; g++) lds4<real>(s4 + ((size_t)g * n + c) * 4, v + 4 * g);
-  lds2<real>(s2 + (size_t)c * 2, v + 12);
+  for (int g = 0; g < L::SG; g++) ld16<real>(sg + ((size_t)g * n + c) * L::U, v + L::U * g);
+  if constexpr (L::ST == 2) {
+    const float2 t = *reinterpret_cast<const float2*>(st + (size_t)c * 2);
+    v[NCOMP - 2] = t.x;
+    v[NCOMP - 1] = t.y;
+  }
+  (void)st;
 }
 template <class real>
-__device__ __forceinline__ void cmp_store(real* s4, real* s2, int n, int c, const real v[NCOMP]) {
+__device__ __forceinline__ void cmp_store(real* sg, real* st, int n, int c, const real v[NCOMP]) {
+  typedef Lanes<real> L;
 #pragma unroll
-  for (int g = 0; g < SG4; g++) sts4<real>(s4 + ((size_t)g * n + c) * 4, v + 4 * g);
-  sts2<real>(s2 + (size_t)c * 2, v + 12);
+  for (int g = 0; g < L::SG; g++) st16<real>(sg + ((size_t)g * n + c) * L::U, v + L::U * g);
+  if constexpr (L::ST == 2) *reinterpret_cast<float2*>(st + (size_t)c * 2) = make_float2(v[NCOMP - 2], v[NCOMP - 1]);
+  (void)st;
 }
 
 inline namespace CLV_ARITH {
@@ -302,10 +313,10 @@ __global__ void __launch_bounds__(TJ * TK, MINB)
   real* const C = &s.C[0][0][0];
   real* A = &s.A[0][0][0];
   real* B = &s.B[0][0][0];
-  real* const SY4 = &s.SY4[0][0][0];
-  real* const SY2 = &s.SY2[0][0];
-  real* const SZ4 = &s.SZ4[0][0][0];
-  real* const SZ2 = &s.SZ2[0][0];
+  real* const SY4 = &s.SY[0][0][0];
+  real* const SY2 = &s.SYT.v[0][0];
+  real* const SZ4 = &s.SZ[0][0][0];
+  real* const SZ2 = &s.SZT.v[0][0];
 
   const int tid = threadIdx.x;
   const int tj = tid / TK, tk = tid % TK;
