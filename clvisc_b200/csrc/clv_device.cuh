@@ -290,11 +290,15 @@ __device__ __forceinline__ real max_speed(const Params& p, real e, real vx, real
 // helper.h:128-167; returns the energy density. With BULK the pressure is
 // P(e) + bulk, the bulk viscous pressure of the cell.
 template <class real, bool BULK = false>
-__device__ __forceinline__ real root_newton(const Params& p, real T00, real M, real bulk = (real)0.0f) {
+__device__ __forceinline__ real root_newton(const Params& p, real T00, real M, real bulk = (real)0.0f,
+                                            real v_start = (real)-1.0f) {
   real vl = 0.0f;
   real vh = 1.0f;
   real dpe = 1.0f / 3.0f;
-  real v = 0.5f * (vl + vh);
+  // the reference starts at the middle of the bracket; a start in [0, 1)
+  // (the tolerance build passes the cell's speed at the start of the step)
+  // leaves the bracket and the safeguards as they are
+  real v = v_start >= (real)0.0f ? v_start : 0.5f * (vl + vh);
   real ed = T00 - M * v;
   real pr = eosP<real>(p, ed);
   if (BULK) pr = pr + bulk;
