@@ -26,7 +26,7 @@ SOURCES = ['csrc/clv_capi.cu', 'csrc/clv_noalloc.cu', 'csrc/clv_batch.cu', 'csrc
 DEPS = ['csrc/clv_device.cuh', 'csrc/clv_stage.cuh', 'csrc/clv_stage_tiled.cuh', 'csrc/clv_stage_tiled2d.cuh',
         'csrc/clv_misc.cuh',
         'csrc/clv_hypersf.cuh', 'csrc/clv_batch.cuh', 'csrc/clv_initial.cuh',
-        'csrc/clv_bulkinfo.cuh', 'csrc/clv_spectra.cuh', 'csrc/clv_unet.cuh', 'csrc/clv_fast.h', 'csrc/clv_batch_launch.cuh',
+        'csrc/clv_bulkinfo.cuh', 'csrc/clv_spectra.cuh', 'csrc/clv_unet.cuh', 'csrc/clv_fast.h', 'csrc/clv_batch_launch.cuh', 'csrc/clv_smem16.cuh',
         '../include/clvisc_b200.h']
 
 NVCC_FLAGS = [

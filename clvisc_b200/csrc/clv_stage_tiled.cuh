@@ -21,6 +21,7 @@
 // Each face flux, slope and record is an expression-for-expression copy of
 // the per-cell kernel's, so the results are identical bit for bit.
 #pragma once
+#include "clv_smem16.cuh"
 #include "clv_stage.cuh"
 
 namespace clv {
@@ -78,21 +79,6 @@ template <class real, int TJ, int TK> struct TileSmem {
   SlopeTail<real, G::NSY, L::ST> SYT;
   SlopeTail<real, G::NSZ, L::ST> SZT;
 };
-
-// 16-byte shared-memory moves: four floats or two doubles
-template <class real> __device__ __forceinline__ void ld16(const real* p, real* o) {
-  if constexpr (sizeof(real) == 4) {
-    const float4 t = *reinterpret_cast<const float4*>(p);
-    o[0] = t.x; o[1] = t.y; o[2] = t.z; o[3] = t.w;
-  } else {
-    const double2 t = *reinterpret_cast<const double2*>(p);
-    o[0] = t.x; o[1] = t.y;
-  }
-}
-template <class real> __device__ __forceinline__ void st16(real* p, const real* v) {
-  if constexpr (sizeof(real) == 4) *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
-  else *reinterpret_cast<double2*>(p) = make_double2(v[0], v[1]);
-}
 
 // a record of cell c of a plane of n cells (plane = &X[0][0][0]); groups
 // whose values go unused are dropped by the compiler
@@ -385,13 +371,34 @@ __global__ void __launch_bounds__(TJ * TK, MINB)
     __syncthreads();
 
     // ---------------------------------------------------- face fluxes
-    real Fy[NCOMP], Fz[NCOMP], Fx[NCOMP], Fh[NCOMP];
+    real Fy[NCOMP], Fz[NCOMP], Fx[NCOMP];
     {
       const int sy = (tj + 1) * TK + tk;        // slope slot of own cell (y)
       const int sz = tj * (TK + 2) + (tk + 1);  // slope slot of own cell (z)
+      real rs[RF_N], rn[RF_N], sa[NCOMP], sb[NCOMP], Fh[NCOMP];
+      // the outer faces of the tile first, each stored at once: its slope
+      // slots (row -1, column -1) are read by this thread alone, and nothing
+      // of it stays live beside the three faces of the own cell
+      if (tid < TK) {  // y face below row 0, column tid
+        const int c0 = 1 * G::CZ + (tid + 2);
+        rec_load<real>(C, G::NC, c0, rs);
+        rec_load<real>(C, G::NC, c0 + G::CZ, rn);
+        cmp_load<real>(SY4, SY2, G::NSY, tid, sa);
+        cmp_load<real>(SY4, SY2, G::NSY, TK + tid, sb);
+        face_flux<real, DO_IS, DO_KT>(p, tau, 1, rs, sa, rn, sb, Fh);
+        cmp_store<real>(SY4, SY2, G::NSY, tid, Fh);
+      } else if (tid < TK + TJ) {  // z face left of column 0, row tid-TK
+        const int r = tid - TK;
+        const int c0 = (r + 2) * G::CZ + 1;
+        rec_load<real>(C, G::NC, c0, rs);
+        rec_load<real>(C, G::NC, c0 + 1, rn);
+        cmp_load<real>(SZ4, SZ2, G::NSZ, r * (TK + 2), sa);
+        cmp_load<real>(SZ4, SZ2, G::NSZ, r * (TK + 2) + 1, sb);
+        face_flux<real, DO_IS, DO_KT>(p, tau, 2, rs, sa, rn, sb, Fh);
+        cmp_store<real>(SZ4, SZ2, G::NSZ, r * (TK + 2), Fh);
+      }
       // the own record is read again for each face: holding its 20 values
       // across the three faces costs more registers than the reads
-      real rs[RF_N], rn[RF_N], sa[NCOMP], sb[NCOMP];
       rec_load<real>(C, G::NC, cself, rs);
       rec_load<real>(A, G::NI, tid, rn);
       face_flux<real, DO_IS, DO_KT>(p, tau, 0, rs, s_cur, rn, s_next, Fx);
@@ -405,29 +412,11 @@ __global__ void __launch_bounds__(TJ * TK, MINB)
       cmp_load<real>(SZ4, SZ2, G::NSZ, sz, sa);
       cmp_load<real>(SZ4, SZ2, G::NSZ, sz + 1, sb);
       face_flux<real, DO_IS, DO_KT>(p, tau, 2, rs, sa, rn, sb, Fz);
-      if (tid < TK) {  // y face below row 0, column tid
-        const int c0 = 1 * G::CZ + (tid + 2);
-        rec_load<real>(C, G::NC, c0, rs);
-        rec_load<real>(C, G::NC, c0 + G::CZ, rn);
-        cmp_load<real>(SY4, SY2, G::NSY, tid, sa);
-        cmp_load<real>(SY4, SY2, G::NSY, TK + tid, sb);
-        face_flux<real, DO_IS, DO_KT>(p, tau, 1, rs, sa, rn, sb, Fh);
-      } else if (tid < TK + TJ) {  // z face left of column 0, row tid-TK
-        const int r = tid - TK;
-        const int c0 = (r + 2) * G::CZ + 1;
-        rec_load<real>(C, G::NC, c0, rs);
-        rec_load<real>(C, G::NC, c0 + 1, rn);
-        cmp_load<real>(SZ4, SZ2, G::NSZ, r * (TK + 2), sa);
-        cmp_load<real>(SZ4, SZ2, G::NSZ, r * (TK + 2) + 1, sb);
-        face_flux<real, DO_IS, DO_KT>(p, tau, 2, rs, sa, rn, sb, Fh);
-      }
     }
     __syncthreads();
     // faces replace slopes: y face j+1/2 in slot (j+1), z face k+1/2 in slot (k+1)
     cmp_store<real>(SY4, SY2, G::NSY, (tj + 1) * TK + tk, Fy);
     cmp_store<real>(SZ4, SZ2, G::NSZ, tj * (TK + 2) + (tk + 1), Fz);
-    if (tid < TK) cmp_store<real>(SY4, SY2, G::NSY, tid, Fh);
-    else if (tid < TK + TJ) cmp_store<real>(SZ4, SZ2, G::NSZ, (tid - TK) * (TK + 2), Fh);
     __syncthreads();
 
     // ------------------------------------------------------ cell update
