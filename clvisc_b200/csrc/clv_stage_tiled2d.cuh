@@ -11,7 +11,8 @@
 //   * Per cell, a record (ev, P(e) + Pi, gamma, Q = tau*(T0m + pi^{tau mu}),
 //     pi, Pi, P(e)) is computed once per plane into shared memory; the two
 //     planes ahead (i+1, i+2) of the thread's own row sit in per-thread
-//     shared-memory slots.
+//     shared-memory slots. Records, slopes and faces are stored as 16-byte
+//     groups (clv_smem16.cuh), one shared-memory access a group.
 //   * The limited slope of every cell is computed once per direction and the
 //     flux through every face once; a cell's flux difference subtracts its
 //     minus face from its plus face, exactly the two values the reference
@@ -22,6 +23,7 @@
 // Each record, slope and face flux is the per-cell kernel's expression, so the
 // results are identical bit for bit.
 #pragma once
+#include "clv_smem16.cuh"
 #include "clv_stage.cuh"
 
 namespace clv {
@@ -41,22 +43,35 @@ template <bool BULK> struct Rec2 {
   };
 };
 
+// a record (and the slope and face components) padded to whole 16-byte
+// groups of U = 16 / sizeof(real) values
+template <class real, bool BULK> struct Rec2L {
+  static constexpr int U = Smem16<real>::U;
+  static constexpr int NP = Smem16<real>::pad(Rec2<BULK>::N), RG = NP / U;
+  static constexpr int CP = Smem16<real>::pad(Rec2<BULK>::NCOMP), CG = CP / U;
+};
+
+// each region stores its values as 16-byte groups, each group row by row
+// ([value / U][row][value % U]): a group moves in one access
 template <class real, bool BULK, int TB> struct Tile2Smem {
-  typedef Rec2<BULK> R;
-  real C[R::N][TB];       // plane i, every row of the block
-  real A[R::N][TB];       // plane i+1, own row
-  real B[R::N][TB];       // plane i+2, own row
-  real SY[R::NCOMP][TB];  // y slope of row t
-  real FY[R::NCOMP][TB];  // flux through the y face between rows t and t+1
+  typedef Rec2L<real, BULK> L;
+  __align__(16) real C[L::RG][TB][L::U];   // plane i, every row of the block
+  __align__(16) real A[L::RG][TB][L::U];   // plane i+1, own row
+  __align__(16) real B[L::RG][TB][L::U];   // plane i+2, own row
+  __align__(16) real SY[L::CG][TB][L::U];  // y slope of row t
+  __align__(16) real FY[L::CG][TB][L::U];  // flux through the y face between rows t and t+1
 };
 
 inline namespace CLV_ARITH {
 
-// record of the (clamped) cell (i, j) of the stage input, NZ = 1
+// record of the (clamped) cell (i, j) of the stage input, NZ = 1, into dst
 template <class real, bool BULK>
 __device__ __forceinline__ void rec2_make(const Params& p, const GridDims& gd, const ViscBuffers<real>& b, real tau,
-                                          int i, int j, real* dst, int stride) {
+                                          int i, int j, real dst[Rec2L<real, BULK>::NP]) {
   typedef Rec2<BULK> R;
+  constexpr int stride = 1;
+#pragma unroll
+  for (int f = R::N; f < Rec2L<real, BULK>::NP; f++) dst[f] = 0.0f;  // padding
   i = min(max(i, 0), gd.nx - 1);
   j = min(max(j, 0), gd.ny - 1);
   const long long I = (long long)i * gd.ny + j;
@@ -90,9 +105,11 @@ __device__ __forceinline__ void rec2_make(const Params& p, const GridDims& gd, c
 
 // limited slopes of every component at the middle of three records
 template <class real, bool BULK>
-__device__ __forceinline__ void rec2_slopes(const real* L, int sl, const real* M, int sm, const real* R_, int sr,
-                                            real* out, int so) {
+__device__ __forceinline__ void rec2_slopes(const real* L, const real* M, const real* R_, real* out) {
   typedef Rec2<BULK> R;
+  constexpr int sl = 1, sm = 1, sr = 1, so = 1;
+#pragma unroll
+  for (int c = R::NCOMP; c < Rec2L<real, BULK>::CP; c++) out[c] = 0.0f;  // padding
 #pragma unroll
   for (int c = 0; c < 4; c++) out[c * so] = slope<real>(L[(R::Q0 + c) * sl], M[(R::Q0 + c) * sm], R_[(R::Q0 + c) * sr]);
   real uL = L[R::U0 * sl], uM = M[R::U0 * sm], uR = R_[R::U0 * sr];
@@ -104,10 +121,12 @@ __device__ __forceinline__ void rec2_slopes(const real* L, int sl, const real* M
 
 // flux through the face between records L and R along axis a (0: x, 1: y)
 template <class real, bool BULK>
-__device__ __forceinline__ void rec2_face(const Params& p, real tau, int a, const real* L, int sl, const real* sL,
-                                          int ssl, const real* R_, int sr, const real* sR, int ssr,
-                                          real F[Rec2<BULK>::NCOMP]) {
+__device__ __forceinline__ void rec2_face(const Params& p, real tau, int a, const real* L, const real* sL,
+                                          const real* R_, const real* sR, real F[Rec2L<real, BULK>::CP]) {
   typedef Rec2<BULK> R;
+  constexpr int sl = 1, ssl = 1, sr = 1, ssr = 1;
+#pragma unroll
+  for (int c = R::NCOMP; c < Rec2L<real, BULK>::CP; c++) F[c] = 0.0f;  // padding
 #if CLV_FAST
   // tolerance build, KT speed 1: the weighted form of the (3+1)D kernel's
   // face_flux (cp = (v+1)/2 on the left state, cm = (v-1)/2 on the right)
@@ -178,7 +197,8 @@ template <class real, bool BULK, int TB>
 __device__ __forceinline__ void tile2d(const Params& p, const GridDims& gd, const ViscBuffers<real>& b, int step,
                                        const TauConst<real>& tc, int j0, int i0, int i1, Tile2Smem<real, BULK, TB>& s) {
   typedef Rec2<BULK> R;
-  constexpr int NC = R::NCOMP;
+  typedef Rec2L<real, BULK> L;
+  constexpr int NC = R::NCOMP, NP = L::NP, CP = L::CP, RG = L::RG, CG = L::CG;
   const real tau = tc.tau;
   const Recips<real>& rc = recips<real>(p);
   const long long ld = gd.ld;
@@ -186,63 +206,93 @@ __device__ __forceinline__ void tile2d(const Params& p, const GridDims& gd, cons
   const int jj = j0 - 2 + t;                  // this thread's row
   const bool mid = (t >= 2) && (t < TB - 2);  // a row of the tile (not its halo)
   const bool inside = mid && (jj < gd.ny);
-  real(*A)[TB] = s.A;
-  real(*B)[TB] = s.B;
-  real* const Cs = &s.C[0][t];  // own record in the plane region (stride TB)
+  real* const Cp = &s.C[0][0][0];  // plane i, slot t: row t
+  real* A = &s.A[0][0][0];         // own slot t
+  real* B = &s.B[0][0][0];
+  real* const SYp = &s.SY[0][0][0];
+  real* const FYp = &s.FY[0][0][0];
 
   // ------------------------------------------------------------ prologue
-  real s_cur[NC], F_prev[NC], s_next[NC], umu_prev[4];
+  real s_cur[CP], F_prev[CP], s_next[CP], umu_prev[4];
   if (mid) {
-    real s_prev[NC];
-    rec2_make<real, BULK>(p, gd, b, tau, i0 - 2, jj, &A[0][t], TB);
-    rec2_make<real, BULK>(p, gd, b, tau, i0 - 1, jj, &B[0][t], TB);
-    rec2_make<real, BULK>(p, gd, b, tau, i0, jj, Cs, TB);
-    rec2_slopes<real, BULK>(&A[0][t], TB, &B[0][t], TB, Cs, TB, s_prev, 1);  // x slope at i0-1
-    rec2_make<real, BULK>(p, gd, b, tau, i0 + 1, jj, &A[0][t], TB);
-    rec2_slopes<real, BULK>(&B[0][t], TB, Cs, TB, &A[0][t], TB, s_cur, 1);   // x slope at i0
-    rec2_face<real, BULK>(p, tau, 0, &B[0][t], TB, s_prev, 1, Cs, TB, s_cur, 1, F_prev);
-    real u0 = B[R::U0][t];
+    real r0[NP], r1[NP], r2[NP], s_prev[CP];
+    rec2_make<real, BULK>(p, gd, b, tau, i0 - 2, jj, r0);
+    rec2_make<real, BULK>(p, gd, b, tau, i0 - 1, jj, r1);
+    rec2_make<real, BULK>(p, gd, b, tau, i0, jj, r2);
+    grp_store<real, RG>(Cp, TB, t, r2);
+    rec2_slopes<real, BULK>(r0, r1, r2, s_prev);  // x slope at i0-1
+    rec2_make<real, BULK>(p, gd, b, tau, i0 + 1, jj, r0);
+    grp_store<real, RG>(A, TB, t, r0);
+    rec2_slopes<real, BULK>(r1, r2, r0, s_cur);  // x slope at i0
+    rec2_face<real, BULK>(p, tau, 0, r1, s_prev, r2, s_cur, F_prev);
+    real u0 = r1[R::U0];
     umu_prev[0] = u0 * 1.0f;
-    umu_prev[1] = u0 * B[R::VX][t];
-    umu_prev[2] = u0 * B[R::VY][t];
-    umu_prev[3] = u0 * B[R::VZ][t];
-    rec2_make<real, BULK>(p, gd, b, tau, i0 + 2, jj, &B[0][t], TB);
+    umu_prev[1] = u0 * r1[R::VX];
+    umu_prev[2] = u0 * r1[R::VY];
+    umu_prev[3] = u0 * r1[R::VZ];
+    rec2_make<real, BULK>(p, gd, b, tau, i0 + 2, jj, r0);
+    grp_store<real, RG>(B, TB, t, r0);
   } else {
-    rec2_make<real, BULK>(p, gd, b, tau, i0, jj, Cs, TB);
+    real r0[NP];
+    rec2_make<real, BULK>(p, gd, b, tau, i0, jj, r0);
+    grp_store<real, RG>(Cp, TB, t, r0);
   }
   __syncthreads();
 
   for (int i = i0; i < i1; i++) {
     // ------------------------------------------- slopes: y of row t, x at i+1
-    if (t >= 1 && t <= TB - 2) rec2_slopes<real, BULK>(Cs - 1, TB, Cs, TB, Cs + 1, TB, &s.SY[0][t], TB);
-    if (mid) rec2_slopes<real, BULK>(Cs, TB, &A[0][t], TB, &B[0][t], TB, s_next, 1);
+    if (t >= 1 && t <= TB - 2) {
+      real rl[NP], rm[NP], rr[NP], sy[CP];
+      grp_load<real, RG>(Cp, TB, t - 1, rl);
+      grp_load<real, RG>(Cp, TB, t, rm);
+      grp_load<real, RG>(Cp, TB, t + 1, rr);
+      rec2_slopes<real, BULK>(rl, rm, rr, sy);
+      grp_store<real, CG>(SYp, TB, t, sy);
+    }
+    if (mid) {
+      real rl[NP], rm[NP], rr[NP];
+      grp_load<real, RG>(Cp, TB, t, rl);
+      grp_load<real, RG>(A, TB, t, rm);
+      grp_load<real, RG>(B, TB, t, rr);
+      rec2_slopes<real, BULK>(rl, rm, rr, s_next);
+    }
     __syncthreads();
 
     // ------------------------------------- faces: y between t and t+1, x at i+1/2
-    real Fx[NC];
+    real Fx[CP];
     if (t >= 1 && t <= TB - 3) {
-      real Fy[NC];
-      rec2_face<real, BULK>(p, tau, 1, Cs, TB, &s.SY[0][t], TB, Cs + 1, TB, &s.SY[0][t + 1], TB, Fy);
-#pragma unroll
-      for (int c = 0; c < NC; c++) s.FY[c][t] = Fy[c];
+      real rl[NP], rr[NP], sl[CP], sr[CP], Fy[CP];
+      grp_load<real, RG>(Cp, TB, t, rl);
+      grp_load<real, RG>(Cp, TB, t + 1, rr);
+      grp_load<real, CG>(SYp, TB, t, sl);
+      grp_load<real, CG>(SYp, TB, t + 1, sr);
+      rec2_face<real, BULK>(p, tau, 1, rl, sl, rr, sr, Fy);
+      grp_store<real, CG>(FYp, TB, t, Fy);
     }
-    if (mid) rec2_face<real, BULK>(p, tau, 0, Cs, TB, s_cur, 1, &A[0][t], TB, s_next, 1, Fx);
+    if (mid) {
+      real rl[NP], rr[NP];
+      grp_load<real, RG>(Cp, TB, t, rl);
+      grp_load<real, RG>(A, TB, t, rr);
+      rec2_face<real, BULK>(p, tau, 0, rl, s_cur, rr, s_next, Fx);
+    }
     __syncthreads();
 
     // ------------------------------------------------------ cell update
     if (inside && i < gd.nx) {
       const long long I = (long long)i * gd.ny + jj;
+      real Cs[NP];
+      grp_load<real, RG>(Cp, TB, t, Cs);
       CellIn<real> cin;
       real* e0 = cin.e0;
-      e0[0] = Cs[R::E * TB];
-      e0[1] = Cs[R::VX * TB];
-      e0[2] = Cs[R::VY * TB];
-      e0[3] = Cs[R::VZ * TB];
-      cin.g0 = Cs[R::U0 * TB];
-      cin.p0 = Cs[R::P0 * TB];
+      e0[0] = Cs[R::E];
+      e0[1] = Cs[R::VX];
+      e0[2] = Cs[R::VY];
+      e0[3] = Cs[R::VZ];
+      cin.g0 = Cs[R::U0];
+      cin.p0 = Cs[R::P0];
       real pc[11];
 #pragma unroll
-      for (int m = 0; m < R::NPI; m++) pc[m] = Cs[(R::PI + m) * TB];
+      for (int m = 0; m < R::NPI; m++) pc[m] = Cs[R::PI + m];
       if (!BULK) pc[10] = 0.0f;
       real pin[5];
 #pragma unroll
@@ -293,14 +343,17 @@ __device__ __forceinline__ void tile2d(const Params& p, const GridDims& gd, cons
         }
       }
       // flux differences in the reference's order x, y (eta: one cell, none)
+      real Fyp[CP], Fym[CP];
+      grp_load<real, CG>(FYp, TB, t, Fyp);
+      grp_load<real, CG>(FYp, TB, t - 1, Fym);
 #pragma unroll
       for (int a = 0; a < 2; a++) {
         const real D = a == 0 ? (real)p.DX : (real)p.DY;
         const real rD = a == 0 ? rc.DX : rc.DY;
 #pragma unroll
         for (int c = 0; c < NC; c++) {
-          real fp = a == 0 ? Fx[c] : s.FY[c][t];
-          real fm = a == 0 ? F_prev[c] : s.FY[c][t - 1];
+          real fp = a == 0 ? Fx[c] : Fyp[c];
+          real fm = a == 0 ? F_prev[c] : Fym[c];
           real src = fp;
           src -= fm;
           if (c < 4) S4[c] = S4[c] - div_by<real>(src, D, rD);
@@ -310,15 +363,17 @@ __device__ __forceinline__ void tile2d(const Params& p, const GridDims& gd, cons
       // velocity gradients, kernel_IS.cl:134-137 / 217-220 / 299-304
       real grad[3][4];
       {
-        const real* Cy0 = Cs - 1;
-        const real* Cy1 = Cs + 1;
+        real Ax[NP], Cy0[NP], Cy1[NP];
+        grp_load<real, RG>(A, TB, t, Ax);
+        grp_load<real, RG>(Cp, TB, t - 1, Cy0);
+        grp_load<real, RG>(Cp, TB, t + 1, Cy1);
         real u0c = cin.g0;
         real umc[4] = {u0c * 1.0f, u0c * e0[1], u0c * e0[2], u0c * e0[3]};
-        real ua = A[R::U0][t];
-        real umx1[4] = {ua * 1.0f, ua * A[R::VX][t], ua * A[R::VY][t], ua * A[R::VZ][t]};
-        real uy0 = Cy0[R::U0 * TB], uy1 = Cy1[R::U0 * TB];
-        real umy0[4] = {uy0 * 1.0f, uy0 * Cy0[R::VX * TB], uy0 * Cy0[R::VY * TB], uy0 * Cy0[R::VZ * TB]};
-        real umy1[4] = {uy1 * 1.0f, uy1 * Cy1[R::VX * TB], uy1 * Cy1[R::VY * TB], uy1 * Cy1[R::VZ * TB]};
+        real ua = Ax[R::U0];
+        real umx1[4] = {ua * 1.0f, ua * Ax[R::VX], ua * Ax[R::VY], ua * Ax[R::VZ]};
+        real uy0 = Cy0[R::U0], uy1 = Cy1[R::U0];
+        real umy0[4] = {uy0 * 1.0f, uy0 * Cy0[R::VX], uy0 * Cy0[R::VY], uy0 * Cy0[R::VZ]};
+        real umy1[4] = {uy1 * 1.0f, uy1 * Cy1[R::VX], uy1 * Cy1[R::VY], uy1 * Cy1[R::VZ]};
 #pragma unroll
         for (int c = 0; c < 4; c++) {
           grad[0][c] = div_by<real>(grad_limit<real>(umu_prev[c], umc[c], umx1[c]), (real)p.DX, rc.DX);
@@ -343,11 +398,13 @@ __device__ __forceinline__ void tile2d(const Params& p, const GridDims& gd, cons
         for (int m = 0; m < R::NPI; m++) b.src[(4 + m) * ld + I] = S10[m];
       }
     } else if (mid) {
-      real u0c = Cs[R::U0 * TB];
+      real Cs[NP];
+      grp_load<real, RG>(Cp, TB, t, Cs);
+      real u0c = Cs[R::U0];
       umu_prev[0] = u0c * 1.0f;
-      umu_prev[1] = u0c * Cs[R::VX * TB];
-      umu_prev[2] = u0c * Cs[R::VY * TB];
-      umu_prev[3] = u0c * Cs[R::VZ * TB];
+      umu_prev[1] = u0c * Cs[R::VX];
+      umu_prev[2] = u0c * Cs[R::VY];
+      umu_prev[3] = u0c * Cs[R::VZ];
     }
     if (mid) {
 #pragma unroll
@@ -361,14 +418,18 @@ __device__ __forceinline__ void tile2d(const Params& p, const GridDims& gd, cons
     // --------------------------------------------------------- advance
     if (i + 1 < i1) {
       if (mid) {
-#pragma unroll
-        for (int f = 0; f < R::N; f++) Cs[f * TB] = A[f][t];
-        real(*tmp)[TB] = A;
+        real r[NP];
+        grp_load<real, RG>(A, TB, t, r);
+        grp_store<real, RG>(Cp, TB, t, r);
+        real* tmp = A;
         A = B;
         B = tmp;
-        rec2_make<real, BULK>(p, gd, b, tau, i + 3, jj, &B[0][t], TB);
+        rec2_make<real, BULK>(p, gd, b, tau, i + 3, jj, r);
+        grp_store<real, RG>(B, TB, t, r);
       } else {
-        rec2_make<real, BULK>(p, gd, b, tau, i + 1, jj, Cs, TB);
+        real r[NP];
+        rec2_make<real, BULK>(p, gd, b, tau, i + 1, jj, r);
+        grp_store<real, RG>(Cp, TB, t, r);
       }
       __syncthreads();
     }
