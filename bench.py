@@ -114,17 +114,31 @@ class ClockSampler(object):
             self.proc = None
         return self
 
-    def _poll(self):
+    def sample_now(self):
         n = self.nvml
+        if n is None:
+            return
+        try:
+            sm = n.nvmlDeviceGetClockInfo(self.h, n.NVML_CLOCK_SM)
+            smax = n.nvmlDeviceGetMaxClockInfo(self.h, n.NVML_CLOCK_SM)
+            r = n.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+            self.samples.append((float(sm), float(smax), int(r)))
+        except Exception:
+            pass
+
+    def _poll(self):
         while not self.stop.is_set():
-            try:
-                sm = n.nvmlDeviceGetClockInfo(self.h, n.NVML_CLOCK_SM)
-                smax = n.nvmlDeviceGetMaxClockInfo(self.h, n.NVML_CLOCK_SM)
-                r = n.nvmlDeviceGetCurrentClocksEventReasons(self.h)
-                self.samples.append((float(sm), float(smax), int(r)))
-            except Exception:
-                pass
+            self.sample_now()
             self.stop.wait(0.02)
+
+    def wait_for(self, event, every=0.01):
+        """Wait for a CUDA event, sampling the clocks from this thread every
+        `every` seconds meanwhile (the queued work is running): the polling
+        thread alone can be starved while the launching thread holds the
+        interpreter."""
+        while not event.query():
+            self.sample_now()
+            time.sleep(every)
 
     def _read(self):
         for ln in self.proc.stdout:
@@ -511,6 +525,7 @@ def run_gpu(args, rank, world, dist):
         for n in range(args.warmup, args.warmup + args.steps):
             v.step(n)
         e1.record(stream)
+        clocks.wait_for(e1)
         torch.cuda.synchronize()
     ms = max_over_ranks(e0.elapsed_time(e1), dist)
     barrier()

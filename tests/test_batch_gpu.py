@@ -132,6 +132,37 @@ def test_batch_tiled_equals_per_cell(cuda_lib, use_float32, bulk):
                 assert_same('%s event %d %s' % (name, e, shape), got, want)
 
 
+@pytest.mark.parametrize('use_float32', [True, False])
+@pytest.mark.parametrize('bulk', [False, True])
+def test_fast_batch_tiled_matches_per_cell(cuda_lib, use_float32, bulk):
+    """The tiled (2+1)D batch kernel in tolerance arithmetic (the shape the
+    batch autotuner picks) against the one-thread-per-cell kernel in the same
+    arithmetic, after 24 fixed steps: every event within the fast build's
+    tolerance (the two kernels evaluate the same expressions; the compiler may
+    contract them differently)."""
+    from clvisc_b200.batch import CLViscBatch
+    from clvisc_b200.eos import Eos
+    from test_fast_gpu import TOL, field_errors
+    ics = [seeded_ic(_cfg(g, use_float32, bulk), seed=200 + e, b=1.5 * e, edmax=7.0 + e)
+           for e, g in enumerate(GRIDS_2D)]
+    cfg0 = _cfg(GRIDS_2D[0], use_float32, bulk, arithmetic='fast')
+    runs = []
+    for shape in (('cell', 128, 148, 0), ('tile', 64, 8, None), ('tile', 128, 3, 7)):
+        b = CLViscBatch(cfg0, GRIDS_2D, max_loops=24, launch=shape)
+        assert b.params.flags & 32
+        for e, ic in enumerate(ics):
+            b.load_ini(e, ic)
+        assert b.evolve() == 24
+        runs.append([(b.ev_to_host(e), b.pi_to_host(e)) for e in range(len(GRIDS_2D))])
+    eos = Eos(cfg0.eos_type)
+    for k, run in enumerate(runs[1:], 1):
+        for e in range(len(GRIDS_2D)):
+            (gev, gpi), (wev, wpi) = run[e], runs[0][e]
+            errs = field_errors(gev, wev, np.asarray(gpi)[:, :10], np.asarray(wpi)[:, :10], eos,
+                                float(cfg0.TAU0 + 24 * cfg0.DT))
+            assert max(errs['e'], errs['T'], errs['pi']) <= TOL[use_float32], (k, e, errs)
+
+
 @pytest.mark.parametrize('bulk', [False, True])
 def test_fast_batch_matches_fast_single_runs(cuda_lib, bulk):
     """The batched stage in tolerance arithmetic (CLV_FLAG_FAST): every event
