@@ -384,8 +384,10 @@ def launch_name(shape):
     return '%dx%d/r%d' % shape[1:]
 
 
-def run_batch(n_events=BATCH_EVENTS, one_at_a_time=True):
-    """events/h of the batched runner against CLVisc one event at a time."""
+def run_batch(n_events=BATCH_EVENTS, one_at_a_time=True, launch=None):
+    """events/h of the batched runner against CLVisc one event at a time;
+    launch: a fixed launch shape (('tile', rows, chunk, grid) or ('cell',
+    block, grid, max_registers)) in place of the autotuner's choice."""
     import numpy as np
     import torch
     from clvisc_b200.batch import CLViscBatch
@@ -402,16 +404,20 @@ def run_batch(n_events=BATCH_EVENTS, one_at_a_time=True):
            'arithmetic': 'exact' if cfg.arithmetic == 'exact' else 'fast',
            'ic_host_s': ic_s}
     # autotuned launch shape (timed separately), then the timed batch from host arrays
-    bt = CLViscBatch(cfg, grids)
-    for e, ic in enumerate(ics):
-        bt.load_ini(e, ic)
-    t = time.perf_counter()
-    tuning = bt.autotune(steps=3)
-    out['autotune_s'] = time.perf_counter() - t
-    shape = bt.launch
-    out['launch'] = {'shape': launch_name(shape),
-                     'candidates_ms_per_step': {launch_name(k): round(v, 4) for k, v in sorted(tuning.items())}}
-    del bt
+    if launch is None:
+        bt = CLViscBatch(cfg, grids)
+        for e, ic in enumerate(ics):
+            bt.load_ini(e, ic)
+        t = time.perf_counter()
+        tuning = bt.autotune(steps=3)
+        out['autotune_s'] = time.perf_counter() - t
+        shape = bt.launch
+        out['launch'] = {'shape': launch_name(shape),
+                         'candidates_ms_per_step': {launch_name(k): round(v, 4) for k, v in sorted(tuning.items())}}
+        del bt
+    else:
+        shape = launch
+        out['launch'] = {'shape': launch_name(shape), 'given': True}
     torch.cuda.synchronize()
     t = time.perf_counter()
     bt = CLViscBatch(cfg, grids, launch=shape)
@@ -610,6 +616,9 @@ def main():
                     help='events of the batched workload reported under "batch" (0: skip)')
     ap.add_argument('--no-one-at-a-time', action='store_true', help='skip the one-event-at-a-time comparison')
     ap.add_argument('--batch-only', action='store_true', help='print only the batched workload line')
+    ap.add_argument('--batch-launch', default=None,
+                    help="fixed batch launch shape instead of the autotuner's: tile,ROWS,CHUNK,GRID or "
+                         "cell,BLOCK,GRID,MAXREGS")
     ap.add_argument('--surrogate-train', type=int, default=20000,
                     help='training events of the learned-surrogate experiment reported under "surrogate" '
                          '(the 20000 / 1000 configuration by default; 0: skip)')
@@ -639,7 +648,12 @@ def main():
     if args.batch_only:
         import torch
         torch.cuda.set_device(int(os.environ.get('LOCAL_RANK', 0)))
-        print(json.dumps(run_batch(args.batch_events, one_at_a_time=not args.no_one_at_a_time)), flush=True)
+        launch = None
+        if args.batch_launch:
+            f = args.batch_launch.split(',')
+            launch = (f[0],) + tuple(int(x) for x in f[1:])
+        print(json.dumps(run_batch(args.batch_events, one_at_a_time=not args.no_one_at_a_time, launch=launch)),
+              flush=True)
         return
     if args.impl == 'reference':
         # rank 0 alone times the CPU path; the other ranks exit without work
