@@ -10,7 +10,7 @@ squared-error loss and Adam on FP32 master weights. Architecture: 4 levels of
 two 3x3 convolutions with 32, 64, 128, 256 channels, skip connections by
 concatenation, a 1x1 head to 6 channels.
 
-The solver is the judge and the fallback: training and test events come from
+The solver is the yardstick and the fallback: training and test events come from
 the batched solver (CLViscBatch) on seeded initial conditions, the error of the
 network is measured against solver results, and an event is run by the solver
 instead when its prediction fails the energy balance (its transverse energy
