@@ -195,3 +195,24 @@ def test_fast_batch_matches_fast_single_runs(cuda_lib, bulk):
         assert max(errs['e'], errs['T'], errs['pi']) <= 1e-5, (e, errs)
         bitwise += int(np.array_equal(got_ev, want_ev) and np.array_equal(got_pi, want_pi))
     print('fast batch: %d of %d events bit for bit equal to their single runs' % (bitwise, len(GRIDS)))
+
+
+@pytest.mark.parametrize('use_float32', [True, False])
+def test_batch_matches_oracle(cuda_lib, oracle_mod, use_float32):
+    """The batched stage (exact build, both kernel families of (2+1)D batches
+    and the per-cell kernel of a (3+1)D event) against the oracle directly:
+    every event's ev and pi after 12 steps, bit for bit, each event run by
+    the oracle alone (OracleVisc.evolve, the restatement of visc.py)."""
+    from clvisc_b200.batch import CLViscBatch
+    grids = [(21, 19, 1), (17, 15, 5), (33, 29, 1)]
+    ics = [seeded_ic(_cfg(g, use_float32, False), seed=300 + e, b=1.0 + e, edmax=8.0 + e) for e, g in enumerate(grids)]
+    b = CLViscBatch(_cfg(grids[0], use_float32, False), grids, max_loops=12, stop_at_freezeout=False)
+    for e, ic in enumerate(ics):
+        b.load_ini(e, ic)
+    assert b.evolve() == 12
+    for e, (g, ic) in enumerate(zip(grids, ics)):
+        o = oracle_mod.OracleVisc(_cfg(g, use_float32, False))
+        o.load_ini(ic)
+        o.evolve(max_loops=12, force_run_to_maxloop=True, save_hypersf=False)
+        assert_same('batch event %d ev' % e, b.ev_to_host(e), o.ideal.d_ev[1])
+        assert_same('batch event %d pi' % e, b.pi_to_host(e), o.d_pi[1])
