@@ -127,6 +127,8 @@ clv::StageOpts stage_opts(const clv::Params& p) {
   o.chunk = p.opt[1] ? p.opt[1] : g_chunk;
   o.minb = p.opt[2] ? p.opt[2] : g_minb;
   o.tile = p.opt[3] ? p.opt[3] - 1 : g_tile;
+  o.rows2d = g_rows2d;
+  o.chunk2d = g_chunk2d;
   return o;
 }
 

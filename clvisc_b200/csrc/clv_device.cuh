@@ -85,6 +85,8 @@ struct StageOpts {
   int chunk;         // x planes per tiled (3+1)D CTA
   int minb;          // resident tiled CTAs per SM (FP32)
   int tile;          // 0 = 8 x 32, 1 = 16 x 16, 2 = 8 x 16 (y, eta)
+  int rows2d;        // threads of a tiled (2+1)D block (64 or 128)
+  int chunk2d;       // x planes per tiled (2+1)D block
 };
 
 template <class real> struct Acu;

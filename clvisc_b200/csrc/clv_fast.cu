@@ -41,6 +41,24 @@ int launch_tiled(const clv::Params& p, const clv::ViscBuffers<real>& v, int step
   return clv_host::check_cuda("fast visc_stage_tiled_kernel");
 }
 
+template <class real, bool BULK, int TB>
+int launch_tiled2d(const clv::Params& p, const clv::ViscBuffers<real>& v, int step, const clv::TauConst<real>& tc,
+                   int chunk, cudaStream_t s) {
+  typedef clv::Tile2Smem<real, BULK, TB> SM;
+  auto kern = clv::visc_stage_tiled2d_kernel<real, BULK, TB, clv::tiled2d_minb<real, TB>()>;
+  static bool configured[kMaxDev] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDev) return clv_host::check_cuda("cudaGetDevice");
+  if (!configured[dev]) {
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SM)) != cudaSuccess)
+      return clv_host::check_cuda("cudaFuncSetAttribute(fast visc_stage_tiled2d_kernel)");
+    configured[dev] = true;
+  }
+  dim3 grid((p.ny + TB - 5) / (TB - 4), (p.nx + chunk - 1) / chunk);
+  kern<<<grid, TB, sizeof(SM), s>>>(p, v, step, tc, chunk);
+  return clv_host::check_cuda("fast visc_stage_tiled2d_kernel");
+}
+
 }  // namespace
 
 template <class real>
@@ -67,6 +85,16 @@ int visc_stage(const clv::Params& p, const clv::ViscBuffers<real>& v, int step, 
       if (o.minb == 1) return launch_tiled<real, false, 1, 8, 32>(p, v, step, tc, o.chunk, s);
       return launch_tiled<real, false, 2, 8, 32>(p, v, step, tc, o.chunk, s);
     }
+  }
+  // (2+1)D grids: the tiled (2+1)D kernel (CLV_OPT_STAGE_KERNEL 3), with
+  // or without the bulk sector; not the coupling terms
+  if (p.nz == 1 && !cpl && o.stage_kernel == 3) {
+    if (o.chunk2d < 1) return clv_host::set_error(CLV_ERR_INVALID, "fast visc stage: chunk2d must be >= 1");
+    if (o.rows2d == 128)
+      return bulk ? launch_tiled2d<real, true, 128>(p, v, step, tc, o.chunk2d, s)
+                  : launch_tiled2d<real, false, 128>(p, v, step, tc, o.chunk2d, s);
+    return bulk ? launch_tiled2d<real, true, 64>(p, v, step, tc, o.chunk2d, s)
+                : launch_tiled2d<real, false, 64>(p, v, step, tc, o.chunk2d, s);
   }
   // one thread per cell: (2+1)D grids, short eta axes, the bulk sector
   const int bs = 128;

@@ -104,6 +104,37 @@ def test_fast_stage_within_tolerance(cuda_lib, oracle_mod, use_float32, grid, st
 
 
 @pytest.mark.parametrize('use_float32', [True, False])
+@pytest.mark.parametrize('bulk', [False, True])
+@pytest.mark.parametrize('rows', [64, 128])
+def test_fast_tiled2d_within_tolerance(cuda_lib, oracle_mod, use_float32, bulk, rows):
+    """The tiled (2+1)D kernel of the fast build for a single event
+    (CLV_OPT_STAGE_KERNEL 3 in the run's own options), 64- and 128-thread
+    blocks, with and without the bulk sector, against the oracle."""
+    from clvisc_b200 import _lib
+    from clvisc_b200.visc import CLVisc
+    extra = dict(ZETAOS_MAX=0.08, ZETAOS_T0=0.18, ZETAOS_WIDTH=0.03) if bulk else {}
+    cfg = make_cfg(61, 67, 1, use_float32=use_float32, arithmetic='fast', **extra)
+    ic = seeded_ic(cfg, seed=13, flow=0.2)
+    lib = _lib.load()
+    assert lib.clv_set_option(_lib.CLV_OPT_TILE2D_ROWS, rows) == 0
+    try:
+        v = CLVisc(cfg)
+        v.params.opt_stage_kernel = 4  # 1 + CLV_OPT_STAGE_KERNEL 3
+        o = oracle_mod.OracleVisc(cfg)
+        v.load_ini(ic)
+        o.load_ini(ic)
+        v.IS_initialize()
+        o.IS_initialize()
+        for n in range(12):
+            v.step(n)
+            o.step(n)
+        compare_fields(v, o, use_float32, 'fast tiled2d rows %d bulk %s %s' % (rows, bulk, 'fp32' if use_float32 else
+                                                                             'fp64'))
+    finally:
+        lib.clv_set_option(_lib.CLV_OPT_TILE2D_ROWS, 64)
+
+
+@pytest.mark.parametrize('use_float32', [True, False])
 def test_fast_bulk_and_gubser_flag(cuda_lib, oracle_mod, use_float32):
     """The fast per-cell instantiations with the bulk sector and with the
     GUBSER_VISC_TEST coupling terms."""
