@@ -7,10 +7,12 @@ the kernels read (the reference's RGBA image2d, eos.py:184-203): nrow x ncol
 texels of (cs2, p, T, s), read with clamp-to-edge nearest sampling and a
 manual linear interpolation (eos_table.h:39-62).
 
-Supported eos_type values: 'ideal_gas' (eos.py:42-59, computed here) and
+Supported eos_type values: 'ideal_gas' (eos.py:42-59, computed here),
 'lattice_pce165' (eos.py:102-113; the table is regenerated from the s95p
 source grids by eos_tables/make_pce165.py because EOS_PST.dat is absent from
-the reference snapshot). A user-built table can be passed as a
+the reference snapshot) and 'lattice_wb' (eos.py:142-153 with wb.py: the
+Wuppertal-Budapest 2014 parametrisation, computed once a process by
+eos_tables/wb.py, on the 200 x 1000 image of eos.py:184). A user-built table can be passed as a
 handcrafted_eos object with the same attributes (ideal.py:60-69).
 """
 import os
@@ -23,6 +25,9 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 TABLE_SHAPE = {
     'ideal_gas': (200, 1000),
     'lattice_pce165': (100, 1555),
+    # the reference's CLIdeal asks for 4 x 1001 here (ideal.py:79-81), which
+    # cannot hold the 200 000 entries; create_table's default shape does
+    'lattice_wb': (200, 1000),
 }
 
 
@@ -35,6 +40,8 @@ class Eos(object):
             self.ideal_gas()
         elif eos_type == 'lattice_pce165':
             self.lattice_pce165()
+        elif eos_type == 'lattice_wb':
+            self.lattice_wb()
         else:
             raise ValueError('unsupported eos_type %r (supported: %s)'
                              % (eos_type, ', '.join(sorted(TABLE_SHAPE))))
@@ -70,6 +77,15 @@ class Eos(object):
         self.s = np.interp(self.ed, e, d['src_s'])
         self.T = np.interp(self.ed, e, d['src_T'])
         self.cs2 = d['cs2'].astype(np.float64)
+        self._from_arrays()
+
+    def lattice_wb(self):
+        """Wuppertal-Budapest 2014 lattice EOS in chemical equilibrium
+        (eos.py:142-153, lattice_ce)."""
+        from .eos_tables.wb import ED_START, ED_STEP, NUM_ED, wb_arrays
+        ed, pr, T, s, cs2 = wb_arrays()
+        self.ed, self.pr, self.T, self.s, self.cs2 = ed, pr, T, s, cs2.copy()
+        self.ed_start, self.ed_step, self.num_of_ed = ED_START, ED_STEP, NUM_ED
         self._from_arrays()
 
     def _from_arrays(self):

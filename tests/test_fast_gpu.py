@@ -104,6 +104,24 @@ def test_fast_stage_within_tolerance(cuda_lib, oracle_mod, use_float32, grid, st
 
 
 @pytest.mark.parametrize('use_float32', [True, False])
+def test_fast_lattice_wb_within_tolerance(cuda_lib, oracle_mod, use_float32):
+    """The tolerance build with the Wuppertal-Budapest EOS (lattice_wb)."""
+    from clvisc_b200.visc import CLVisc
+    cfg = make_cfg(40, 37, 35, use_float32=use_float32, arithmetic='fast', eos_type='lattice_wb')
+    ic = seeded_ic(cfg, seed=23, flow=0.2)
+    v = CLVisc(cfg)
+    o = oracle_mod.OracleVisc(cfg)
+    v.load_ini(ic)
+    o.load_ini(ic)
+    v.IS_initialize()
+    o.IS_initialize()
+    for n in range(10):
+        v.step(n)
+        o.step(n)
+    compare_fields(v, o, use_float32, 'fast lattice_wb %s' % ('fp32' if use_float32 else 'fp64'))
+
+
+@pytest.mark.parametrize('use_float32', [True, False])
 @pytest.mark.parametrize('bulk', [False, True])
 @pytest.mark.parametrize('rows', [64, 128])
 def test_fast_tiled2d_within_tolerance(cuda_lib, oracle_mod, use_float32, bulk, rows):

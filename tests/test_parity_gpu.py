@@ -288,3 +288,25 @@ def test_tuned_choice_is_per_run(cuda_lib):
     assert_same('per-run kernels', a.ideal.field_to_host(a.ideal.d_ev[1]), b.ideal.field_to_host(b.ideal.d_ev[1]))
     c = CLVisc(cfg)
     assert c.params.opt_stage_kernel == 0
+
+
+@pytest.mark.parametrize('use_float32', [True, False])
+@pytest.mark.parametrize('grid', [(17, 15, 13), (40, 37, 35), (21, 19, 1)])
+def test_lattice_wb_parity(cuda_lib, oracle_mod, use_float32, grid):
+    """The Wuppertal-Budapest EOS (eos_type lattice_wb, a 200 x 1000 image):
+    fused steps of the exact build against the oracle, bit for bit, per-cell
+    and tiled kernels."""
+    from clvisc_b200.visc import CLVisc
+    cfg = make_cfg(*grid, use_float32=use_float32, eos_type='lattice_wb')
+    ic = seeded_ic(cfg, seed=21, flow=0.2)
+    v = CLVisc(cfg)
+    o = oracle_mod.OracleVisc(cfg)
+    v.load_ini(ic)
+    o.load_ini(ic)
+    for n in range(6):
+        v.step(n, edmax=True)
+        o.step(n)
+        tag = 'lattice_wb n=%d' % n
+        assert_same(tag + ' ev[1]', v.ideal.field_to_host(v.ideal.d_ev[1]), o.ideal.d_ev[1])
+        assert_same(tag + ' pi[1]', v.ideal.field_to_host(v.d_pi[1]), o.d_pi[1])
+        assert v.read_edmax_key() == o.ideal.max_energy_density()
