@@ -10,9 +10,12 @@ manual linear interpolation (eos_table.h:39-62).
 Supported eos_type values: 'ideal_gas' (eos.py:42-59, computed here),
 'lattice_pce165' (eos.py:102-113; the table is regenerated from the s95p
 source grids by eos_tables/make_pce165.py because EOS_PST.dat is absent from
-the reference snapshot) and 'lattice_wb' (eos.py:142-153 with wb.py: the
+the reference snapshot), 'lattice_wb' (eos.py:142-153 with wb.py: the
 Wuppertal-Budapest 2014 parametrisation, computed once a process by
-eos_tables/wb.py, on the 200 x 1000 image of eos.py:184). A user-built table can be passed as a
+eos_tables/wb.py, on the 200 x 1000 image of eos.py:184) and 'pure_gauge'
+(eos.py:171-182 with glueball.py: the SU(3) gauge EOS with its first-order
+transition, from the reference's glueball_v2.dat extracted by
+eos_tables/make_glueball.py). A user-built table can be passed as a
 handcrafted_eos object with the same attributes (ideal.py:60-69).
 """
 import os
@@ -28,6 +31,7 @@ TABLE_SHAPE = {
     # the reference's CLIdeal asks for 4 x 1001 here (ideal.py:79-81), which
     # cannot hold the 200 000 entries; create_table's default shape does
     'lattice_wb': (200, 1000),
+    'pure_gauge': (200, 1000),
 }
 
 
@@ -42,6 +46,8 @@ class Eos(object):
             self.lattice_pce165()
         elif eos_type == 'lattice_wb':
             self.lattice_wb()
+        elif eos_type == 'pure_gauge':
+            self.pure_gauge()
         else:
             raise ValueError('unsupported eos_type %r (supported: %s)'
                              % (eos_type, ', '.join(sorted(TABLE_SHAPE))))
@@ -88,27 +94,39 @@ class Eos(object):
         self.ed_start, self.ed_step, self.num_of_ed = ED_START, ED_STEP, NUM_ED
         self._from_arrays()
 
+    def pure_gauge(self):
+        """Pure SU(3) gauge EOS (eos.py:171-182, pure_su3): the glueball
+        table linearly interpolated onto e = 0, 0.01, .., 1999.99 GeV/fm^3
+        (glueball.py:34-40), s = (e + p) / (T + 1e-10), cs2 from p(e)."""
+        from scipy import interpolate
+        from .eos_tables.make_pce165 import cs2_from_pressure
+        d = np.load(os.path.join(_HERE, 'eos_tables', 'glueball.npz'))
+        ed = np.linspace(0.0, 2000, 200000, endpoint=False)
+        T = interpolate.interp1d(d['ed'], d['T'])(ed)
+        pr = interpolate.interp1d(d['ed'], d['pr'])(ed)
+        self.ed, self.pr, self.T = ed, pr, T
+        self.s = (ed + pr) / (T + 1.0E-10)
+        self.ed_start, self.ed_step, self.num_of_ed = 0.0, 0.01, 200000
+        self.cs2 = cs2_from_pressure(ed, pr.copy(), self.ed_step)
+        self._from_arrays()
+
     def _from_arrays(self):
-        """Linear (k=1) interpolants as eos.py:78-83 builds them."""
+        """Linear (k=1) interpolants as eos.py:78-83 builds them, with the
+        same scipy spline (linear extrapolation outside the table)."""
+        from scipy.interpolate import InterpolatedUnivariateSpline as Spline
         ed, pr, T, s = self.ed, self.pr, self.T, self.s
 
-        def lin(x, xp, fp):
-            x = np.asarray(x, dtype=np.float64)
-            y = np.interp(x, xp, fp)
-            # InterpolatedUnivariateSpline(k=1, ext=0) extrapolates linearly
-            lo = x < xp[0]
-            hi = x > xp[-1]
-            if np.any(lo):
-                y = np.where(lo, fp[0] + (x - xp[0]) * (fp[1] - fp[0]) / (xp[1] - xp[0]), y)
-            if np.any(hi):
-                y = np.where(hi, fp[-1] + (x - xp[-1]) * (fp[-1] - fp[-2]) / (xp[-1] - xp[-2]), y)
-            return y[()] if y.ndim == 0 else y
+        def wrap(f):
+            def g(x):
+                y = f(np.asarray(x, dtype=np.float64))
+                return y[()] if np.ndim(y) == 0 else y
+            return g
 
-        self.f_ed = lambda t: lin(t, T, ed)
-        self.f_T = lambda e: lin(e, ed, T)
-        self.f_P = lambda e: lin(e, ed, pr)
-        self.f_S = lambda e: lin(e, ed, s)
-        self.f_cs2 = lambda e: lin(e, ed, self.cs2)
+        self.f_ed = wrap(Spline(T, ed, k=1, ext=0))
+        self.f_T = wrap(Spline(ed, T, k=1, ext=0))
+        self.f_P = wrap(Spline(ed, pr, k=1, ext=0))
+        self.f_S = wrap(Spline(ed, s, k=1, ext=0))
+        self.f_cs2 = wrap(Spline(ed, self.cs2, k=1, ext=0))
 
     def create_table(self, nrow=None, ncol=None):
         """Return (table, meta): the float32 (nrow, ncol, 4) image of

@@ -104,10 +104,12 @@ def test_fast_stage_within_tolerance(cuda_lib, oracle_mod, use_float32, grid, st
 
 
 @pytest.mark.parametrize('use_float32', [True, False])
-def test_fast_lattice_wb_within_tolerance(cuda_lib, oracle_mod, use_float32):
-    """The tolerance build with the Wuppertal-Budapest EOS (lattice_wb)."""
+@pytest.mark.parametrize('eos_type', ['lattice_wb', 'pure_gauge'])
+def test_fast_computed_eos_within_tolerance(cuda_lib, oracle_mod, use_float32, eos_type):
+    """The tolerance build with the Wuppertal-Budapest and the pure-gauge
+    EOS."""
     from clvisc_b200.visc import CLVisc
-    cfg = make_cfg(40, 37, 35, use_float32=use_float32, arithmetic='fast', eos_type='lattice_wb')
+    cfg = make_cfg(40, 37, 35, use_float32=use_float32, arithmetic='fast', eos_type=eos_type)
     ic = seeded_ic(cfg, seed=23, flow=0.2)
     v = CLVisc(cfg)
     o = oracle_mod.OracleVisc(cfg)
@@ -118,7 +120,7 @@ def test_fast_lattice_wb_within_tolerance(cuda_lib, oracle_mod, use_float32):
     for n in range(10):
         v.step(n)
         o.step(n)
-    compare_fields(v, o, use_float32, 'fast lattice_wb %s' % ('fp32' if use_float32 else 'fp64'))
+    compare_fields(v, o, use_float32, 'fast %s %s' % (eos_type, 'fp32' if use_float32 else 'fp64'))
 
 
 @pytest.mark.parametrize('use_float32', [True, False])

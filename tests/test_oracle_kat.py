@@ -157,21 +157,23 @@ def test_eos_tables_match_reference_construction():
     assert float(Eos('lattice_pce165').f_ed(0.137)) == meta['pce165_f_ed_0137']
 
 
-def test_lattice_wb_table_matches_reference():
+@pytest.mark.parametrize('key,eos_type', [('wb', 'lattice_wb'), ('gb', 'pure_gauge')])
+def test_computed_eos_tables_match_reference(key, eos_type):
     """Eos('lattice_wb') (the Wuppertal-Budapest 2014 EOS, eos.py:142-153
-    with wb.py) gives the reference's float32 image bit for bit at the
-    golden rows (tests/golden/make_golden_wb.py imported the reference), and
-    its f_ed(0.137)."""
-    g = np.load(os.path.join(GOLD, 'golden_wb.npz'))
-    e = Eos('lattice_wb')
+    with wb.py) and Eos('pure_gauge') (eos.py:171-182 with glueball.py) give
+    the reference's float32 image bit for bit at the golden rows
+    (tests/golden/make_golden_eos.py imported the reference), and its
+    f_ed(0.137)."""
+    g = np.load(os.path.join(GOLD, 'golden_eos.npz'))
+    e = Eos(eos_type)
     t, m = e.create_table()
-    assert t.shape == (200, 1000, 4) and int(g['n']) == 200000
-    assert m['num_of_ed'] == int(g['num_of_ed']) and m['ed_step'] == float(g['ed_step'])
-    np.testing.assert_array_equal(t.reshape(-1, 4)[g['rows']], g['table'])
-    assert float(e.f_ed(0.137)) == float(g['f_ed_0137'])
+    assert t.shape == (200, 1000, 4) and int(g[key + '_n']) == 200000
+    assert m['num_of_ed'] == int(g[key + '_num_of_ed']) and m['ed_step'] == float(g[key + '_ed_step'])
+    np.testing.assert_array_equal(t.reshape(-1, 4)[g[key + '_rows']], g[key + '_table'])
+    assert float(e.f_ed(0.137)) == float(g[key + '_f_ed_0137'])
 
 
-@pytest.mark.parametrize('eos_type', ['ideal_gas', 'lattice_pce165', 'lattice_wb'])
+@pytest.mark.parametrize('eos_type', ['ideal_gas', 'lattice_pce165', 'lattice_wb', 'pure_gauge'])
 def test_oracle_eos_lookup_matches_table(oracle_mod, eos_type):
     """Inside the table the oracle's P() reproduces the tabulated pressure at
     grid points and interpolates linearly between them (eos_table.h:39-71)."""

@@ -292,12 +292,13 @@ def test_tuned_choice_is_per_run(cuda_lib):
 
 @pytest.mark.parametrize('use_float32', [True, False])
 @pytest.mark.parametrize('grid', [(17, 15, 13), (40, 37, 35), (21, 19, 1)])
-def test_lattice_wb_parity(cuda_lib, oracle_mod, use_float32, grid):
-    """The Wuppertal-Budapest EOS (eos_type lattice_wb, a 200 x 1000 image):
+@pytest.mark.parametrize('eos_type', ['lattice_wb', 'pure_gauge'])
+def test_computed_eos_parity(cuda_lib, oracle_mod, use_float32, grid, eos_type):
+    """The Wuppertal-Budapest and the pure-gauge EOS (200 x 1000 images):
     fused steps of the exact build against the oracle, bit for bit, per-cell
     and tiled kernels."""
     from clvisc_b200.visc import CLVisc
-    cfg = make_cfg(*grid, use_float32=use_float32, eos_type='lattice_wb')
+    cfg = make_cfg(*grid, use_float32=use_float32, eos_type=eos_type)
     ic = seeded_ic(cfg, seed=21, flow=0.2)
     v = CLVisc(cfg)
     o = oracle_mod.OracleVisc(cfg)
@@ -306,7 +307,7 @@ def test_lattice_wb_parity(cuda_lib, oracle_mod, use_float32, grid):
     for n in range(6):
         v.step(n, edmax=True)
         o.step(n)
-        tag = 'lattice_wb n=%d' % n
+        tag = '%s n=%d' % (eos_type, n)
         assert_same(tag + ' ev[1]', v.ideal.field_to_host(v.ideal.d_ev[1]), o.ideal.d_ev[1])
         assert_same(tag + ' pi[1]', v.ideal.field_to_host(v.d_pi[1]), o.d_pi[1])
         assert v.read_edmax_key() == o.ideal.max_energy_density()

@@ -105,12 +105,14 @@ def test_ideal_steps_match_reference_kernels(oracle_mod, use_float32):
     (dict(gubser_visc_test=True, LAM1=-10.0), dict(eos_type='ideal_gas'), (17, 15, 1)),
     (dict(riemann_test=True), {}, (21, 5, 3)),
     ({}, dict(eos_type='lattice_wb'), (15, 13, 11)),
+    ({}, dict(eos_type='pure_gauge'), (15, 13, 11)),
 ])
 @pytest.mark.parametrize('use_float32', [True, False])
 def test_switches_match_reference_kernels(oracle_mod, use_float32, extra, kw, grid):
     """The compile-time switches (visc.py:110-121): the π-ω and ω-ω
-    couplings, GUBSER_VISC_TEST, RIEMANN_TEST; and the Wuppertal-Budapest
-    EOS image (200 x 1000, EOS_NUM_OF_ROWS/COLS of eos.py:194-200)."""
+    couplings, GUBSER_VISC_TEST, RIEMANN_TEST; and the Wuppertal-Budapest and
+    pure-gauge EOS images (200 x 1000, EOS_NUM_OF_ROWS/COLS of
+    eos.py:194-200)."""
     cfg = make_cfg(*grid, use_float32=use_float32, **kw, **extra)
     o, r = _pair(oracle_mod, cfg)
     ic = seeded_ic(cfg, flow=0.3)
