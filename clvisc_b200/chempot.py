@@ -26,16 +26,20 @@ _HERE = os.path.join(os.path.dirname(os.path.abspath(__file__)), 'eos_tables')
 PCE_TYPES = ('lattice_pce165', 'lattice_pce150')
 
 
-def _tables():
-    t = np.load(os.path.join(_HERE, 'pce165_chem.npz'))
-    with open(os.path.join(_HERE, 'pce165_decays.json')) as f:
+def _tables(eos_type='lattice_pce165'):
+    """The stable species' chemical-potential table and the decay table of
+    the EOS's data set: s95p-PCE-v1 for lattice_pce150, s95p-PCE165-v0
+    otherwise (chemical_potential.py:33-36, 62-64)."""
+    tag = 'pce150' if eos_type == 'lattice_pce150' else 'pce165'
+    t = np.load(os.path.join(_HERE, '%s_chem.npz' % tag))
+    with open(os.path.join(_HERE, '%s_decays.json' % tag)) as f:
         d = json.load(f)
     return t, d['stable'], d['hadrons']
 
 
 def mu_for_stable(efrz, tab=None):
-    """Chemical potentials of the 28 stable species at efrz
-    (chemical_potential.py:61-93)."""
+    """Chemical potentials of the stable species (28 in s95p-PCE165-v0, 35 in
+    s95p-PCE-v1) at efrz (chemical_potential.py:61-93)."""
     if tab is None:
         tab = _tables()[0]
     e0, de, ne = float(tab['e0']), float(tab['de']), int(tab['ne'])
@@ -53,7 +57,7 @@ def mu_for_stable(efrz, tab=None):
 
 def chemical_potentials(efrz, eos_type='lattice_pce165'):
     """[(pid, mu)] for every hadron of the decay table, in its order."""
-    tab, stable, hadrons = _tables()
+    tab, stable, hadrons = _tables(eos_type)
     mu_s = mu_for_stable(efrz, tab)
     mu = {pid: mu_s[i] for i, pid in enumerate(stable)}
     mu['22'] = 0.0

@@ -8,9 +8,9 @@ texels of (cs2, p, T, s), read with clamp-to-edge nearest sampling and a
 manual linear interpolation (eos_table.h:39-62).
 
 Supported eos_type values: 'ideal_gas' (eos.py:42-59, computed here),
-'lattice_pce165' (eos.py:102-113; the table is regenerated from the s95p
-source grids by eos_tables/make_pce165.py because EOS_PST.dat is absent from
-the reference snapshot), 'lattice_wb' (eos.py:142-153 with wb.py: the
+'lattice_pce165' and 'lattice_pce150' (eos.py:102-127; the tables are
+regenerated from the s95p source grids by eos_tables/make_pce165.py because
+EOS_PST.dat is absent from the reference snapshot), 'lattice_wb' (eos.py:142-153 with wb.py: the
 Wuppertal-Budapest 2014 parametrisation, computed once a process by
 eos_tables/wb.py, on the 200 x 1000 image of eos.py:184) and 'pure_gauge'
 (eos.py:171-182 with glueball.py: the SU(3) gauge EOS with its first-order
@@ -28,6 +28,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 TABLE_SHAPE = {
     'ideal_gas': (200, 1000),
     'lattice_pce165': (100, 1555),
+    'lattice_pce150': (100, 1555),
     # the reference's CLIdeal asks for 4 x 1001 here (ideal.py:79-81), which
     # cannot hold the 200 000 entries; create_table's default shape does
     'lattice_wb': (200, 1000),
@@ -44,6 +45,8 @@ class Eos(object):
             self.ideal_gas()
         elif eos_type == 'lattice_pce165':
             self.lattice_pce165()
+        elif eos_type == 'lattice_pce150':
+            self.lattice_pce150()
         elif eos_type == 'lattice_wb':
             self.lattice_wb()
         elif eos_type == 'pure_gauge':
@@ -71,9 +74,9 @@ class Eos(object):
         self.ed_step = 0.01
         self.num_of_ed = 200000
 
-    def lattice_pce165(self):
+    def lattice_pce165(self, name='lattice_pce165'):
         """s95p-PCE165-v0 lattice + partial-chemical-equilibrium HRG EOS."""
-        d = np.load(os.path.join(_HERE, 'eos_tables', 'lattice_pce165.npz'))
+        d = np.load(os.path.join(_HERE, 'eos_tables', name + '.npz'))
         self.ed_start = float(d['ed_start'])
         self.ed_step = float(d['ed_step'])
         self.num_of_ed = int(d['num_of_ed'])
@@ -84,6 +87,12 @@ class Eos(object):
         self.T = np.interp(self.ed, e, d['src_T'])
         self.cs2 = d['cs2'].astype(np.float64)
         self._from_arrays()
+
+    def lattice_pce150(self):
+        """s95p-PCE-v1 lattice + partial-chemical-equilibrium HRG EOS with
+        chemical freeze-out at 150 MeV (eos.py:116-127), regenerated like
+        PCE165 (eos_tables/make_pce165.py)."""
+        self.lattice_pce165('lattice_pce150')
 
     def lattice_wb(self):
         """Wuppertal-Budapest 2014 lattice EOS in chemical equilibrium

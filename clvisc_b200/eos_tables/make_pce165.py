@@ -1,5 +1,5 @@
-"""Regenerate the s95p-PCE165-v0 equation-of-state table used by eos_type
-'lattice_pce165'.
+"""Regenerate the s95p-PCE165-v0 and s95p-PCE-v1 equation-of-state tables
+used by eos_type 'lattice_pce165' and 'lattice_pce150'.
 
 The reference loads this EOS from pyvisc/eos/eos_table/s95p-PCE165-v0/EOS_PST.dat
 (pyvisc/eos/eos.py:102-113), a file that is not present in the reference
@@ -19,9 +19,12 @@ num_of_ed = 155500 rows at e_k = 0.002*k (ed_start 0.0, ed_step 0.002):
     |cs2| > 0.34, and a least-squares fit cs2 = a/(exp(b/e) + c) for e >= 30.
 lattice_pce165.npz next to this file holds the merged source grid (float64)
 and cs2 (float32); clvisc_b200.eos rebuilds the uniform p, s, T columns from
-the source grid with the same numpy.interp call at load time. Run it from the repository root:
+the source grid with the same numpy.interp call at load time. The
+s95p-PCE-v1 table behind 'lattice_pce150' (eos.py:116-127, EOS_PST.dat of
+s95p-PCE-v1, also absent) has the same four grids and is regenerated the same
+way into lattice_pce150.npz. Run it from the repository root:
 
-    python clvisc_b200/eos_tables/make_pce165.py /path/to/reference
+    python clvisc_b200/eos_tables/make_pce165.py /path/to/reference [lattice_pce150]
 """
 import os
 import sys
@@ -65,14 +68,18 @@ def cs2_from_pressure(ed, pr, ed_step):
     return cs2
 
 
-def source_grid(refroot):
+TABLES = {'lattice_pce165': 's95p-PCE165-v0', 'lattice_pce150': 's95p-PCE-v1'}
+
+
+def source_grid(refroot, eos_type='lattice_pce165'):
     """Merged ascending (e, p, s, T) points of the four s95p grids, with the
     zero row prepended."""
-    d = os.path.join(refroot, 'pyvisc', 'eos', 'eos_table', 's95p-PCE165-v0')
+    name = TABLES[eos_type]
+    d = os.path.join(refroot, 'pyvisc', 'eos', 'eos_table', name)
     es, ps, ss, ts = [], [], [], []
     for n in range(1, 5):
-        _, _, dens = _read_grid(os.path.join(d, 's95p-PCE165-v0_dens%d.dat' % n))
-        _, _, par = _read_grid(os.path.join(d, 's95p-PCE165-v0_par%d.dat' % n))
+        _, _, dens = _read_grid(os.path.join(d, '%s_dens%d.dat' % (name, n)))
+        _, _, par = _read_grid(os.path.join(d, '%s_par%d.dat' % (name, n)))
         es.append(dens[:, 0]); ps.append(dens[:, 1]); ss.append(dens[:, 2]); ts.append(par[:, 0])
     e = np.concatenate(es); p = np.concatenate(ps); s = np.concatenate(ss); T = np.concatenate(ts)
     order = np.argsort(e, kind='stable')
@@ -89,12 +96,12 @@ def uniform(e, p, s, T):
     return ed, np.interp(ed, e, p), np.interp(ed, e, s), np.interp(ed, e, T)
 
 
-def regenerate(refroot):
-    return uniform(*source_grid(refroot))
+def regenerate(refroot, eos_type='lattice_pce165'):
+    return uniform(*source_grid(refroot, eos_type))
 
 
-def build(refroot):
-    src = source_grid(refroot)
+def build(refroot, eos_type='lattice_pce165'):
+    src = source_grid(refroot, eos_type)
     ed, pr, sd, Td = uniform(*src)
     cs2 = cs2_from_pressure(ed, pr.copy(), ED_STEP)
     return src, cs2
@@ -103,10 +110,11 @@ def build(refroot):
 if __name__ == '__main__':
     ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get('CLVISC_REFERENCE_ROOT')
     if not ref:
-        sys.exit('usage: make_pce165.py REFERENCE_ROOT (or set CLVISC_REFERENCE_ROOT): '
-                 'the directory that holds the reference project (pyvisc/, eos tables)')
-    (e, p, s, T), cs2 = build(ref)
-    out = os.path.join(os.path.dirname(os.path.abspath(__file__)), 'lattice_pce165.npz')
+        sys.exit('usage: make_pce165.py REFERENCE_ROOT [lattice_pce165|lattice_pce150] (or set '
+                 'CLVISC_REFERENCE_ROOT): the directory that holds the reference project (pyvisc/, eos tables)')
+    eos_type = sys.argv[2] if len(sys.argv) > 2 else 'lattice_pce165'
+    (e, p, s, T), cs2 = build(ref, eos_type)
+    out = os.path.join(os.path.dirname(os.path.abspath(__file__)), '%s.npz' % eos_type)
     np.savez_compressed(out, src_e=e, src_p=p, src_s=s, src_T=T, cs2=cs2.astype(np.float32),
                         ed_start=np.float64(0.0), ed_step=np.float64(ED_STEP), num_of_ed=np.int64(NUM_ED))
     print('wrote', out, e.shape, os.path.getsize(out), 'bytes')

@@ -6,10 +6,11 @@ Imports the reference's pyvisc/eos/chemical_potential.py on its own (numpy
 only) and runs ChemicalPotential(efrz, eos_type).get_chemical_potential_for_
 resonance (chemical_potential.py:95-133), the work create_table does before it
 copies the file into the reference's own tree (:146-169), for
-eos_type lattice_pce165 and ideal_gas. efrz is the freeze-out energy density
-at T = 0.137 GeV of this repository's lattice_pce165 table (the reference's
-Eos('lattice_pce165') needs EOS_PST.dat, which its snapshot lacks), also
-recorded in the fixture's name file.
+eos_type lattice_pce165 and ideal_gas, and lattice_pce150 (s95p-PCE-v1
+data). efrz is the freeze-out energy density at T = 0.137 GeV of this
+repository's lattice_pce165 (lattice_pce150) table (the reference's Eos of
+those types needs EOS_PST.dat, which its snapshot lacks), also recorded in
+the fixtures' efrz files.
 """
 import importlib.util
 import os
@@ -36,7 +37,16 @@ def main(refroot):
         shutil.rmtree(tmp)
     with open(os.path.join(HERE, 'chemical_potential_efrz.txt'), 'w') as f:
         f.write(repr(efrz) + '\n')
-    print('wrote chemical_potential_{lattice_pce165,ideal_gas}.dat at efrz', efrz)
+    # lattice_pce150 (s95p-PCE-v1 data) at its own table's T = 0.137 GeV
+    efrz150 = float(Eos('lattice_pce150').f_ed(0.137))
+    tmp = tempfile.mkdtemp()
+    mod.ChemicalPotential(efrz150, eos_type='lattice_pce150').get_chemical_potential_for_resonance(tmp)
+    shutil.copy(os.path.join(tmp, 'chemical_potential.dat'), os.path.join(HERE, 'chemical_potential_lattice_pce150.dat'))
+    shutil.rmtree(tmp)
+    with open(os.path.join(HERE, 'chemical_potential_efrz_pce150.txt'), 'w') as f:
+        f.write(repr(efrz150) + '\n')
+    print('wrote chemical_potential_{lattice_pce165,ideal_gas}.dat at efrz', efrz,
+          'and chemical_potential_lattice_pce150.dat at efrz', efrz150)
 
 
 if __name__ == '__main__':

@@ -292,11 +292,11 @@ def test_tuned_choice_is_per_run(cuda_lib):
 
 @pytest.mark.parametrize('use_float32', [True, False])
 @pytest.mark.parametrize('grid', [(17, 15, 13), (40, 37, 35), (21, 19, 1)])
-@pytest.mark.parametrize('eos_type', ['lattice_wb', 'pure_gauge'])
+@pytest.mark.parametrize('eos_type', ['lattice_wb', 'pure_gauge', 'lattice_pce150'])
 def test_computed_eos_parity(cuda_lib, oracle_mod, use_float32, grid, eos_type):
-    """The Wuppertal-Budapest and the pure-gauge EOS (200 x 1000 images):
-    fused steps of the exact build against the oracle, bit for bit, per-cell
-    and tiled kernels."""
+    """The Wuppertal-Budapest and the pure-gauge EOS (200 x 1000 images) and
+    the regenerated s95p-PCE-v1 table (100 x 1555): fused steps of the exact
+    build against the oracle, bit for bit, per-cell and tiled kernels."""
     from clvisc_b200.visc import CLVisc
     cfg = make_cfg(*grid, use_float32=use_float32, eos_type=eos_type)
     ic = seeded_ic(cfg, seed=21, flow=0.2)

@@ -106,6 +106,7 @@ def test_ideal_steps_match_reference_kernels(oracle_mod, use_float32):
     (dict(riemann_test=True), {}, (21, 5, 3)),
     ({}, dict(eos_type='lattice_wb'), (15, 13, 11)),
     ({}, dict(eos_type='pure_gauge'), (15, 13, 11)),
+    ({}, dict(eos_type='lattice_pce150'), (15, 13, 11)),
 ])
 @pytest.mark.parametrize('use_float32', [True, False])
 def test_switches_match_reference_kernels(oracle_mod, use_float32, extra, kw, grid):
