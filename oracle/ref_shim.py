@@ -8,7 +8,8 @@ vector types, address-space qualifiers, work-item functions and one image
 read, so they compile with g++ through refshim/cl_shim.hpp once the vector
 literals (real4)(a, b, c, d) are rewritten as braced lists real4{a, b, c, d}. This recipe
 copies kernel_ideal.cl, kernel_visc.cl, kernel_IS.cl, kernel_hypersf.cl,
-helper.h, eos_table.h, real_type.h and kernel_vorticity.h from the reference
+kernel_reduction.cl, helper.h, eos_table.h, real_type.h and
+kernel_vorticity.h from the reference
 tree into oracle/_ref/<configuration>/, applies that one rewrite, and
 compiles refshim/ref_driver.cpp with the -D constants the reference host
 would pass (ideal.py:146-171 and 190-194, visc.py:107-121, eos.py:194-200)
@@ -28,8 +29,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_ROOT = os.environ.get('CLVISC_REFERENCE_ROOT', '/root/reference')
 KDIR = os.path.join(REF_ROOT, 'pyvisc', 'kernel')
-SOURCES = ('kernel_ideal.cl', 'kernel_visc.cl', 'kernel_IS.cl', 'kernel_hypersf.cl', 'helper.h', 'eos_table.h',
-           'real_type.h', 'kernel_vorticity.h')
+SOURCES = ('kernel_ideal.cl', 'kernel_visc.cl', 'kernel_IS.cl', 'kernel_hypersf.cl', 'kernel_reduction.cl',
+           'helper.h', 'eos_table.h', 'real_type.h', 'kernel_vorticity.h')
 _VEC = re.compile(r'\((real[0-9]|float[0-9]|double[0-9]|int[0-9])\)\s*\(')
 
 
@@ -123,9 +124,9 @@ def _p(a):
 
 class RefKernels(object):
     """oracle.Kernels' interface over the reference's compiled kernels (the
-    hydro stages and the surface finder); the other methods (the max
-    reduction, the bulk sector, which the reference lacks) are the
-    oracle's."""
+    hydro stages and the surface finder; the max reduction as
+    reference_reduction_stage1); the other methods (reduction_stage1, the
+    bulk sector, which the reference lacks) are the oracle's."""
 
     def __init__(self, oracle_kernels, cfg, meta, table, efrz):
         self.o = oracle_kernels
@@ -187,6 +188,15 @@ class RefKernels(object):
 
     def get_udiff(self, udiff, ev0, ev1):
         self.lib.ref_get_udiff(_p(udiff), _p(ev0), _p(ev1))
+
+    def reference_reduction_stage1(self, ev, semi, size):
+        """kernel_reduction.cl's reduction_stage1 into semi[64] (64
+        work-groups of 256 work-items, each a team of 256 threads here: about
+        2 s a call on a few cores, so the orchestration keeps the oracle's
+        reduction_stage1, which a test checks against this one)."""
+        assert semi.shape[0] >= 64
+        self.lib.ref_reduction_stage1(_p(ev), _p(semi), int(size))
+        self._check()
 
     def hypersf(self, ev_old, ev_new, pi_old, pi_new, t_old, t_new, visc, sf, txyz, pisf, capacity):
         """The reference's get_hypersf / visc_hypersf into buffers of one

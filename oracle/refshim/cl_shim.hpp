@@ -4,7 +4,8 @@
 //
 // What the reference's hydro kernels (pyvisc/kernel/helper.h, eos_table.h,
 // kernel_ideal.cl, kernel_visc.cl, kernel_IS.cl, kernel_hypersf.cl,
-// kernel_vorticity.h) use of OpenCL C, given a C++ meaning here:
+// kernel_vorticity.h, kernel_reduction.cl) use of OpenCL C, given a C++
+// meaning here:
 //  * vector types float3/4/8, double3/4/8, int2 with .x..w / .s0..s3 / .s123
 //    members and element-wise arithmetic; the literal (real4)(a, b, c, d) is
 //    rewritten to the braced list real4{a, b, c, d} by the build recipe (C++
@@ -12,8 +13,8 @@
 //    also fixes the left-to-right evaluation of its elements);
 //  * address-space and kernel qualifiers (empty), __local (static: one copy
 //    shared by the work-group, whose work-items run as one OpenMP team);
-//  * work-item functions from per-thread state the launcher sets;
-//    barrier() is an OpenMP barrier of that team;
+//  * work-item functions (ids, sizes, group id) from per-thread state the
+//    launcher sets; barrier() is an OpenMP barrier of the team; MAXFLOAT;
 //  * min/max/sign with OpenCL's semantics; dot; the image read of the EOS
 //    table (clamp-to-edge, nearest) returning its four float32 channels;
 //  * atomic_inc (kernel_hypersf.cl's element counter).
@@ -21,6 +22,7 @@
 // math, as the oracle is built, and -fwrapv (the 32-bit wrap of the surface
 // finder's random-number step, kernel_hypersf.cl:126-132).
 #pragma once
+#include <cfloat>
 #include <cmath>
 #include <omp.h>
 
@@ -42,9 +44,16 @@ typedef int sampler_t;
 namespace clshim {
 extern thread_local int g_gid[3];
 extern thread_local int g_lid[3];
+extern thread_local int g_grp[3];
+extern thread_local int g_gsize[3];
+extern thread_local int g_lsize[3];
 }  // namespace clshim
 inline int get_global_id(int d) { return clshim::g_gid[d]; }
 inline int get_local_id(int d) { return clshim::g_lid[d]; }
+inline int get_group_id(int d) { return clshim::g_grp[d]; }
+inline int get_global_size(int d) { return clshim::g_gsize[d]; }
+inline int get_local_size(int d) { return clshim::g_lsize[d]; }
+#define MAXFLOAT FLT_MAX
 inline void barrier(int) {
 #pragma omp barrier
 }

@@ -1,6 +1,6 @@
 // The reference's own hydro kernels (pyvisc/kernel/kernel_ideal.cl,
-// kernel_visc.cl, kernel_IS.cl, kernel_hypersf.cl with helper.h, eos_table.h,
-// real_type.h, kernel_vorticity.h),
+// kernel_visc.cl, kernel_IS.cl, kernel_hypersf.cl, kernel_reduction.cl with
+// helper.h, eos_table.h, real_type.h, kernel_vorticity.h),
 // compiled on the CPU through cl_shim.hpp, with the launch geometry of the
 // reference host (ideal.py:211-255, visc.py:232-314): one work-item per cell
 // for the point-wise kernels; for the kt_src_along* / visc_src_along*
@@ -22,6 +22,9 @@
 namespace clshim {
 thread_local int g_gid[3];
 thread_local int g_lid[3];
+thread_local int g_grp[3];
+thread_local int g_gsize[3];
+thread_local int g_lsize[3];
 }  // namespace clshim
 
 // Each OpenCL program is built on its own; here they share one translation
@@ -38,6 +41,11 @@ namespace visc_prg {
 #include "undef_program.h"
 namespace hsf_prg {
 #include "kernel_hypersf.cl.i"
+}
+#undef __REAL_TYPE__
+#undef acu
+namespace red_prg {
+#include "kernel_reduction.cl.i"
 }
 
 typedef visc_prg::real R;
@@ -94,6 +102,33 @@ template <class F> void per_cube(int nx, int ny, int nz, F f) {
         clshim::g_lid[0] = clshim::g_lid[1] = clshim::g_lid[2] = 0;
         f();
       }
+}
+
+// a one-dimensional launch of ngroups work-groups of lsize work-items, each
+// work-group an OpenMP team (its __local arrays shared, barrier() a team
+// barrier), one work-group after another
+template <class F> void per_group_1d(int ngroups, int lsize, F f) {
+  for (int g = 0; g < ngroups; g++) {
+#pragma omp parallel num_threads(lsize)
+    {
+      if (omp_get_num_threads() != lsize) {
+#pragma omp atomic write
+        g_team_error = 1;
+      } else {
+        const int t = omp_get_thread_num();
+        for (int d = 0; d < 3; d++) {
+          clshim::g_gid[d] = clshim::g_lid[d] = clshim::g_grp[d] = 0;
+          clshim::g_gsize[d] = clshim::g_lsize[d] = 1;
+        }
+        clshim::g_gid[0] = g * lsize + t;
+        clshim::g_lid[0] = t;
+        clshim::g_grp[0] = g;
+        clshim::g_gsize[0] = ngroups * lsize;
+        clshim::g_lsize[0] = lsize;
+        f();
+      }
+    }
+  }
 }
 }  // namespace
 
@@ -154,6 +189,12 @@ void ref_update_pimn(R* pinew, R* goodcell, R* pi1, R* pistep, R4* ev1, R4* ev2,
 }
 void ref_get_udiff(R4* udiff, R4* ev0, R4* ev1) {
   per_cell([&] { visc_prg::get_udiff(udiff, ev0, ev1); });
+}
+
+// kernel_reduction.cl's first stage with the reference's launch, 64
+// work-groups of 256 (ideal.py:259-262): semi[64] gets each group's maximum
+void ref_reduction_stage1(R4* x, R* semi, int size) {
+  per_group_1d(REDUCTION_NBlocks, REDUCTION_BSZ, [&] { red_prg::reduction_stage1(x, semi, size); });
 }
 
 // kernel_hypersf.cl; sf, txyz, pisf (and the vorticity outputs) must hold one

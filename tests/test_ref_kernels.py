@@ -161,6 +161,24 @@ def test_ideal_surface_matches_reference_kernel(oracle_mod, use_float32):
     _same('surface', _surface_rows(*sr), _surface_rows(*so))
 
 
+@pytest.mark.parametrize('use_float32', [True, False])
+def test_reduction_matches_reference_kernel(oracle_mod, use_float32):
+    """kernel_reduction.cl's reduction_stage1 with the reference's launch
+    (64 work-groups of 256, ideal.py:259-262): the 64 partial maxima equal the
+    oracle's, for sizes below one pass, between, and above several passes."""
+    cfg = make_cfg(15, 13, 11, use_float32=use_float32)
+    o = oracle_mod.OracleVisc(cfg)
+    rk = ref_shim.RefKernels(o.k, cfg, o.ideal.meta, o.ideal.table, o.ideal.efrz)
+    rng = np.random.default_rng(3)
+    for n in (1000, 16384 + 5, 300001):
+        ev = rng.uniform(-5.0, 50.0, (n, 4)).astype(o.k.real)
+        a, b = np.empty(64, o.k.real), np.empty(64, o.k.real)
+        rk.reference_reduction_stage1(ev, a, n)
+        o.k.reduction_stage1(ev, b, n)
+        _same('semi n=%d' % n, a, b)
+        assert a.max() == ev[:, 0].max()
+
+
 def test_a_planted_difference_shows(oracle_mod):
     """The comparison is not vacuous: one energy density of the oracle run
     changed by one part in 1e7 shows after a step."""
